@@ -1,0 +1,293 @@
+"""Python bindings (ctypes) of the B200 B+tree engine's C ABI.
+
+The engine is the shared library ``lib/libbtree_b200.so`` (C ABI declared in
+``include/btree_b200.h``).  This module only marshals pointers: device arrays
+are ``torch`` CUDA tensors (plumbing for device memory and streams), host
+arrays are ``numpy`` arrays.  Every search runs in the library's own kernels;
+there is no Python or CPU fallback -- a missing library raises.
+
+Mirrors the reference's host API (BPTree.h:26-55) in Python form:
+
+    tree = Tree.build(keys, values)          # genBPlusTree
+    tree.point_search(q, mode="basic")       # SearchingBTreeGPUOnlyOneState
+    tree.point_search(q, mode="grouped")     # SearchingBTreeGPUCombineStep
+    tree.range_count(lo, hi, mode="basic")   # SearchingBTreeGPURange
+    tree.range_count(lo, hi, mode="2d")      # ...RangeWithGrouping
+    tree.range_count(lo, hi, mode="zorder")  # ...RangeWithGroupingZorder
+"""
+import ctypes
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libbtree_b200.so")
+
+POINT_MODES = {"basic": 0, "grouped": 1}
+RANGE_MODES = {"basic": 0, "2d": 1, "zorder": 2}
+
+STATUS = {
+    0: "BT_OK", 1: "BT_ERR_INVALID_ARGUMENT", 2: "BT_ERR_UNSORTED",
+    3: "BT_ERR_OUT_OF_MEMORY", 4: "BT_ERR_CUDA", 5: "BT_ERR_CAPACITY",
+    6: "BT_ERR_NOT_SUPPORTED", 7: "BT_ERR_TIMEOUT", 8: "BT_ERR_INTERNAL",
+}
+
+
+class BTreeError(RuntimeError):
+    """A C-ABI call returned a status other than BT_OK."""
+
+    def __init__(self, status, where, detail):
+        self.status = status
+        self.name = STATUS.get(status, str(status))
+        super().__init__(f"{where}: {self.name}: {detail}")
+
+
+class bt_info(ctypes.Structure):
+    _fields_ = [
+        ("num_keys", ctypes.c_uint64),
+        ("key_bytes", ctypes.c_uint32),
+        ("value_bytes", ctypes.c_uint32),
+        ("num_levels", ctypes.c_uint32),
+        ("fanout", ctypes.c_uint32),
+        ("leaf_keys", ctypes.c_uint32),
+        ("smem_levels", ctypes.c_uint32),
+        ("device_bytes", ctypes.c_uint64),
+        ("min_key", ctypes.c_uint64),
+        ("max_key", ctypes.c_uint64),
+        ("device", ctypes.c_int32),
+        ("values_sorted", ctypes.c_int32),
+    ]
+
+
+_lib = None
+
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_I = ctypes.c_int
+_PROTOS = {
+    "bt_version": (ctypes.c_int, []),
+    "bt_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "bt_last_error": (ctypes.c_char_p, []),
+    "bt_build": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
+    "bt_build_host": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
+    "bt_destroy": (_I, [_P]),
+    "bt_get_info": (_I, [_P, ctypes.POINTER(bt_info)]),
+    "bt_point_search": (_I, [_P, _I, _P, _U64, _P, _P]),
+    "bt_point_search_host": (_I, [_P, _I, _P, _U64, _P, _P]),
+    "bt_group_queries": (_I, [_P, _P, _U64, _P, _P, _P]),
+    "bt_range_count": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
+    "bt_range_search": (_I, [_P, _I, _P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64), _P]),
+    "bt_range_count_host": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
+    "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
+    "bt_kernel_launches": (ctypes.c_uint64, []),
+}
+
+
+def lib():
+    """Load the engine library (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python __graft_entry__.py build` "
+                "(the engine has no CPU fallback)")
+        h = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib
+
+
+def _check(status, where):
+    if status != 0:
+        detail = lib().bt_last_error().decode(errors="replace")
+        raise BTreeError(status, where, detail)
+
+
+def _width(dtype):
+    return np.dtype(dtype).itemsize
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return ctypes.c_void_p(stream)
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def _is_cuda(x):
+    return hasattr(x, "is_cuda") and x.is_cuda
+
+
+def _torch_dtype(nbytes):
+    import torch
+    return {4: torch.uint32, 8: torch.uint64}[nbytes]
+
+
+class Tree:
+    """One B+tree in device memory, built from sorted keys."""
+
+    def __init__(self, handle, info):
+        self._h = ctypes.c_void_p(handle)
+        self.info = info
+        self.key_bytes = info.key_bytes
+        self.value_bytes = info.value_bytes
+
+    @classmethod
+    def build(cls, keys, values, stream=None):
+        """keys/values: CUDA tensors (device build) or numpy arrays (host
+        build), of unsigned 4- or 8-byte integers, keys sorted ascending."""
+        L = lib()
+        out = ctypes.c_void_p()
+        n = len(keys)
+        if len(values) != n:
+            raise ValueError("keys and values differ in length")
+        if _is_cuda(keys):
+            kb, vb = keys.element_size(), values.element_size()
+            keys = keys.contiguous()
+            values = values.contiguous()
+            st = L.bt_build(_P(keys.data_ptr()), _P(values.data_ptr()), n, kb, vb,
+                            _stream_ptr(stream), ctypes.byref(out))
+        else:
+            keys = np.ascontiguousarray(keys)
+            values = np.ascontiguousarray(values)
+            kb, vb = keys.dtype.itemsize, values.dtype.itemsize
+            st = L.bt_build_host(keys.ctypes.data_as(_P), values.ctypes.data_as(_P), n, kb, vb,
+                                 _stream_ptr(stream), ctypes.byref(out))
+        _check(st, "bt_build")
+        info = bt_info()
+        _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
+        return cls(out.value, info)
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().bt_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- point search ---------------------------------------------------
+    def point_search(self, queries, mode="basic", out=None, stream=None):
+        """Values of the queried keys (all-ones on a miss), in query order.
+        CUDA tensor in -> CUDA tensor out (asynchronous on `stream`);
+        numpy in -> numpy out (host pipeline, synchronous)."""
+        L = lib()
+        m = POINT_MODES[mode]
+        n = len(queries)
+        if _is_cuda(queries):
+            import torch
+            if queries.element_size() != self.key_bytes:
+                raise ValueError("query width differs from the tree's key width")
+            queries = queries.contiguous()
+            if out is None:
+                out = torch.empty(n, dtype=_torch_dtype(self.value_bytes), device=queries.device)
+            _check(L.bt_point_search(self._h, m, _P(queries.data_ptr()), n, _P(out.data_ptr()),
+                                     _stream_ptr(stream)), "bt_point_search")
+            return out
+        queries = np.ascontiguousarray(queries)
+        if queries.dtype.itemsize != self.key_bytes:
+            raise ValueError("query width differs from the tree's key width")
+        if out is None:
+            out = np.empty(n, dtype=np.uint32 if self.value_bytes == 4 else np.uint64)
+        _check(L.bt_point_search_host(self._h, m, queries.ctypes.data_as(_P), n,
+                                      out.ctypes.data_as(_P), _stream_ptr(stream)),
+               "bt_point_search_host")
+        return out
+
+    def group(self, queries, stream=None):
+        """The grouping step alone: (grouped queries, caller index per slot)."""
+        import torch
+        n = len(queries)
+        g = torch.empty_like(queries)
+        perm = torch.empty(n, dtype=torch.uint32, device=queries.device)
+        _check(lib().bt_group_queries(self._h, _P(queries.data_ptr()), n, _P(g.data_ptr()),
+                                      _P(perm.data_ptr()), _stream_ptr(stream)), "bt_group_queries")
+        return g, perm
+
+    def search_grouped_batch(self, grouped, perm, out=None, stream=None):
+        """Search a batch from group(): out[perm[i]] = value of grouped[i]."""
+        import torch
+        n = len(grouped)
+        if out is None:
+            out = torch.empty(n, dtype=_torch_dtype(self.value_bytes), device=grouped.device)
+        _check(lib().bt_point_search_grouped_batch(self._h, _P(grouped.data_ptr()),
+                                                   _P(perm.data_ptr()), n, _P(out.data_ptr()),
+                                                   _stream_ptr(stream)),
+               "bt_point_search_grouped_batch")
+        return out
+
+    # -- range search ----------------------------------------------------
+    def range_count(self, lo, hi, mode="basic", out=None, stream=None):
+        """Number of keys in [lo[i], hi[i]] (u64), in query order."""
+        L = lib()
+        m = RANGE_MODES[mode]
+        n = len(lo)
+        if _is_cuda(lo):
+            import torch
+            lo, hi = lo.contiguous(), hi.contiguous()
+            if out is None:
+                out = torch.empty(n, dtype=torch.uint64, device=lo.device)
+            _check(L.bt_range_count(self._h, m, _P(lo.data_ptr()), _P(hi.data_ptr()), n,
+                                    _P(out.data_ptr()), _stream_ptr(stream)), "bt_range_count")
+            return out
+        lo, hi = np.ascontiguousarray(lo), np.ascontiguousarray(hi)
+        if out is None:
+            out = np.empty(n, dtype=np.uint64)
+        _check(L.bt_range_count_host(self._h, m, lo.ctypes.data_as(_P), hi.ctypes.data_as(_P), n,
+                                     out.ctypes.data_as(_P), _stream_ptr(stream)),
+               "bt_range_count_host")
+        return out
+
+    def range_search(self, lo, hi, mode="basic", ids_capacity=None, stream=None):
+        """(counts, offsets, ids): ids[offsets[i]:offsets[i]+counts[i]] are the
+        values of the keys in [lo[i], hi[i]], sorted ascending.  CUDA tensors."""
+        import torch
+        L = lib()
+        m = RANGE_MODES[mode]
+        n = len(lo)
+        lo, hi = lo.contiguous(), hi.contiguous()
+        counts = torch.empty(n, dtype=torch.uint64, device=lo.device)
+        offsets = torch.empty(n, dtype=torch.uint64, device=lo.device)
+        total = ctypes.c_uint64(0)
+        if ids_capacity is None:
+            # count first, then size the ID buffer exactly
+            st = L.bt_range_search(self._h, m, _P(lo.data_ptr()), _P(hi.data_ptr()), n,
+                                   _P(counts.data_ptr()), _P(offsets.data_ptr()), None, 0,
+                                   ctypes.byref(total), _stream_ptr(stream))
+            if st not in (0, 5):
+                _check(st, "bt_range_search")
+            ids_capacity = total.value
+        ids = torch.empty(max(1, ids_capacity), dtype=_torch_dtype(self.value_bytes),
+                          device=lo.device)
+        _check(L.bt_range_search(self._h, m, _P(lo.data_ptr()), _P(hi.data_ptr()), n,
+                                 _P(counts.data_ptr()), _P(offsets.data_ptr()), _P(ids.data_ptr()),
+                                 ids_capacity, ctypes.byref(total), _stream_ptr(stream)),
+               "bt_range_search")
+        return counts, offsets, ids[: total.value]
+
+
+def version():
+    return lib().bt_version()
+
+
+def kernel_launches():
+    """Kernel launches issued by the library so far in this process."""
+    return lib().bt_kernel_launches()

@@ -1,0 +1,269 @@
+// Bulk build: sorted (key, value) arrays -> padded leaf sectors + separator
+// levels.  Replaces genBPlusTree (BPTree.cu:127-306): the reference copies
+// PAGESIZE pairs per leaf page (assignDataToLeaf, BPTree.cu:73-125) and builds
+// (child.max, child index) pages per level with a host-synchronized loop
+// (kernelMaxIntermidatePage, BPTree.cu:28-70, :218-243).  Here the leaf level
+// is the padded sorted array itself and each separator level is one strided
+// gather of the level below; nothing is pointer-linked, so the whole build is
+// a few streaming passes with no host round trip between levels.
+#include <algorithm>
+#include <cstring>
+
+#include "bt_internal.cuh"
+
+namespace bt {
+namespace {
+
+// One thread per leaf position: copy + pad keys and values, check the
+// ascending order of keys (bit 0) and values (bit 1), and emit the bottom
+// separator level (the last key of every sector).
+template <typename K, typename V>
+__global__ void __launch_bounds__(256)
+copy_pad_kernel(const K *__restrict__ keys, const V *__restrict__ vals, uint64_t n,
+                uint64_t n_pos, K *__restrict__ out_k, V *__restrict__ out_v,
+                K *__restrict__ bottom_sep, unsigned int *__restrict__ flags) {
+    constexpr int S = kSectorBytes / sizeof(K);
+    unsigned int f = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_pos;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        K k = key_max<K>();
+        V v = 0;
+        if (i < n) {
+            k = keys[i];
+            v = vals[i];
+            if (i + 1 < n) {
+                if (keys[i + 1] < k) f |= 1u;
+                if (vals[i + 1] < v) f |= 2u;
+            }
+        }
+        out_k[i] = k;
+        out_v[i] = v;
+        if ((i % S) == S - 1) bottom_sep[i / S] = k;
+    }
+    unsigned int w = __reduce_or_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && w) atomicOr(flags, w);
+}
+
+// dst[j] = src[j*F + F-1] for j < entries (maximum of node j of the level
+// below), all-ones for the padding up to nodes*F.
+template <typename K>
+__global__ void __launch_bounds__(256)
+level_kernel(const K *__restrict__ src, uint64_t entries, uint64_t padded, K *__restrict__ dst) {
+    constexpr int F = kLineBytes / sizeof(K);
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < padded;
+         j += (uint64_t)gridDim.x * blockDim.x)
+        dst[j] = j < entries ? src[j * F + F - 1] : key_max<K>();
+}
+
+template <typename K>
+__global__ void pad_kernel(K *__restrict__ dst, uint64_t from, uint64_t to) {
+    for (uint64_t j = from + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < to;
+         j += (uint64_t)gridDim.x * blockDim.x)
+        dst[j] = key_max<K>();
+}
+
+unsigned grid_for(uint64_t n, int block) {
+    uint64_t g = (n + block - 1) / block;
+    uint64_t cap = (uint64_t)sm_count() * 16;
+    if (g > cap) g = cap;
+    return (unsigned)std::max<uint64_t>(1, g);
+}
+
+template <typename K, typename V>
+bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStream_t s) {
+    constexpr int S = kSectorBytes / sizeof(K);
+    constexpr int F = kLineBytes / sizeof(K);
+    const uint64_t n = t->n;
+    t->n_sectors = (n + S - 1) / S;
+    const uint64_t n_pos = t->n_sectors * S;
+
+    // Level geometry, bottom-up, then stored root first.
+    uint64_t ent_bu[kMaxLevels], nod_bu[kMaxLevels];
+    int L = 0;
+    uint64_t entries = t->n_sectors;
+    for (;;) {
+        if (L >= kMaxLevels) return fail(BT_ERR_INVALID_ARGUMENT, "too many keys");
+        uint64_t nodes = (entries + F - 1) / F;
+        ent_bu[L] = entries;
+        nod_bu[L] = nodes;
+        L++;
+        if (nodes == 1) break;
+        entries = nodes;
+    }
+    DevTree &dt = t->dev;
+    dt.nlevels = L;
+    uint64_t off = 0;
+    for (int lvl = 0; lvl < L; lvl++) {
+        t->lvl_entries[lvl] = ent_bu[L - 1 - lvl];
+        t->lvl_nodes[lvl] = nod_bu[L - 1 - lvl];
+        dt.lvl_off[lvl] = off;
+        off += t->lvl_nodes[lvl] * F;
+    }
+    t->seps_elems = off;
+
+    BT_CUDA(cudaMalloc(&t->d_keys, n_pos * sizeof(K)));
+    BT_CUDA(cudaMalloc(&t->d_vals, n_pos * sizeof(V)));
+    BT_CUDA(cudaMalloc(&t->d_seps, t->seps_elems * sizeof(K)));
+    unsigned int *d_flags = nullptr;
+    bt_status st = ws_alloc((void **)&d_flags, sizeof(unsigned int), s);
+    if (st != BT_OK) return st;
+    BT_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(unsigned int), s));
+
+    K *seps = (K *)t->d_seps;
+    K *bottom = seps + dt.lvl_off[L - 1];
+    count_launch();
+    copy_pad_kernel<K, V><<<grid_for(n_pos, 256), 256, 0, s>>>(
+        (const K *)d_keys, (const V *)d_vals, n, n_pos, (K *)t->d_keys, (V *)t->d_vals, bottom,
+        d_flags);
+    const uint64_t bottom_pad = t->lvl_nodes[L - 1] * F;
+    if (bottom_pad > t->n_sectors) {
+        count_launch();
+        pad_kernel<K><<<grid_for(bottom_pad - t->n_sectors, 256), 256, 0, s>>>(
+            bottom, t->n_sectors, bottom_pad);
+    }
+    for (int lvl = L - 2; lvl >= 0; lvl--) {
+        const uint64_t padded = t->lvl_nodes[lvl] * F;
+        count_launch();
+        level_kernel<K><<<grid_for(padded, 256), 256, 0, s>>>(
+            seps + dt.lvl_off[lvl + 1], t->lvl_entries[lvl], padded, seps + dt.lvl_off[lvl]);
+    }
+    BT_CUDA(cudaGetLastError());
+
+    unsigned int flags = 0;
+    K kmin = 0, kmax = 0;
+    BT_CUDA(cudaMemcpyAsync(&flags, d_flags, sizeof(flags), cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaMemcpyAsync(&kmin, t->d_keys, sizeof(K), cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaMemcpyAsync(&kmax, (const K *)t->d_keys + (n - 1), sizeof(K),
+                            cudaMemcpyDeviceToHost, s));
+    ws_free(d_flags, s);
+    BT_CUDA(cudaStreamSynchronize(s));
+    if (flags & 1u) return fail(BT_ERR_UNSORTED, "build keys are not sorted ascending");
+    t->values_sorted = (flags & 2u) ? 0 : 1;
+    t->min_key = (uint64_t)kmin;
+    t->max_key = (uint64_t)kmax;
+
+    dt.keys = t->d_keys;
+    dt.vals = t->d_vals;
+    dt.seps = t->d_seps;
+    dt.n = n;
+    dt.max_key = t->max_key;
+    dt.n_sectors = t->n_sectors;
+    // sl = number of top levels whose total size fits the budget; never the
+    // bottom level (the largest, and the last one a query reaches).
+    // lvl_off[sl] is the size of levels 0 .. sl-1.
+    int sl = 0;
+    while (sl + 1 <= L - 1 && dt.lvl_off[sl + 1] * sizeof(K) <= kSmemTopBudget) sl++;
+    dt.smem_levels = sl;
+    dt.smem_elems = (uint32_t)dt.lvl_off[sl];
+    return BT_OK;
+}
+
+template <typename K>
+bt_status build_k(bt_tree *t, const void *dk, const void *dv, cudaStream_t s) {
+    return t->val_bytes == 4 ? build_impl<K, uint32_t>(t, dk, dv, s)
+                             : build_impl<K, uint64_t>(t, dk, dv, s);
+}
+
+void free_tree(bt_tree *t) {
+    if (!t) return;
+    if (t->d_keys) cudaFree(t->d_keys);
+    if (t->d_vals) cudaFree(t->d_vals);
+    if (t->d_seps) cudaFree(t->d_seps);
+    delete t;
+}
+
+}  // namespace
+}  // namespace bt
+
+extern "C" {
+
+bt_status bt_build(const void *d_sorted_keys, const void *d_values, uint64_t n, int key_bytes,
+                   int value_bytes, void *stream, bt_tree **out) {
+    using namespace bt;
+    if (!out) return fail(BT_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if (key_bytes != 4 && key_bytes != 8)
+        return fail(BT_ERR_INVALID_ARGUMENT, "key_bytes must be 4 or 8");
+    if (value_bytes != 4 && value_bytes != 8)
+        return fail(BT_ERR_INVALID_ARGUMENT, "value_bytes must be 4 or 8");
+    if (n > 0 && (!d_sorted_keys || !d_values))
+        return fail(BT_ERR_INVALID_ARGUMENT, "keys or values pointer is NULL");
+    if (n >= (1ull << 40)) return fail(BT_ERR_INVALID_ARGUMENT, "n exceeds 2^40");
+    int dev = 0;
+    BT_CUDA(cudaGetDevice(&dev));
+    bt_status st = require_device(dev);
+    if (st != BT_OK) return st;
+    bt_tree *t = new bt_tree();
+    std::memset(t, 0, sizeof(*t));
+    t->device = dev;
+    t->key_bytes = key_bytes;
+    t->val_bytes = value_bytes;
+    t->n = n;
+    t->values_sorted = 1;
+    if (n > 0) {
+        cudaStream_t s = (cudaStream_t)stream;
+        st = key_bytes == 4 ? build_k<uint32_t>(t, d_sorted_keys, d_values, s)
+                            : build_k<uint64_t>(t, d_sorted_keys, d_values, s);
+        if (st != BT_OK) {
+            free_tree(t);
+            return st;
+        }
+    }
+    *out = t;
+    return BT_OK;
+}
+
+bt_status bt_build_host(const void *h_sorted_keys, const void *h_values, uint64_t n,
+                        int key_bytes, int value_bytes, void *stream, bt_tree **out) {
+    using namespace bt;
+    if (!out) return fail(BT_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if ((key_bytes != 4 && key_bytes != 8) || (value_bytes != 4 && value_bytes != 8))
+        return fail(BT_ERR_INVALID_ARGUMENT, "key_bytes and value_bytes must be 4 or 8");
+    if (n == 0) return bt_build(nullptr, nullptr, 0, key_bytes, value_bytes, stream, out);
+    if (!h_sorted_keys || !h_values)
+        return fail(BT_ERR_INVALID_ARGUMENT, "keys or values pointer is NULL");
+    cudaStream_t s = (cudaStream_t)stream;
+    void *dk = nullptr, *dv = nullptr;
+    bt_status st = ws_alloc(&dk, n * key_bytes, s);
+    if (st == BT_OK) st = ws_alloc(&dv, n * value_bytes, s);
+    if (st == BT_OK) {
+        cudaError_t e = cudaMemcpyAsync(dk, h_sorted_keys, n * key_bytes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dv, h_values, n * value_bytes, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpyAsync");
+    }
+    if (st == BT_OK) st = bt_build(dk, dv, n, key_bytes, value_bytes, stream, out);
+    ws_free(dk, s);
+    ws_free(dv, s);
+    return st;
+}
+
+bt_status bt_destroy(bt_tree *tree) {
+    if (!tree) return BT_OK;
+    cudaDeviceSynchronize();
+    bt::free_tree(tree);
+    return BT_OK;
+}
+
+bt_status bt_get_info(const bt_tree *t, bt_info *info) {
+    using namespace bt;
+    if (!t || !info) return fail(BT_ERR_INVALID_ARGUMENT, "tree or info is NULL");
+    std::memset(info, 0, sizeof(*info));
+    info->num_keys = t->n;
+    info->key_bytes = (uint32_t)t->key_bytes;
+    info->value_bytes = (uint32_t)t->val_bytes;
+    info->num_levels = (uint32_t)t->dev.nlevels;
+    info->fanout = (uint32_t)(kLineBytes / t->key_bytes);
+    info->leaf_keys = (uint32_t)(kSectorBytes / t->key_bytes);
+    info->smem_levels = (uint32_t)t->dev.smem_levels;
+    uint64_t npos = t->n_sectors * (kSectorBytes / t->key_bytes);
+    info->device_bytes = npos * t->key_bytes + npos * t->val_bytes + t->seps_elems * t->key_bytes;
+    info->min_key = t->min_key;
+    info->max_key = t->max_key;
+    info->device = t->device;
+    info->values_sorted = t->values_sorted;
+    return BT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+// The reference's C++ host API (BPTree.h:26-55) on top of the C ABI.  See
+// include/btree_b200_compat.h for the conventions kept and the differences.
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <iostream>
+#include <mutex>
+#include <set>
+#include <vector>
+
+#include "../../include/btree_b200_compat.h"
+#include "bt_internal.cuh"
+
+namespace {
+
+std::mutex g_mu;
+std::set<bt_tree *> g_trees;
+std::vector<ulli> g_last;
+
+// The reference's error behaviour: report and exit (gpuAssert,
+// BPTreeExactSearch.cu:864-871; CUDA_RT_CALL, BPTree.cu:16-22).
+void check(bt_status s, const char *what) {
+    if (s != BT_OK) {
+        fprintf(stderr, "GPUassert: %s failed: %s (%s)\n", what, bt_status_string(s), bt_last_error());
+        exit((int)s);
+    }
+}
+
+bt_tree *tree_of(BTPage *handle) {
+    bt_tree *t = reinterpret_cast<bt_tree *>(handle);
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_trees.count(t)) {
+        fprintf(stderr, "GPUassert: unknown tree handle %p\n", (void *)handle);
+        exit(-1);
+    }
+    return t;
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+// The reference's self-check after a point search (BPTreeExactSearch.cu:466-480):
+// results are expected to equal the query (its datasets use value == key).
+void found_report(const ulli *res, const ulli *q, ulli n) {
+    ulli miss = 0;
+    for (ulli i = 0; i < n; i++) {
+        if (res[i] != q[i] && res[i] != INVALID_DATA) {
+            std::cout << "Something wrong with searching!!!!" << std::endl;
+            std::cout << res[i] << "!=" << q[i] << std::endl;
+            break;
+        }
+        if (res[i] == INVALID_DATA) miss++;
+    }
+    std::cout << "Search step checking complete" << std::endl;
+    std::cout << "Found:" << (1 - ((float)miss) / ((float)n)) * 100 << "% of key" << std::endl;
+}
+
+void *range_common(ulli *lo, ulli *hi, ulli n, BTPage *pool, int mode, const char *banner) {
+    std::cout << banner << std::endl;
+    bt_tree *t = tree_of(pool);
+    cudaSetDevice(0);
+    std::vector<ulli> counts(n);
+    double t0 = now_ms();
+    check(bt_range_count_host(t, mode, lo, hi, n, (uint64_t *)counts.data(), nullptr),
+          "range search");
+    std::cout << "Running time Searching State2 Start-end: " << (now_ms() - t0) << std::endl;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last.swap(counts);
+    return 0;
+}
+
+}  // namespace
+
+BT_API void *genBPlusTree(ulli *devInputKey, ulli *devInput, ulli inputSize,
+                          std::vector<ulli> groupList, std::vector<ulli> groupPrefix,
+                          ulli *&dev_btree_out, ulli &treeLevel_out, ulli *&btreeIndex_out,
+                          ulli &bTreeSize_out, BTPage *&dev_globalPointer_in,
+                          ulli *&dev_currentPage_in) {
+    (void)groupList;
+    (void)groupPrefix;
+    (void)treeLevel_out;
+    (void)btreeIndex_out;
+    (void)bTreeSize_out;
+    cudaSetDevice(0);
+    double t0 = now_ms();
+    bt_tree *t = nullptr;
+    check(bt_build(devInputKey, devInput, inputSize, 8, 8, nullptr, &t), "genBPlusTree");
+    cudaFree(devInput);
+    cudaFree(devInputKey);
+    bt_info info;
+    bt_get_info(t, &info);
+    ulli root = 0;
+    if (cudaMalloc((void **)&dev_btree_out, sizeof(ulli)) != cudaSuccess ||
+        cudaMemcpy(dev_btree_out, &root, sizeof(ulli), cudaMemcpyHostToDevice) != cudaSuccess)
+        check(BT_ERR_CUDA, "genBPlusTree root");
+    ulli *pages = nullptr;
+    if (cudaMallocManaged((void **)&pages, sizeof(ulli)) != cudaSuccess)
+        check(BT_ERR_CUDA, "genBPlusTree page counter");
+    *pages = (info.device_bytes + 127) / 128;  // 128-byte lines held by the tree
+    dev_currentPage_in = pages;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_trees.insert(t);
+    }
+    dev_globalPointer_in = reinterpret_cast<BTPage *>(t);
+    std::cout << "Building the Tree " << (now_ms() - t0) / 1000.0 << std::endl;
+    return t;
+}
+
+BT_API void *SearchingBTreeGPUOnlyOneState(ulli *input_key, ulli inputSize, ulli *dev_Btree,
+                                           BTPage *dev_globalPointer) {
+    (void)dev_Btree;
+    std::cout << "SearchingBTreeGPU Naive One state Searching" << std::endl;
+    bt_tree *t = tree_of(dev_globalPointer);
+    cudaSetDevice(0);
+    std::vector<ulli> res(inputSize);
+    double t0 = now_ms();
+    check(bt_point_search_host(t, BT_POINT_BASIC, input_key, inputSize, res.data(), nullptr),
+          "point search");
+    std::cout << "Naive Running time Searching =" << (now_ms() - t0) << std::endl;
+    found_report(res.data(), input_key, inputSize);
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last.swap(res);
+    return 0;
+}
+
+BT_API void *SearchingBTreeGPUCombineStep(ulli *input_key, ulli inputSize, ulli *dev_Btree,
+                                          BTPage *dev_globalPointer) {
+    (void)dev_Btree;
+    std::cout << "SearchingBTreeGPU Combine Step" << std::endl;
+    bt_tree *t = tree_of(dev_globalPointer);
+    cudaSetDevice(0);
+    ulli *host_result = new ulli[inputSize];
+    if (inputSize > 0) {
+        ulli *dq = nullptr, *dg = nullptr, *dout = nullptr;
+        uint32_t *dperm = nullptr;
+        if (cudaMalloc((void **)&dq, inputSize * 8) != cudaSuccess ||
+            cudaMalloc((void **)&dg, inputSize * 8) != cudaSuccess ||
+            cudaMalloc((void **)&dout, inputSize * 8) != cudaSuccess ||
+            cudaMalloc((void **)&dperm, inputSize * 4) != cudaSuccess)
+            check(BT_ERR_OUT_OF_MEMORY, "grouped point search");
+        cudaMemcpy(dq, input_key, inputSize * 8, cudaMemcpyHostToDevice);
+        double t0 = now_ms();
+        check(bt_group_queries(t, dq, inputSize, dg, dperm, nullptr), "genGrouping");
+        // searching the grouped array in place returns results in grouped order
+        check(bt_point_search(t, BT_POINT_BASIC, dg, inputSize, dout, nullptr), "grouped search");
+        if (cudaDeviceSynchronize() != cudaSuccess) check(BT_ERR_CUDA, "grouped search");
+        std::cout << "combi Running time Searching State2:" << (now_ms() - t0) << std::endl;
+        cudaMemcpy(input_key, dg, inputSize * 8, cudaMemcpyDeviceToHost);
+        cudaMemcpy(host_result, dout, inputSize * 8, cudaMemcpyDeviceToHost);
+        cudaFree(dq);
+        cudaFree(dg);
+        cudaFree(dout);
+        cudaFree(dperm);
+    }
+    found_report(host_result, input_key, inputSize);
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last.assign(host_result, host_result + inputSize);
+    return host_result;
+}
+
+BT_API void *SearchingBTreeGPURange(ulli *input_key_start, ulli *input_key_end, ulli inputSize,
+                                    ulli *dev_Btree, BTPage *dev_globalPointer) {
+    (void)dev_Btree;
+    return range_common(input_key_start, input_key_end, inputSize, dev_globalPointer,
+                        BT_RANGE_BASIC, "SearchingBTreeGPU Range");
+}
+
+BT_API void *SearchingBTreeGPURangeWithGrouping(ulli *input_key_start, ulli *input_key_end,
+                                                ulli inputSize, ulli *dev_Btree,
+                                                BTPage *dev_globalPointer) {
+    (void)dev_Btree;
+    return range_common(input_key_start, input_key_end, inputSize, dev_globalPointer,
+                        BT_RANGE_GROUPED_2D, "SearchingBTreeGPU Range With Grouping");
+}
+
+BT_API void *SearchingBTreeGPURangeWithGroupingZorder(ulli *input_key_start, ulli *input_key_end,
+                                                      ulli inputSize, ulli *dev_Btree,
+                                                      BTPage *dev_globalPointer) {
+    (void)dev_Btree;
+    return range_common(input_key_start, input_key_end, inputSize, dev_globalPointer,
+                        BT_RANGE_ZORDER, "SearchingBTreeGPU Range With Grouping Zorder");
+}
+
+extern "C" {
+
+BT_API const ulli *bt_compat_last_results(ulli *n) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (n) *n = g_last.size();
+    return g_last.data();
+}
+
+BT_API bt_tree *bt_compat_tree(BTPage *dev_globalPointer) {
+    bt_tree *t = reinterpret_cast<bt_tree *>(dev_globalPointer);
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_trees.count(t) ? t : nullptr;
+}
+
+}  // extern "C"

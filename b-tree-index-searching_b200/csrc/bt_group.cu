@@ -1,0 +1,483 @@
+// Query grouping, exclusive scan and range-ID fill.
+//
+// Grouping reorders a query batch so that queries that walk the same part of
+// the tree run next to each other (in the same CTAs, at the same time), which
+// turns repeated node and leaf-sector reads into L1/L2 hits.  The reference
+// does this with an MSD radix partition by 8-bit digits, iterated until every
+// group holds at most GROUP_SEARCH_SIZE = 33,000 queries, with a host round
+// trip per pass and per group (genGrouping, grouping.cu:1677-1851;
+// radixGroupGPU :776; radixGroupSingleKernelGPU :1288), and one CTA per group.
+//
+// Here a group key of D bits is computed per query and the batch is sorted by
+// it with D/8 stable LSD counting passes (histogram -> scan -> scatter), all
+// on the device with no host round trip.  Each scatter carries the caller's
+// index, so results are written straight back in the caller's order.
+//   point : the top D bits of the key (relative to the tree's key width);
+//   2D    : (top D/2 bits of start, top D/2 bits of end), row-major -- a true
+//           2-D cell, where the reference buckets by the product of two
+//           digits (bucketIdentify2d, grouping2d.cu:24-31);
+//   Z     : the Morton interleave of those two D/2-bit coordinates, as the
+//           reference interleaves start and end (calcuateZorder2d,
+//           zOrder2d.cu:27-54) before grouping by the code.
+// A pass is stable, so the order is deterministic (the reference's in-block
+// atomicAdd scatter is not, grouping.cu:451-452).
+#include <algorithm>
+
+#include "bt_internal.cuh"
+
+namespace bt {
+namespace {
+
+constexpr int kPT = 512;             // partition threads per CTA
+constexpr int kPWarps = kPT / 32;    // 16
+constexpr int kIPL = 8;              // items per lane
+constexpr int kPTile = kPT * kIPL;   // 4096 items per tile
+constexpr int kPerWarp = 32 * kIPL;  // 256 items per warp sub-tile
+
+struct GroupKeyParams {
+    int kind;   // PartitionKind
+    int shift;  // right shift applied to keys
+    int cbits;  // bits per coordinate (2D/Z) or total bits (point)
+};
+
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+    x &= 0xFFFFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
+}
+
+template <typename K>
+__device__ __forceinline__ uint32_t group_key(K a, K b, const GroupKeyParams &p) {
+    const uint64_t lim = (1ull << p.cbits) - 1;
+    uint64_t x = (uint64_t)a >> p.shift;
+    x = x < lim ? x : lim;
+    if (p.kind == kPartPoint) return (uint32_t)x;
+    uint64_t y = (uint64_t)b >> p.shift;
+    y = y < lim ? y : lim;
+    if (p.kind == kPart2D) return (uint32_t)((x << p.cbits) | y);
+    return spread16((uint32_t)x) | (spread16((uint32_t)y) << 1);
+}
+
+template <typename K, bool HAS_B>
+__global__ void __launch_bounds__(kPT)
+part_hist_kernel(const K *__restrict__ a, const K *__restrict__ b, uint64_t n, GroupKeyParams gp,
+                 int pass, uint32_t *__restrict__ counts, uint64_t ntiles) {
+    __shared__ uint32_t h[256];
+    for (int i = threadIdx.x; i < 256; i += kPT) h[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t t0 = (uint64_t)blockIdx.x * kPTile;
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        const uint64_t i = t0 + (uint64_t)j * kPT + threadIdx.x;
+        uint32_t d = 0xFFFFFFFFu;
+        if (i < n) d = (group_key<K>(a[i], HAS_B ? b[i] : (K)0, gp) >> (8 * pass)) & 0xFFu;
+        const unsigned m = __match_any_sync(0xffffffffu, d);
+        if (d != 0xFFFFFFFFu && lane == __ffs(m) - 1) atomicAdd(&h[d], (uint32_t)__popc(m));
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < 256; d += kPT) counts[(uint64_t)d * ntiles + blockIdx.x] = h[d];
+}
+
+// Exclusive scan of 256 values held one per thread by threads 0..255.
+__device__ __forceinline__ uint32_t block_exscan256(uint32_t v, uint32_t *warp_tot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_tot[w] = x;
+    __syncwarp();
+    return x - v;  // exclusive within the warp; caller adds the warp prefix
+}
+
+template <typename K, bool HAS_B>
+__global__ void __launch_bounds__(kPT)
+part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
+                    const uint32_t *__restrict__ perm_in, uint64_t n, GroupKeyParams gp, int pass,
+                    const uint32_t *__restrict__ base, uint64_t ntiles, K *__restrict__ oa,
+                    K *__restrict__ ob, uint32_t *__restrict__ operm) {
+    __shared__ uint32_t cnt[kPWarps][256];
+    __shared__ uint32_t tile_start[256];
+    __shared__ uint32_t warp_tot[8];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sa = reinterpret_cast<K *>(smem_raw);
+    K *sb = sa + kPTile;
+    uint32_t *sp = reinterpret_cast<uint32_t *>(sb + (HAS_B ? kPTile : 0));
+    uint8_t *sd = reinterpret_cast<uint8_t *>(sp + kPTile);
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kPWarps * 256; i += kPT) (&cnt[0][0])[i] = 0;
+    __syncthreads();
+
+    const uint64_t t0 = (uint64_t)blockIdx.x * kPTile;
+    K av[kIPL], bv[kIPL];
+    uint32_t pv[kIPL], dg[kIPL], rk[kIPL];
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        const uint64_t i = t0 + (uint64_t)w * kPerWarp + (uint64_t)j * 32 + lane;
+        dg[j] = 0xFFFFFFFFu;
+        av[j] = 0;
+        bv[j] = 0;
+        pv[j] = 0;
+        if (i < n) {
+            av[j] = a[i];
+            if (HAS_B) bv[j] = b[i];
+            pv[j] = perm_in ? perm_in[i] : (uint32_t)i;
+            dg[j] = (group_key<K>(av[j], bv[j], gp) >> (8 * pass)) & 0xFFu;
+        }
+    }
+    // Stable rank of every item among the same-digit items of this warp's
+    // sub-tile (item order = j-major, then lane).
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        const unsigned m = __match_any_sync(0xffffffffu, dg[j]);
+        uint32_t c = 0;
+        if (dg[j] != 0xFFFFFFFFu) c = cnt[w][dg[j]];
+        __syncwarp();
+        if (dg[j] != 0xFFFFFFFFu && lane == __ffs(m) - 1) cnt[w][dg[j]] = c + __popc(m);
+        __syncwarp();
+        rk[j] = c + __popc(m & lt);
+    }
+    __syncthreads();
+    uint32_t tot = 0;
+    if (threadIdx.x < 256) {
+        const int d = threadIdx.x;
+        for (int ww = 0; ww < kPWarps; ww++) {
+            const uint32_t c = cnt[ww][d];
+            cnt[ww][d] = tot;
+            tot += c;
+        }
+    }
+    uint32_t ex = 0;
+    if (threadIdx.x < 256) ex = block_exscan256(tot, warp_tot);
+    __syncthreads();
+    if (threadIdx.x < 256) {
+        uint32_t wp = 0;
+        for (int ww = 0; ww < (threadIdx.x >> 5); ww++) wp += warp_tot[ww];
+        tile_start[threadIdx.x] = ex + wp;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        if (dg[j] != 0xFFFFFFFFu) {
+            const uint32_t lp = tile_start[dg[j]] + cnt[w][dg[j]] + rk[j];
+            sa[lp] = av[j];
+            if (HAS_B) sb[lp] = bv[j];
+            sp[lp] = pv[j];
+            sd[lp] = (uint8_t)dg[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t tn = (uint32_t)min((uint64_t)kPTile, n - t0);
+    for (uint32_t lp = threadIdx.x; lp < tn; lp += kPT) {
+        const uint32_t d = sd[lp];
+        const uint64_t g = (uint64_t)base[(uint64_t)d * ntiles + blockIdx.x] + (lp - tile_start[d]);
+        oa[g] = sa[lp];
+        if (HAS_B) ob[g] = sb[lp];
+        operm[g] = sp[lp];
+    }
+}
+
+// ---------------------------------------------------------------- scan ----
+
+constexpr int kST = 512;
+constexpr int kSIPT = 8;
+constexpr int kSTile = kST * kSIPT;
+
+template <typename T>
+__device__ __forceinline__ T block_exscan(T v, T *s_warp, T *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        T y = lane < (kST / 32) ? s_warp[lane] : (T)0;
+        T z = y;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T u = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += u;
+        }
+        if (lane < (kST / 32)) s_warp[lane] = z - y;
+        if (lane == 31) *total = z;
+    }
+    __syncthreads();
+    return x - v + s_warp[w];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kST) scan_reduce_kernel(const T *__restrict__ in, uint64_t n,
+                                                          T *__restrict__ sums) {
+    __shared__ T s_warp[kST / 32];
+    __shared__ T total;
+    const uint64_t t0 = (uint64_t)blockIdx.x * kSTile + (uint64_t)threadIdx.x * kSIPT;
+    T acc = 0;
+#pragma unroll
+    for (int j = 0; j < kSIPT; j++)
+        if (t0 + j < n) acc += in[t0 + j];
+    block_exscan<T>(acc, s_warp, &total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kST)
+scan_down_kernel(const T *__restrict__ in, uint64_t n, const T *__restrict__ offs,
+                 T *__restrict__ out, T *__restrict__ grand_total) {
+    __shared__ T s_warp[kST / 32];
+    __shared__ T total;
+    const uint64_t t0 = (uint64_t)blockIdx.x * kSTile + (uint64_t)threadIdx.x * kSIPT;
+    T v[kSIPT];
+    T acc = 0;
+#pragma unroll
+    for (int j = 0; j < kSIPT; j++) {
+        v[j] = (t0 + j < n) ? in[t0 + j] : (T)0;
+        acc += v[j];
+    }
+    T run = block_exscan<T>(acc, s_warp, &total) + (offs ? offs[blockIdx.x] : (T)0);
+#pragma unroll
+    for (int j = 0; j < kSIPT; j++) {
+        if (t0 + j < n) out[t0 + j] = run;
+        run += v[j];
+    }
+    if (grand_total && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0)
+        *grand_total = total + (offs ? offs[blockIdx.x] : (T)0);
+}
+
+template <typename T>
+bt_status scan_impl(const T *d_in, T *d_out, uint64_t n, T *d_total, cudaStream_t s) {
+    if (n == 0) {
+        if (d_total) BT_CUDA(cudaMemsetAsync(d_total, 0, sizeof(T), s));
+        return BT_OK;
+    }
+    const uint64_t nb = (n + kSTile - 1) / kSTile;
+    if (nb == 1) {
+        count_launch();
+        scan_down_kernel<T><<<1, kST, 0, s>>>(d_in, n, nullptr, d_out, d_total);
+        BT_CUDA(cudaGetLastError());
+        return BT_OK;
+    }
+    T *sums = nullptr, *offs = nullptr;
+    bt_status st = ws_alloc((void **)&sums, nb * sizeof(T), s);
+    if (st != BT_OK) return st;
+    st = ws_alloc((void **)&offs, nb * sizeof(T), s);
+    if (st != BT_OK) {
+        ws_free(sums, s);
+        return st;
+    }
+    count_launch();
+    scan_reduce_kernel<T><<<(unsigned)nb, kST, 0, s>>>(d_in, n, sums);
+    st = scan_impl<T>(sums, offs, nb, nullptr, s);
+    if (st == BT_OK) {
+        count_launch();
+        scan_down_kernel<T><<<(unsigned)nb, kST, 0, s>>>(d_in, n, offs, d_out, d_total);
+    }
+    ws_free(sums, s);
+    ws_free(offs, s);
+    if (st != BT_OK) return st;
+    BT_CUDA(cudaGetLastError());
+    return BT_OK;
+}
+
+// -------------------------------------------------------- partition host --
+
+template <typename K, bool HAS_B>
+bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b, uint64_t nq,
+                         K *out_a, K *out_b, uint32_t *out_perm, cudaStream_t s) {
+    GroupKeyParams gp;
+    gp.kind = kind;
+    const int kb = bitlen64(t->max_key);
+    int dbits;
+    if (kind == kPartPoint) {
+        dbits = kPointGroupBits;
+        gp.cbits = dbits;
+    } else {
+        dbits = kRangeGroupBits * 2;  // two coordinates
+        gp.cbits = kRangeGroupBits;
+    }
+    gp.shift = std::max(0, kb - gp.cbits);
+    const int passes = (dbits + 7) / 8;
+    const uint64_t ntiles = (nq + kPTile - 1) / kPTile;
+    if (ntiles * 256 >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "batch too large");
+
+    uint32_t *counts = nullptr;
+    bt_status st = ws_alloc((void **)&counts, ntiles * 256 * sizeof(uint32_t), s);
+    if (st != BT_OK) return st;
+    // ping-pong buffers for multi-pass sorts
+    K *ta[2] = {nullptr, nullptr}, *tb[2] = {nullptr, nullptr};
+    uint32_t *tp[2] = {nullptr, nullptr};
+    if (passes > 1) {
+        for (int i = 0; i < 2 && st == BT_OK; i++) {
+            st = ws_alloc((void **)&ta[i], nq * sizeof(K), s);
+            if (st == BT_OK && HAS_B) st = ws_alloc((void **)&tb[i], nq * sizeof(K), s);
+            if (st == BT_OK) st = ws_alloc((void **)&tp[i], nq * sizeof(uint32_t), s);
+        }
+    }
+    const size_t smem = (size_t)kPTile * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t) + 1);
+    auto scat = part_scatter_kernel<K, HAS_B>;
+    if (st == BT_OK) {
+        cudaError_t e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaFuncSetAttribute");
+    }
+    const K *ia = d_a, *ib = d_b;
+    const uint32_t *ip = nullptr;
+    for (int p = 0; p < passes && st == BT_OK; p++) {
+        const bool last = p == passes - 1;
+        K *oa = last ? out_a : ta[p & 1];
+        K *ob = last ? out_b : tb[p & 1];
+        uint32_t *op = last ? out_perm : tp[p & 1];
+        count_launch();
+        part_hist_kernel<K, HAS_B><<<(unsigned)ntiles, kPT, 0, s>>>(ia, ib, nq, gp, p, counts, ntiles);
+        st = scan_impl<uint32_t>(counts, counts, ntiles * 256, nullptr, s);
+        if (st != BT_OK) break;
+        count_launch();
+        scat<<<(unsigned)ntiles, kPT, smem, s>>>(ia, ib, ip, nq, gp, p, counts, ntiles, oa, ob, op);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "partition kernels");
+        ia = oa;
+        ib = ob;
+        ip = op;
+    }
+    ws_free(counts, s);
+    for (int i = 0; i < 2; i++) {
+        ws_free(ta[i], s);
+        ws_free(tb[i], s);
+        ws_free(tp[i], s);
+    }
+    return st;
+}
+
+// --------------------------------------------------------- range fill ----
+
+// One warp per query: ids[off .. off+cnt) = vals[lb .. lb+cnt).
+template <typename V>
+__global__ void __launch_bounds__(256)
+range_fill_kernel(const V *__restrict__ vals, const uint64_t *__restrict__ lb,
+                  const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off, uint64_t nq,
+                  V *__restrict__ ids) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < nq; i += nw) {
+        const uint64_t c = cnt[i], l = lb[i], o = off[i];
+        for (uint64_t k = lane; k < c; k += 32) ids[o + k] = vals[l + k];
+    }
+}
+
+// Sorts each query's ID segment when values do not ascend with keys.
+// Segments up to kSortCap values are sorted by one CTA with an in-shared-
+// memory bitonic network; longer segments are reported as unsupported.
+constexpr int kSortCap = 4096;
+
+template <typename V>
+__global__ void __launch_bounds__(512)
+segment_sort_kernel(const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off,
+                    uint64_t nq, V *__restrict__ ids, unsigned int *__restrict__ too_long) {
+    __shared__ V buf[kSortCap];
+    for (uint64_t i = blockIdx.x; i < nq; i += gridDim.x) {
+        const uint64_t c = cnt[i];
+        if (c < 2) continue;
+        if (c > kSortCap) {
+            if (threadIdx.x == 0) atomicOr(too_long, 1u);
+            continue;
+        }
+        uint32_t p2 = 1;
+        while (p2 < c) p2 <<= 1;
+        V *seg = ids + off[i];
+        for (uint32_t k = threadIdx.x; k < p2; k += blockDim.x) buf[k] = k < c ? seg[k] : key_max<V>();
+        __syncthreads();
+        for (uint32_t size = 2; size <= p2; size <<= 1) {
+            for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+                for (uint32_t k = threadIdx.x; k < p2; k += blockDim.x) {
+                    const uint32_t partner = k ^ stride;
+                    if (partner > k) {
+                        const bool asc = (k & size) == 0;
+                        const V x = buf[k], y = buf[partner];
+                        if ((x > y) == asc) {
+                            buf[k] = y;
+                            buf[partner] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) seg[k] = buf[k];
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+bt_status launch_partition(const bt_tree *t, int kind, const void *d_a, const void *d_b,
+                           uint64_t nq, void *d_out_a, void *d_out_b, uint32_t *d_perm,
+                           cudaStream_t s) {
+    if (nq == 0) return BT_OK;
+    if (nq >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "grouped batches need nq < 2^32");
+    const bool hb = kind != kPartPoint;
+    if (t->key_bytes == 4)
+        return hb ? partition_impl<uint32_t, true>(t, kind, (const uint32_t *)d_a,
+                                                   (const uint32_t *)d_b, nq, (uint32_t *)d_out_a,
+                                                   (uint32_t *)d_out_b, d_perm, s)
+                  : partition_impl<uint32_t, false>(t, kind, (const uint32_t *)d_a, nullptr, nq,
+                                                    (uint32_t *)d_out_a, nullptr, d_perm, s);
+    return hb ? partition_impl<uint64_t, true>(t, kind, (const uint64_t *)d_a,
+                                               (const uint64_t *)d_b, nq, (uint64_t *)d_out_a,
+                                               (uint64_t *)d_out_b, d_perm, s)
+              : partition_impl<uint64_t, false>(t, kind, (const uint64_t *)d_a, nullptr, nq,
+                                                (uint64_t *)d_out_a, nullptr, d_perm, s);
+}
+
+bt_status launch_scan_u64(const uint64_t *d_in, uint64_t *d_out, uint64_t n, uint64_t *d_total,
+                          cudaStream_t s) {
+    return scan_impl<uint64_t>(d_in, d_out, n, d_total, s);
+}
+
+bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
+                            const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s) {
+    if (nq == 0 || t->n == 0) return BT_OK;
+    const unsigned grid = (unsigned)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sm_count() * 8);
+    count_launch();
+    if (t->val_bytes == 4)
+        range_fill_kernel<uint32_t><<<grid, 256, 0, s>>>((const uint32_t *)t->d_vals, d_lb,
+                                                         d_counts, d_offsets, nq,
+                                                         (uint32_t *)d_ids);
+    else
+        range_fill_kernel<uint64_t><<<grid, 256, 0, s>>>((const uint64_t *)t->d_vals, d_lb,
+                                                         d_counts, d_offsets, nq,
+                                                         (uint64_t *)d_ids);
+    BT_CUDA(cudaGetLastError());
+    if (t->values_sorted) return BT_OK;
+    unsigned int *flag = nullptr;
+    bt_status st = ws_alloc((void **)&flag, sizeof(unsigned int), s);
+    if (st != BT_OK) return st;
+    BT_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), s));
+    const unsigned g2 = (unsigned)std::min<uint64_t>(nq, (uint64_t)sm_count() * 4);
+    count_launch();
+    if (t->val_bytes == 4)
+        segment_sort_kernel<uint32_t><<<g2, 512, 0, s>>>(d_counts, d_offsets, nq, (uint32_t *)d_ids,
+                                                         flag);
+    else
+        segment_sort_kernel<uint64_t><<<g2, 512, 0, s>>>(d_counts, d_offsets, nq, (uint64_t *)d_ids,
+                                                         flag);
+    unsigned int h = 0;
+    BT_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, s));
+    ws_free(flag, s);
+    BT_CUDA(cudaStreamSynchronize(s));
+    if (h) return fail(BT_ERR_NOT_SUPPORTED, "a range hit more than 4096 keys whose values are not ascending; ID sort for such ranges is not built");
+    return BT_OK;
+}
+
+}  // namespace bt

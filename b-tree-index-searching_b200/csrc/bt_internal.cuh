@@ -1,0 +1,130 @@
+// Internal definitions shared by the engine's translation units.
+//
+// Tree layout in HBM (one allocation per array, 256-byte aligned):
+//
+//   keys   K[n_sectors * S]   the sorted keys, padded with the all-ones key;
+//                             S = 32 / sizeof(key) keys form one 32-byte
+//                             DRAM sector ("leaf sector").
+//   vals   V[n_sectors * S]   the values, same positions (struct of arrays).
+//   seps   separator levels, stored root first.  Level t holds nodes of
+//                             F = 128 / sizeof(key) separators (one 128-byte
+//                             line).  A separator is the maximum key of the
+//                             node (or leaf sector) below it, as in the
+//                             reference's internal pages (BPTree.cu:54-55).
+//
+// Child j of node i at level t is node i*F + j of level t+1; the children of
+// the bottom level are leaf sectors.  No pointers are stored.  A search for
+// q <= max_key takes, at every level, the first separator >= q (lower bound)
+// or > q (upper bound); padding separators are all-ones and never win.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/btree_b200.h"
+
+#define BT_VERSION_NUMBER 10000
+
+namespace bt {
+
+constexpr int kLineBytes = 128;   // internal node size
+constexpr int kSectorBytes = 32;  // leaf sector size
+constexpr int kMaxLevels = 24;
+
+// Shared-memory budget for the staged top levels of one search CTA.
+constexpr size_t kSmemTopBudget = 40 * 1024;
+
+struct DevTree {
+    const void *keys;
+    const void *vals;
+    const void *seps;
+    uint64_t n;
+    uint64_t max_key;
+    uint64_t n_sectors;
+    uint64_t lvl_off[kMaxLevels];  // element offset of level t in seps (t = 0 is the root)
+    int nlevels;
+    int smem_levels;               // levels 0 .. smem_levels-1 are staged in shared memory
+    uint32_t smem_elems;           // elements staged (= lvl_off[smem_levels])
+};
+
+}  // namespace bt
+
+struct bt_tree {
+    int device;
+    int key_bytes;
+    int val_bytes;
+    uint64_t n;
+    uint64_t n_sectors;
+    void *d_keys;
+    void *d_vals;
+    void *d_seps;
+    uint64_t seps_elems;
+    uint64_t lvl_nodes[bt::kMaxLevels];
+    uint64_t lvl_entries[bt::kMaxLevels];
+    uint64_t min_key, max_key;
+    int values_sorted;
+    bt::DevTree dev;
+};
+
+namespace bt {
+
+// Thread-local error detail, set by fail().
+void set_error(const std::string &msg);
+bt_status fail(bt_status s, const std::string &msg);
+bt_status cuda_fail(cudaError_t e, const char *what);
+
+#define BT_CUDA(call)                                            \
+    do {                                                         \
+        cudaError_t e__ = (call);                                \
+        if (e__ != cudaSuccess) return ::bt::cuda_fail(e__, #call); \
+    } while (0)
+
+// Stream-ordered allocation from the engine's own memory pool on the
+// current device (cached between calls, never returned to other users).
+bt_status ws_alloc(void **p, size_t bytes, cudaStream_t s);
+void ws_free(void *p, cudaStream_t s);
+
+// Counts one kernel launch (bt_kernel_launches).
+void count_launch();
+// Number of SMs of the current device (cached).
+int sm_count();
+// Checks the current device is sm_100 class.
+bt_status require_device(int device);
+
+template <typename K>
+__host__ __device__ constexpr K key_max() {
+    return (K)~(K)0;
+}
+
+inline int bitlen64(uint64_t v) {
+    int b = 0;
+    while (v) {
+        v >>= 1;
+        b++;
+    }
+    return b;
+}
+
+// Host launchers implemented in the .cu files.
+bt_status launch_point_search(const bt_tree *t, const void *d_q, const uint32_t *d_perm,
+                              uint64_t nq, void *d_out, cudaStream_t s);
+bt_status launch_bounds(const bt_tree *t, const void *d_lo, const void *d_hi,
+                        const uint32_t *d_perm, uint64_t nq, uint64_t *d_counts,
+                        uint64_t *d_lb, cudaStream_t s);
+bt_status launch_partition(const bt_tree *t, int kind, const void *d_a, const void *d_b,
+                           uint64_t nq, void *d_out_a, void *d_out_b, uint32_t *d_perm,
+                           cudaStream_t s);
+bt_status launch_scan_u64(const uint64_t *d_in, uint64_t *d_out, uint64_t n, uint64_t *d_total,
+                          cudaStream_t s);
+bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
+                            const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
+
+// Partition kinds for launch_partition.
+enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2 };
+// Digit bits used by the grouping passes.
+constexpr int kPointGroupBits = 8;
+constexpr int kRangeGroupBits = 8;
+
+}  // namespace bt

@@ -1,0 +1,160 @@
+"""Seeded synthetic workloads for the benchmark configurations.
+
+The reference ships no datasets (its runs read files at author paths,
+run.sh:1, script.sh:5) and its generator cannot be built (randgen.cu:12
+includes an absent third-party library), so every workload here is generated
+from fixed seeds with numpy's PCG64:
+
+  point_uniform  -- n unique uniform u32 keys (value = rank); queries: even
+                    slots an existing key, odd slots uniform u32.
+  point_zipf     -- n unique uniform u32 keys; queries: 90% keys whose rank
+                    follows Zipf(0.99) through a random rank permutation,
+                    10% uniform u32.
+  zorder_points  -- (x, y) uniform u16 points keyed by their 32-bit Morton
+                    code, value = point ID, sorted by (code, ID); rectangles
+                    with a uniform corner and sides uniform in [1, 256].
+  lognormal_keys -- u64 keys = cumulative sum of floor(lognormal(4, 2)) + 1.
+
+Zipf sampling uses rejection-inversion (W. Hormann, G. Derflinger, "Rejection-
+inversion to generate variates from monotone discrete distributions", ACM
+TOMACS 6(3), 1996), vectorised.
+"""
+import numpy as np
+
+KEY_SEED = 1
+
+
+def rng(seed):
+    return np.random.Generator(np.random.PCG64(seed))
+
+
+def unique_sorted_u32(n, seed=KEY_SEED):
+    """n distinct u32 values, uniform over [0, 2^32), sorted ascending."""
+    if n > (1 << 31):
+        raise ValueError("n too large for unique u32 keys")
+    g = rng(seed)
+    extra = max(1024, int(n * n / float(1 << 32)) * 2 + 4096)
+    while True:
+        v = np.unique(g.integers(0, 1 << 32, size=n + extra, dtype=np.uint64).astype(np.uint32))
+        if len(v) >= n:
+            break
+        extra *= 2
+    if len(v) > n:
+        drop = g.choice(len(v), size=len(v) - n, replace=False)
+        keep = np.ones(len(v), dtype=bool)
+        keep[drop] = False
+        v = v[keep]
+    return v
+
+
+def _h_integral(x, s):
+    lx = np.log(x)
+    t = (1.0 - s) * lx
+    return np.where(np.abs(t) > 1e-8, np.expm1(t) / np.where(t == 0, 1, t), 1.0 + t / 2) * lx
+
+
+def _h_integral_inv(x, s):
+    t = x * (1.0 - s)
+    t = np.maximum(t, -1.0 + 1e-16)
+    f = np.where(np.abs(t) > 1e-8, np.log1p(t) / np.where(t == 0, 1, t), 1.0 - t / 2)
+    return np.exp(f * x)
+
+
+def zipf_ranks(num, n, s, g):
+    """num draws from Zipf(s) over ranks 1..n (rejection-inversion)."""
+    h = lambda x: np.exp(-s * np.log(x))
+    hx1 = _h_integral(np.array(1.5), s) - 1.0
+    hn = _h_integral(np.array(n + 0.5), s)
+    ss = 2.0 - _h_integral_inv(_h_integral(np.array(2.5), s) - h(2.0), s)
+    out = np.empty(num, dtype=np.int64)
+    todo = np.arange(num)
+    while len(todo):
+        u = hn + g.random(len(todo)) * (hx1 - hn)
+        x = _h_integral_inv(u, s)
+        k = np.clip(np.floor(x + 0.5), 1, n)
+        ok = (k - x <= ss) | (u >= _h_integral(k + 0.5, s) - h(k))
+        out[todo[ok]] = k[ok].astype(np.int64)
+        todo = todo[~ok]
+    return out
+
+
+def point_uniform(n_keys=1 << 20, n_queries=1 << 20, seed=KEY_SEED):
+    """Plain point search workload: value = rank, 50% hits / 50% uniform."""
+    keys = unique_sorted_u32(n_keys, seed)
+    vals = np.arange(n_keys, dtype=np.uint32)
+    g = rng(seed + 1)
+    q = g.integers(0, 1 << 32, size=n_queries, dtype=np.uint64).astype(np.uint32)
+    q[0::2] = keys[g.integers(0, n_keys, size=len(q[0::2]))]
+    return keys, vals, q
+
+
+def point_zipf(n_keys=1 << 26, n_queries=1 << 24, s=0.99, miss=0.10, seed=KEY_SEED):
+    """Radix-grouped point search workload: Zipf(s) ranks over a random rank
+    permutation, a `miss` fraction of uniform u32 queries."""
+    keys = unique_sorted_u32(n_keys, seed)
+    vals = np.arange(n_keys, dtype=np.uint32)
+    g = rng(seed + 1)
+    ranks = zipf_ranks(n_queries, n_keys, s, g) - 1
+    perm = g.permutation(n_keys).astype(np.int64)
+    q = keys[perm[ranks]]
+    m = g.random(n_queries) < miss
+    q[m] = g.integers(0, 1 << 32, size=int(m.sum()), dtype=np.uint64).astype(np.uint32)
+    return keys, vals, q
+
+
+def morton_u16(x, y):
+    """32-bit Morton code: bits of x at even, bits of y at odd positions."""
+    def spread(v):
+        v = v.astype(np.uint32) & np.uint32(0xFFFF)
+        v = (v | (v << np.uint32(8))) & np.uint32(0x00FF00FF)
+        v = (v | (v << np.uint32(4))) & np.uint32(0x0F0F0F0F)
+        v = (v | (v << np.uint32(2))) & np.uint32(0x33333333)
+        v = (v | (v << np.uint32(1))) & np.uint32(0x55555555)
+        return v
+    return spread(x) | (spread(y) << np.uint32(1))
+
+
+def zorder_points(n_points=1 << 24, n_rects=1 << 20, max_side=256, seed=KEY_SEED):
+    """2-D points keyed by Morton code (duplicates allowed) and rectangles.
+    Returns (z_sorted u32, ids u32 in the same order, x0, y0, x1, y1 u16)."""
+    g = rng(seed)
+    x = g.integers(0, 1 << 16, size=n_points, dtype=np.uint32)
+    y = g.integers(0, 1 << 16, size=n_points, dtype=np.uint32)
+    z = morton_u16(x, y)
+    ids = np.arange(n_points, dtype=np.uint32)
+    order = np.lexsort((ids, z))
+    z, ids = z[order], ids[order]
+    g2 = rng(seed + 1)
+    x0 = g2.integers(0, 1 << 16, size=n_rects, dtype=np.uint32)
+    y0 = g2.integers(0, 1 << 16, size=n_rects, dtype=np.uint32)
+    w = g2.integers(1, max_side + 1, size=n_rects, dtype=np.uint32)
+    h = g2.integers(1, max_side + 1, size=n_rects, dtype=np.uint32)
+    x1 = np.minimum(x0 + w - 1, 0xFFFF)
+    y1 = np.minimum(y0 + h - 1, 0xFFFF)
+    u16 = np.uint16
+    return z, ids, x0.astype(u16), y0.astype(u16), x1.astype(u16), y1.astype(u16)
+
+
+def lognormal_keys(n_keys=1 << 28, mu=4.0, sigma=2.0, seed=KEY_SEED, chunk=1 << 24):
+    """Unique ascending u64 keys: cumulative sum of floor(lognormal) + 1 gaps."""
+    g = rng(seed)
+    keys = np.empty(n_keys, dtype=np.uint64)
+    acc = np.uint64(0)
+    for i in range(0, n_keys, chunk):
+        m = min(chunk, n_keys - i)
+        gaps = np.floor(g.lognormal(mu, sigma, size=m)).astype(np.uint64) + np.uint64(1)
+        c = np.cumsum(gaps, dtype=np.uint64) + acc
+        keys[i:i + m] = c
+        acc = c[-1]
+    return keys
+
+
+def range_queries(keys, n_queries, max_width_ranks, seed=KEY_SEED + 2):
+    """Ranges [key[r], key[min(r + w - 1, n - 1)]] with w uniform in
+    [1, max_width_ranks] (width in ranks), plus their exact counts."""
+    g = rng(seed)
+    n = len(keys)
+    r = g.integers(0, n, size=n_queries)
+    w = g.integers(1, max_width_ranks + 1, size=n_queries)
+    e = np.minimum(r + w - 1, n - 1)
+    return keys[r], keys[e]

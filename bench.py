@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 B+tree engine.
+
+Default workload (one "step" = one radix-grouped batch point search):
+2^26 unique uniform u32 keys (value = rank), bulk-built once; a batch of
+2^24 point queries, 90% keys drawn with Zipf(0.99) ranks, 10% uniform u32;
+queries radix-grouped by their top 8 bits, then searched.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line on rank 0.  `value` is whole-job queries/s with the
+queries resident in HBM (device-timed with CUDA events, max over ranks);
+`e2e` is the same metric through the host-buffer C-ABI call
+bt_point_search_host (H2D of the queries and D2H of the results inside the
+timed region).  The path shards as independent replicas (every rank holds the
+tree and answers its own batch, no collective on the data path), so N GPUs
+report weak scaling.  `--impl reference` times the CPU restatement of the
+reference's algorithm (its fanout-5000 page tree, oracle/oracle.c) on the
+host cores.
+"""
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "b-tree-index-searching_b200"
+METRIC = "point & range queries/sec on 1 B200, plain vs batched+learned; p99 latency"
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse_args(argv=None):
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--keys-log2", type=int, default=26)
+    p.add_argument("--queries-log2", type=int, default=24)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-log2", type=int, default=22)
+    return p.parse_args(argv)
+
+
+# ----------------------------------------------------------------- ranks ----
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def init_dist(world, local_rank, backend="nccl"):
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as dist
+    kw = {}
+    if backend == "nccl":
+        kw["device_id"] = torch.device("cuda", local_rank)
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+    return dist
+
+
+def max_over_ranks(x, dist, device=None):
+    """Max of a float over all ranks (the job's time is its slowest rank)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, device=None):
+    if dist is not None:
+        if device is not None:
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ---------------------------------------------------------------- clocks ----
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of the local GPU during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons, n = [], None, set(), 0
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                n += 1
+                for name, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": n}
+
+
+# -------------------------------------------------------------- workload ----
+
+def workload(keys_log2, queries_log2, rank):
+    wl = importlib.import_module(PKG + ".workloads")
+    cache = os.path.join(tempfile.gettempdir(), "btree_b200_bench")
+    os.makedirs(cache, exist_ok=True)
+    tag = f"zipf_k{keys_log2}_q{queries_log2}_r{rank}"
+    f = os.path.join(cache, tag + ".npz")
+    if os.path.exists(f):
+        d = np.load(f)
+        return d["keys"], d["vals"], d["q"]
+    keys, vals, q = wl.point_zipf(1 << keys_log2, 1 << queries_log2, seed=wl.KEY_SEED)
+    if rank:
+        # each replica answers its own batch (weak scaling)
+        _, _, q = wl.point_zipf(1 << keys_log2, 1 << queries_log2, seed=wl.KEY_SEED + 100 * rank)
+    np.savez(f, keys=keys, vals=vals, q=q)
+    return keys, vals, q
+
+
+def workload_desc(args):
+    return {
+        "workload": (f"radix-grouped point search: 2^{args.keys_log2} unique uniform u32 keys "
+                     f"(value = rank), batches of 2^{args.queries_log2} queries, 90% keys by "
+                     "Zipf(0.99) rank, 10% uniform u32; grouped by the top 8 key bits"),
+        "keys": 1 << args.keys_log2,
+        "queries_per_step": 1 << args.queries_log2,
+        "key_type": "u32", "value_type": "u32",
+        "l2": "flushed before every timed step (512 MiB write); tree (512 MiB) > L2",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(name):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)[name]
+        return float(d["bytes_per_query"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+# ------------------------------------------------------------ cpu leg -------
+
+def cpu_refc_qps(keys, vals, q, sample_log2, repeats=3):
+    """The reference's algorithm on the host cores: its fanout-5000 page tree
+    restated in C (oracle/oracle.c refc_*), OpenMP over all cores."""
+    from oracle.oracle import Oracle
+    orc = Oracle()
+    t = orc.refc_build(keys.astype(np.uint64), vals.astype(np.uint64))
+    qs = q[: min(len(q), 1 << sample_log2)].astype(np.uint64)
+    best = None
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        t.point_basic(qs)
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    t.close()
+    # lower_bound over the sorted array, same sample (secondary figure)
+    t0 = time.perf_counter()
+    orc.point_search(keys, vals, q[: len(qs)])
+    lb = len(qs) / (time.perf_counter() - t0)
+    return len(qs) / best, lb, len(qs)
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    keys, vals, q = workload(args.keys_log2, args.queries_log2, 0)
+    from oracle.oracle import Oracle
+    orc = Oracle()
+    t = orc.refc_build(keys.astype(np.uint64), vals.astype(np.uint64))
+    sample = min(len(q), 1 << args.cpu_sample_log2)
+    qs = q[:sample].astype(np.uint64)
+    for _ in range(args.warmup):
+        t.point_basic(qs)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        t.point_basic(qs)
+        times.append(time.perf_counter() - t0)
+    t.close()
+    ms = 1000.0 * statistics.mean(times)
+    qps = sample / statistics.mean(times)
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (seeded)", "config": workload_desc(args),
+        "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
+                         "sample": f"{sample} of the step's queries per step, reference page "
+                                   "tree (fanout 5000) restated in C, OpenMP"},
+        "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------ GPU leg -------
+
+def run_ours(args):
+    import torch
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    dist = init_dist(world, local_rank)
+    bt = importlib.import_module(PKG)
+    L = bt.lib()
+
+    keys, vals, q = workload(args.keys_log2, args.queries_log2, rank)
+    nq = len(q)
+    stream = torch.cuda.current_stream(device)
+    tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
+    dq = torch.from_numpy(q).to(device)
+    grouped = torch.empty_like(dq)
+    perm = torch.empty(nq, dtype=torch.uint32, device=device)
+    out = torch.empty(nq, dtype=torch.uint32, device=device)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    P = ctypes.c_void_p
+    sp = P(stream.cuda_stream)
+
+    def group_into():
+        bt._check(L.bt_group_queries(tree.handle, P(dq.data_ptr()), nq, P(grouped.data_ptr()),
+                                     P(perm.data_ptr()), sp), "group")
+
+    def search_grouped():
+        bt._check(L.bt_point_search_grouped_batch(tree.handle, P(grouped.data_ptr()),
+                                                  P(perm.data_ptr()), nq, P(out.data_ptr()), sp),
+                  "search")
+
+    def search_basic():
+        bt._check(L.bt_point_search(tree.handle, 0, P(dq.data_ptr()), nq, P(out.data_ptr()), sp),
+                  "basic")
+
+    # warm-up (also checks the result against the CPU judge on rank 0)
+    for _ in range(max(args.warmup, 3)):
+        group_into()
+        search_grouped()
+    torch.cuda.synchronize(device)
+    res = out.cpu().numpy()
+    hits = int(np.count_nonzero(res != np.uint32(0xFFFFFFFF)))
+    checked = None
+    if rank == 0:
+        from oracle.oracle import Oracle
+        checked = bool(np.array_equal(res, Oracle().point_search(keys, vals, q)))
+
+    # ---- timed region: K grouped steps, device time per step ----------------
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    clocks = ClockSampler(local_rank)
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    clocks.start()
+    launches0 = L.bt_kernel_launches()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        group_into()
+        ev[i][1].record(stream)
+        search_grouped()
+        ev[i][2].record(stream)
+    torch.cuda.synchronize(device)
+    launches = L.bt_kernel_launches() - launches0
+    barrier(dist, device)
+    clk = clocks.stop()
+    step_ms = [ev[i][0].elapsed_time(ev[i][2]) for i in range(args.steps)]
+    search_ms = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
+    group_ms = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
+    ms = max_over_ranks(statistics.mean(step_ms), dist, device)
+    value = world * nq / (ms / 1000.0)
+
+    # ---- ungrouped basic search, same batch (the plain path) ----------------
+    for _ in range(2):
+        search_basic()
+    bev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        bev[i][0].record(stream)
+        search_basic()
+        bev[i][1].record(stream)
+    torch.cuda.synchronize(device)
+    basic_ms = max_over_ranks(statistics.mean(b[0].elapsed_time(b[1]) for b in bev), dist, device)
+
+    # ---- end to end through the host-buffer C-ABI call ----------------------
+    hq = torch.from_numpy(q).pin_memory()
+    hout = torch.empty(nq, dtype=torch.uint32).pin_memory()
+    hq_p, hout_p = P(hq.data_ptr()), P(hout.data_ptr())
+    for _ in range(2):
+        bt._check(L.bt_point_search_host(tree.handle, 1, hq_p, nq, hout_p, sp), "e2e")
+    e2e_t = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        bt._check(L.bt_point_search_host(tree.handle, 1, hq_p, nq, hout_p, sp), "e2e")
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(statistics.mean(e2e_t), dist, device)
+    e2e_ok = bool(np.array_equal(hout.numpy(), res))
+
+    # ---- roofline of the dominant kernel (the grouped search kernel) --------
+    kb = vb = 4
+    alg_bytes = nq * (kb + vb + 32) + hits * 32  # per launch, see DESIGN.md
+    search_s = statistics.mean(search_ms) / 1000.0
+    achieved = alg_bytes / search_s / 1e9
+    peak, peak_kind = measured_peak()
+    tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            qps_refc, qps_lb, sample = cpu_refc_qps(keys, vals, q, args.cpu_sample_log2)
+            cpu = {"value": qps_refc, "unit": "queries/s", "cores": os.cpu_count(),
+                   "kind": "port",
+                   "sample": f"{sample} queries of the batch, reference page tree (fanout 5000) "
+                             "restated in C, OpenMP all cores",
+                   "lower_bound_qps": qps_lb}
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (seeded)", "config": workload_desc(args),
+            "e2e": {"value": world * nq / e2e_s, "unit": "queries/s",
+                    "h2d_bytes_per_step": nq * kb, "d2h_bytes_per_step": nq * vb,
+                    "api": "bt_point_search_host (grouped), pinned host buffers",
+                    "matches_device_result": e2e_ok},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": None if tq is None else tq * nq,
+                         "kernel": "point_kernel (grouped batch)",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "kernel_ms": statistics.mean(search_ms)},
+            "cpu_baseline": cpu,
+            "clocks": clk,
+            "gpu_launches": int(launches),
+            "breakdown_ms": {"group": statistics.mean(group_ms),
+                             "search": statistics.mean(search_ms)},
+            "plain_basic": {"value": world * nq / (basic_ms / 1000.0), "unit": "queries/s",
+                            "ms_per_step": basic_ms},
+            "hit_fraction": hits / nq,
+            "checked_vs_oracle": checked,
+        }
+        print(json.dumps(line), flush=True)
+    tree.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

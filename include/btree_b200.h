@@ -1,0 +1,181 @@
+/*
+ * btree_b200.h -- C ABI of the B200 B+tree index engine.
+ *
+ * This is the engine's real interface: plain pointers, sizes and status
+ * codes, no C++ types.  It replaces the reference's C++ host API
+ * (BPTree.h:26-55, grouping.h:6-28, grouping2d.h:8-10, zOrder2d.h:8); the
+ * C++ compatibility shim with the reference's exact signatures is in
+ * btree_b200_compat.h and is implemented on top of these functions.
+ *
+ * Conventions (all functions):
+ *   - Every call returns a bt_status; nothing calls exit().  A thread-local
+ *     message with details is available from bt_last_error().
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default
+ *     stream).  Device-pointer calls are asynchronous on that stream unless
+ *     stated otherwise; host-pointer calls (suffix _host) return after the
+ *     results are in host memory.
+ *   - The caller keeps ownership of every buffer it passes.
+ *   - Results always come back in the caller's query order, also for the
+ *     grouped modes (the reference returns grouped order instead,
+ *     BPTreeExactSearch.cu:613,722).
+ *   - Keys are unsigned integers of 4 or 8 bytes, values of 4 or 8 bytes.
+ *     A point-search miss yields the all-ones value of the value width
+ *     (INVALID_DATA, BPTree.h:12, for 8-byte values).
+ *   - Duplicate keys are allowed.  A point search returns the value at the
+ *     first occurrence (std::lower_bound), a range search counts every
+ *     occurrence.
+ */
+#ifndef BTREE_B200_H
+#define BTREE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define BT_API __attribute__((visibility("default")))
+#else
+#define BT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bt_status {
+    BT_OK = 0,
+    BT_ERR_INVALID_ARGUMENT = 1, /* null pointer, bad width, bad mode, size limit */
+    BT_ERR_UNSORTED = 2,         /* build keys are not in ascending order */
+    BT_ERR_OUT_OF_MEMORY = 3,    /* device allocation failed */
+    BT_ERR_CUDA = 4,             /* a CUDA runtime call failed */
+    BT_ERR_CAPACITY = 5,         /* the caller's output buffer is too small */
+    BT_ERR_NOT_SUPPORTED = 6,    /* no sm_100 device, or feature not built */
+    BT_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
+    BT_ERR_INTERNAL = 8          /* a device-side consistency check failed */
+} bt_status;
+
+typedef enum bt_point_mode {
+    BT_POINT_BASIC = 0,  /* SearchingBTreeGPUOnlyOneState, BPTreeExactSearch.cu:409 */
+    BT_POINT_GROUPED = 1 /* SearchingBTreeGPUCombineStep, BPTreeExactSearch.cu:602 */
+} bt_point_mode;
+
+typedef enum bt_range_mode {
+    BT_RANGE_BASIC = 0,      /* SearchingBTreeGPURange, BtreeRangeSearch.cu:786 */
+    BT_RANGE_GROUPED_2D = 1, /* SearchingBTreeGPURangeWithGrouping, BtreeRangeSearch.cu:377 */
+    BT_RANGE_ZORDER = 2      /* SearchingBTreeGPURangeWithGroupingZorder, BtreeRangeSearch.cu:578 */
+} bt_range_mode;
+
+typedef struct bt_tree bt_tree;
+
+typedef struct bt_info {
+    uint64_t num_keys;
+    uint32_t key_bytes;
+    uint32_t value_bytes;
+    uint32_t num_levels;   /* separator levels above the leaf sectors */
+    uint32_t fanout;       /* separators per internal node (one 128-byte line) */
+    uint32_t leaf_keys;    /* keys per leaf sector (one 32-byte sector) */
+    uint32_t smem_levels;  /* top levels the search kernels stage in shared memory */
+    uint64_t device_bytes; /* HBM held by the tree */
+    uint64_t min_key;
+    uint64_t max_key;
+    int32_t device;
+    int32_t values_sorted; /* values ascend with keys (range IDs need no sort) */
+} bt_info;
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+BT_API int bt_version(void);
+/* Static string for a status code. */
+BT_API const char *bt_status_string(bt_status s);
+/* Details of the last failure on the calling thread ("" if none). */
+BT_API const char *bt_last_error(void);
+
+/*
+ * Bulk build from keys sorted ascending (device memory) and their values.
+ * Replaces genBPlusTree (BPTree.cu:127-306) together with the leaf plan of
+ * main.cu:126-129.  Unlike the reference, the inputs are not freed and are
+ * not referenced after the call returns (the tree keeps its own copy).
+ * Synchronizes `stream` (it reads back the sortedness check).
+ * n == 0 builds an empty tree (every search misses).
+ */
+BT_API bt_status bt_build(const void *d_sorted_keys, const void *d_values, uint64_t n,
+                   int key_bytes, int value_bytes, void *stream, bt_tree **out);
+
+/* Same, from host memory (pageable or pinned). */
+BT_API bt_status bt_build_host(const void *h_sorted_keys, const void *h_values, uint64_t n,
+                        int key_bytes, int value_bytes, void *stream, bt_tree **out);
+
+/* Free every device resource of a tree.  NULL is accepted. */
+BT_API bt_status bt_destroy(bt_tree *tree);
+
+BT_API bt_status bt_get_info(const bt_tree *tree, bt_info *info);
+
+/*
+ * Point search: d_out[i] = value of key d_queries[i], or all-ones on a miss.
+ * Replaces kernelSearchingNaiveOneStep (BPTreeExactSearch.cu:25, mode
+ * BASIC) and genGrouping + kernelSearchingKeyGroupTwoStep
+ * (grouping.cu:1677, BPTreeExactSearch.cu:207, mode GROUPED).
+ * Queries have key_bytes each, outputs value_bytes each; nq < 2^32.
+ */
+BT_API bt_status bt_point_search(const bt_tree *tree, int mode, const void *d_queries, uint64_t nq,
+                          void *d_out, void *stream);
+
+/* Same with host buffers; copies are pipelined with the search in chunks.
+ * Returns when h_out is filled. */
+BT_API bt_status bt_point_search_host(const bt_tree *tree, int mode, const void *h_queries,
+                               uint64_t nq, void *h_out, void *stream);
+
+/*
+ * The grouping step alone (genGrouping, grouping.cu:1677): writes the
+ * queries in grouped order to d_grouped and, for each grouped slot, the
+ * caller's index of that query to d_perm (u32).  The order is a stable
+ * partition by the top bits of the key, deterministic for a given tree.
+ */
+BT_API bt_status bt_group_queries(const bt_tree *tree, const void *d_queries, uint64_t nq,
+                           void *d_grouped, uint32_t *d_perm, void *stream);
+
+/*
+ * Search a batch already grouped by bt_group_queries: d_out[d_perm[i]] =
+ * value of d_grouped[i].  This is the search stage of BT_POINT_GROUPED on
+ * its own, for callers that group once and search repeatedly (and the
+ * kernel a benchmark times alone).  d_perm must be a permutation of 0..nq-1.
+ */
+BT_API bt_status bt_point_search_grouped_batch(const bt_tree *tree, const void *d_grouped,
+                                               const uint32_t *d_perm, uint64_t nq, void *d_out,
+                                               void *stream);
+
+/*
+ * Range count over inclusive intervals [d_lo[i], d_hi[i]]: d_counts[i] = number
+ * of keys k with lo <= k <= hi (0 when lo > hi).  Replaces
+ * kernelSearchingKeyRangeGroupStateTwo + kernelGenerateSearchResult
+ * (BtreeRangeSearch.cu:215,297) and their grouped twins (:33,:123), whose
+ * counts the reference never returns.  mode selects the query reordering
+ * (bt_range_mode); results do not depend on it.
+ */
+BT_API bt_status bt_range_count(const bt_tree *tree, int mode, const void *d_lo, const void *d_hi,
+                         uint64_t nq, uint64_t *d_counts, void *stream);
+
+/*
+ * Range search with hit IDs: counts as above, d_offsets = exclusive scan of
+ * the counts, and d_ids[d_offsets[i] .. + d_counts[i]) = the values of the
+ * hit keys of query i, sorted ascending.  *h_total receives the total hit
+ * count.  If it exceeds ids_capacity (in values) the call returns
+ * BT_ERR_CAPACITY with counts, offsets and *h_total filled and d_ids
+ * untouched.  Synchronizes `stream` (it reads the total back).
+ */
+BT_API bt_status bt_range_search(const bt_tree *tree, int mode, const void *d_lo, const void *d_hi,
+                          uint64_t nq, uint64_t *d_counts, uint64_t *d_offsets, void *d_ids,
+                          uint64_t ids_capacity, uint64_t *h_total, void *stream);
+
+/* Range count with host buffers (pipelined like bt_point_search_host). */
+BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *h_lo,
+                              const void *h_hi, uint64_t nq, uint64_t *h_counts,
+                              void *stream);
+
+/* Number of kernel launches this library has issued in this process (all
+ * devices, all threads).  Lets a caller count the device work behind a call. */
+BT_API uint64_t bt_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BTREE_B200_H */

@@ -1,0 +1,60 @@
+"""The oracle pinned against outputs of the reference implementation itself.
+
+tests/golden/reference_outputs.npz holds inputs and outputs of the
+reference's own kernels (compiled from its sources for sm_100a and run on a
+B200 by tests/golden/make_golden.py).  Here, on the CPU:
+  * the judge (lower_bound) reproduces the reference's basic point search;
+  * the literal restatement reproduces every reference output, including the
+    grouped point search and the off-by-one range counts.
+"""
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.npz")
+
+
+@pytest.fixture(scope="module")
+def g():
+    if not os.path.exists(GOLDEN):
+        pytest.skip("golden vectors not generated yet (tests/golden/make_golden.py on a GPU)")
+    return np.load(GOLDEN)
+
+
+def test_point_basic_pinned(g, orc):
+    k, v, q, out = g["pb_keys"], g["pb_vals"], g["pb_q"], g["pb_out"]
+    assert np.array_equal(orc.point_search(k, v, q), out)
+    t = orc.refc_build(k, v)
+    assert np.array_equal(t.point_basic(q), out)
+
+
+def test_point_grouped_pinned(g, orc):
+    k, q, gq, out = g["pg_keys"], g["pg_q"], g["pg_grouped_q"], g["pg_out"]
+    assert np.array_equal(np.sort(gq), np.sort(q)), "grouping lost or duplicated queries"
+    t = orc.refc_build(k, k)
+    assert np.array_equal(t.point_grouped(gq), out)
+    assert np.array_equal(orc.point_search(k, k, gq), out)
+
+
+def test_range_endpoints_and_counts_pinned(g, orc):
+    k, lo, hi = g["rg_keys"], g["rg_lo"], g["rg_hi"]
+    t = orc.refc_build(k, k)
+    assert np.array_equal(t.range_endpoint(lo), g["rg_ep_lo"])
+    assert np.array_equal(t.range_endpoint(hi), g["rg_ep_hi"])
+    c, rc = t.range_count(lo, hi)
+    assert rc == 0
+    assert np.array_equal(c, g["rg_count"])
+    # the judge is exact; the reference is 0-3 low
+    d = orc.range_count(k, lo, hi).astype(np.int64) - g["rg_count"].astype(np.int64)
+    assert d.min() >= 0 and d.max() <= 3
+
+
+@pytest.mark.parametrize("tag", ["r2d", "rz"])
+def test_grouped_range_counts_pinned(g, orc, tag):
+    k = g["rg_keys"]
+    lo, hi, cnt = g[tag + "_lo"], g[tag + "_hi"], g[tag + "_count"]
+    t = orc.refc_build(k, k)
+    c, rc = t.range_count(lo, hi, grouped=True)
+    assert rc == 0
+    assert np.array_equal(c, cnt)
