@@ -56,6 +56,8 @@ class bt_info(ctypes.Structure):
         ("max_key", ctypes.c_uint64),
         ("device", ctypes.c_int32),
         ("values_sorted", ctypes.c_int32),
+        ("lanes_per_query", ctypes.c_uint32),
+        ("queries_per_group", ctypes.c_uint32),
     ]
 
 
@@ -80,6 +82,7 @@ _PROTOS = {
     "bt_range_count_host": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
     "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
     "bt_kernel_launches": (ctypes.c_uint64, []),
+    "bt_set_search_config": (_I, [_P, _I, _I]),
 }
 
 
@@ -183,6 +186,15 @@ class Tree:
     @property
     def handle(self):
         return self._h
+
+    def set_search_config(self, lanes_per_query, queries_per_group):
+        """Search kernel shape (see bt_set_search_config); results unchanged."""
+        L = lib()
+        _check(L.bt_set_search_config(self._h, lanes_per_query, queries_per_group),
+               "bt_set_search_config")
+        _check(L.bt_get_info(self._h, ctypes.byref(self.info)), "bt_get_info")
+
+    SEARCH_CONFIGS = ((8, 2), (8, 4), (4, 2), (4, 4), (2, 2), (1, 2))
 
     # -- point search ---------------------------------------------------
     def point_search(self, queries, mode="basic", out=None, stream=None):

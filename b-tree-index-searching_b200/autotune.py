@@ -1,0 +1,85 @@
+"""Autotuner for the search kernels' shape.
+
+For a tree and a sample batch, times every supported (lanes per query,
+queries per lane group) configuration of the search kernels with CUDA events
+and keeps the fastest.  Results do not depend on the configuration (the tests
+check every one against the oracle), only speed does.  Decisions can be
+cached in a JSON file keyed by (keys, key width, value width, mode, batch
+size class), so a serving process tunes once per shape.
+
+The reference has no tuning: one thread per query, 1024-thread blocks,
+fanout fixed at PAGESIZE = 5000 (BPTree.h:8, BPTreeExactSearch.cu:31).  Here
+the node fanout is fixed by the 128-byte line (32 u32 / 16 u64 separators);
+what is tuned is how many lanes share a query and how many queries each lane
+group keeps in flight.
+"""
+import json
+import os
+import statistics
+
+SEARCH_CONFIGS = ((8, 2), (8, 4), (4, 2), (4, 4), (2, 2), (1, 2))
+
+
+def _key(tree, mode, nq):
+    cls = max(0, int(nq).bit_length() - 1)
+    return f"n{tree.info.num_keys}_k{tree.key_bytes}_v{tree.value_bytes}_{mode}_q2^{cls}"
+
+
+def _time(fn, stream, repeats):
+    import torch
+    fn()
+    fn()
+    ts = []
+    for _ in range(repeats):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.median(ts)
+
+
+def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, configs=SEARCH_CONFIGS):
+    """Pick and set the fastest search configuration for `tree` on this batch.
+
+    mode: "basic" / "grouped" (point search; `queries` a CUDA tensor), or
+    "range" (`queries` = lo, `hi` = hi).  Returns (lanes, slots, {cfg: ms}).
+    """
+    import torch
+    key = _key(tree, mode, len(queries))
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cached = json.load(f).get(key)
+        if cached:
+            tree.set_search_config(*cached["best"])
+            return cached["best"][0], cached["best"][1], cached["ms"]
+    stream = torch.cuda.current_stream(queries.device)
+    out = None
+    if mode in ("basic", "grouped"):
+        out = torch.empty(len(queries), dtype={4: torch.uint32, 8: torch.uint64}[tree.value_bytes],
+                          device=queries.device)
+        fn = lambda: tree.point_search(queries, mode=mode, out=out, stream=stream)  # noqa: E731
+    elif mode == "range":
+        out = torch.empty(len(queries), dtype=torch.uint64, device=queries.device)
+        fn = lambda: tree.range_count(queries, hi, out=out, stream=stream)  # noqa: E731
+    else:
+        raise ValueError(mode)
+    ms = {}
+    for g, i in configs:
+        tree.set_search_config(g, i)
+        ms[f"{g}x{i}"] = _time(fn, stream, repeats)
+    best = min(ms, key=ms.get)
+    g, i = (int(x) for x in best.split("x"))
+    tree.set_search_config(g, i)
+    if cache_path:
+        data = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                data = json.load(f)
+        data[key] = {"best": [g, i], "ms": ms}
+        os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
+        with open(cache_path, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+    return g, i, ms

@@ -1,11 +1,11 @@
-// Bulk build: sorted (key, value) arrays -> padded leaf sectors + separator
-// levels.  Replaces genBPlusTree (BPTree.cu:127-306): the reference copies
+// Bulk build: sorted (key, value) arrays -> leaf blocks + separator levels.  Replaces genBPlusTree (BPTree.cu:127-306): the reference copies
 // PAGESIZE pairs per leaf page (assignDataToLeaf, BPTree.cu:73-125) and builds
 // (child.max, child index) pages per level with a host-synchronized loop
 // (kernelMaxIntermidatePage, BPTree.cu:28-70, :218-243).  Here the leaf level
-// is the padded sorted array itself and each separator level is one strided
-// gather of the level below; nothing is pointer-linked, so the whole build is
-// a few streaming passes with no host round trip between levels.
+// is the sorted array itself, cut into 32-byte key sectors with their values
+// alongside, and each separator level is one strided gather of the level
+// below; nothing is pointer-linked, so the whole build is a few streaming
+// passes with no host round trip between levels.
 #include <algorithm>
 #include <cstring>
 
@@ -14,15 +14,16 @@
 namespace bt {
 namespace {
 
-// One thread per leaf position: copy + pad keys and values, check the
-// ascending order of keys (bit 0) and values (bit 1), and emit the bottom
-// separator level (the last key of every sector).
+// One thread per leaf position: copy keys and values into their leaf block
+// (all-ones keys pad the last block), check the ascending order of keys
+// (bit 0) and values (bit 1), and emit the bottom separator level (the last
+// key of every block).
 template <typename K, typename V>
 __global__ void __launch_bounds__(256)
 copy_pad_kernel(const K *__restrict__ keys, const V *__restrict__ vals, uint64_t n,
-                uint64_t n_pos, K *__restrict__ out_k, V *__restrict__ out_v,
-                K *__restrict__ bottom_sep, unsigned int *__restrict__ flags) {
-    constexpr int S = kSectorBytes / sizeof(K);
+                uint64_t n_pos, unsigned char *__restrict__ leaves, K *__restrict__ bottom_sep,
+                unsigned int *__restrict__ flags) {
+    using LG = LeafGeom<K, V>;
     unsigned int f = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_pos;
          i += (uint64_t)gridDim.x * blockDim.x) {
@@ -36,9 +37,12 @@ copy_pad_kernel(const K *__restrict__ keys, const V *__restrict__ vals, uint64_t
                 if (vals[i + 1] < v) f |= 2u;
             }
         }
-        out_k[i] = k;
-        out_v[i] = v;
-        if ((i % S) == S - 1) bottom_sep[i / S] = k;
+        const uint64_t b = i / LG::S;
+        const int j = (int)(i % LG::S);
+        unsigned char *blk = leaves + b * LG::BS;
+        reinterpret_cast<K *>(blk)[j] = k;
+        reinterpret_cast<V *>(blk + kSectorBytes)[j] = v;
+        if (j == LG::S - 1) bottom_sep[b] = k;
     }
     unsigned int w = __reduce_or_sync(0xffffffffu, f);
     if ((threadIdx.x & 31) == 0 && w) atomicOr(flags, w);
@@ -101,8 +105,9 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     }
     t->seps_elems = off;
 
-    BT_CUDA(cudaMalloc(&t->d_keys, n_pos * sizeof(K)));
-    BT_CUDA(cudaMalloc(&t->d_vals, n_pos * sizeof(V)));
+    const size_t leaf_bytes = t->n_sectors * (size_t)LeafGeom<K, V>::BS;
+    BT_CUDA(cudaMalloc(&t->d_leaves, leaf_bytes));
+    BT_CUDA(cudaMemsetAsync(t->d_leaves, 0, leaf_bytes, s));  // block padding bytes
     BT_CUDA(cudaMalloc(&t->d_seps, t->seps_elems * sizeof(K)));
     unsigned int *d_flags = nullptr;
     bt_status st = ws_alloc((void **)&d_flags, sizeof(unsigned int), s);
@@ -113,7 +118,7 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     K *bottom = seps + dt.lvl_off[L - 1];
     count_launch();
     copy_pad_kernel<K, V><<<grid_for(n_pos, 256), 256, 0, s>>>(
-        (const K *)d_keys, (const V *)d_vals, n, n_pos, (K *)t->d_keys, (V *)t->d_vals, bottom,
+        (const K *)d_keys, (const V *)d_vals, n, n_pos, (unsigned char *)t->d_leaves, bottom,
         d_flags);
     const uint64_t bottom_pad = t->lvl_nodes[L - 1] * F;
     if (bottom_pad > t->n_sectors) {
@@ -132,9 +137,11 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     unsigned int flags = 0;
     K kmin = 0, kmax = 0;
     BT_CUDA(cudaMemcpyAsync(&flags, d_flags, sizeof(flags), cudaMemcpyDeviceToHost, s));
-    BT_CUDA(cudaMemcpyAsync(&kmin, t->d_keys, sizeof(K), cudaMemcpyDeviceToHost, s));
-    BT_CUDA(cudaMemcpyAsync(&kmax, (const K *)t->d_keys + (n - 1), sizeof(K),
-                            cudaMemcpyDeviceToHost, s));
+    const unsigned char *lv = (const unsigned char *)t->d_leaves;
+    BT_CUDA(cudaMemcpyAsync(&kmin, lv, sizeof(K), cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaMemcpyAsync(&kmax,
+                            lv + ((n - 1) / S) * LeafGeom<K, V>::BS + ((n - 1) % S) * sizeof(K),
+                            sizeof(K), cudaMemcpyDeviceToHost, s));
     ws_free(d_flags, s);
     BT_CUDA(cudaStreamSynchronize(s));
     if (flags & 1u) return fail(BT_ERR_UNSORTED, "build keys are not sorted ascending");
@@ -142,8 +149,7 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     t->min_key = (uint64_t)kmin;
     t->max_key = (uint64_t)kmax;
 
-    dt.keys = t->d_keys;
-    dt.vals = t->d_vals;
+    dt.leaves = t->d_leaves;
     dt.seps = t->d_seps;
     dt.n = n;
     dt.max_key = t->max_key;
@@ -166,8 +172,7 @@ bt_status build_k(bt_tree *t, const void *dk, const void *dv, cudaStream_t s) {
 
 void free_tree(bt_tree *t) {
     if (!t) return;
-    if (t->d_keys) cudaFree(t->d_keys);
-    if (t->d_vals) cudaFree(t->d_vals);
+    if (t->d_leaves) cudaFree(t->d_leaves);
     if (t->d_seps) cudaFree(t->d_seps);
     delete t;
 }
@@ -188,7 +193,8 @@ bt_status bt_build(const void *d_sorted_keys, const void *d_values, uint64_t n, 
         return fail(BT_ERR_INVALID_ARGUMENT, "value_bytes must be 4 or 8");
     if (n > 0 && (!d_sorted_keys || !d_values))
         return fail(BT_ERR_INVALID_ARGUMENT, "keys or values pointer is NULL");
-    if (n >= (1ull << 40)) return fail(BT_ERR_INVALID_ARGUMENT, "n exceeds 2^40");
+    // leaf block and node indices are 32-bit in the search kernels
+    if (n >= (1ull << 34)) return fail(BT_ERR_INVALID_ARGUMENT, "n must be below 2^34");
     int dev = 0;
     BT_CUDA(cudaGetDevice(&dev));
     bt_status st = require_device(dev);
@@ -200,6 +206,7 @@ bt_status bt_build(const void *d_sorted_keys, const void *d_values, uint64_t n, 
     t->val_bytes = value_bytes;
     t->n = n;
     t->values_sorted = 1;
+    t->search_cfg = default_search_cfg(key_bytes);
     if (n > 0) {
         cudaStream_t s = (cudaStream_t)stream;
         st = key_bytes == 4 ? build_k<uint32_t>(t, d_sorted_keys, d_values, s)
@@ -246,6 +253,15 @@ bt_status bt_destroy(bt_tree *tree) {
     return BT_OK;
 }
 
+bt_status bt_set_search_config(bt_tree *t, int lanes_per_query, int queries_per_group) {
+    using namespace bt;
+    if (!t) return fail(BT_ERR_INVALID_ARGUMENT, "tree is NULL");
+    const int k = search_cfg_index(lanes_per_query, queries_per_group);
+    if (k < 0) return fail(BT_ERR_INVALID_ARGUMENT, "unsupported (lanes, slots) search configuration");
+    t->search_cfg = k;
+    return BT_OK;
+}
+
 bt_status bt_get_info(const bt_tree *t, bt_info *info) {
     using namespace bt;
     if (!t || !info) return fail(BT_ERR_INVALID_ARGUMENT, "tree or info is NULL");
@@ -257,12 +273,14 @@ bt_status bt_get_info(const bt_tree *t, bt_info *info) {
     info->fanout = (uint32_t)(kLineBytes / t->key_bytes);
     info->leaf_keys = (uint32_t)(kSectorBytes / t->key_bytes);
     info->smem_levels = (uint32_t)t->dev.smem_levels;
-    uint64_t npos = t->n_sectors * (kSectorBytes / t->key_bytes);
-    info->device_bytes = npos * t->key_bytes + npos * t->val_bytes + t->seps_elems * t->key_bytes;
+    info->device_bytes = t->n_sectors * (uint64_t)leaf_stride(t->key_bytes, t->val_bytes) +
+                         t->seps_elems * t->key_bytes;
     info->min_key = t->min_key;
     info->max_key = t->max_key;
     info->device = t->device;
     info->values_sorted = t->values_sorted;
+    info->lanes_per_query = (uint32_t)search_cfg_lanes(t->search_cfg);
+    info->queries_per_group = (uint32_t)search_cfg_slots(t->search_cfg);
     return BT_OK;
 }
 

@@ -361,18 +361,24 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
 
 // --------------------------------------------------------- range fill ----
 
-// One warp per query: ids[off .. off+cnt) = vals[lb .. lb+cnt).
-template <typename V>
+// One warp per query: ids[off .. off+cnt) = values of positions lb .. lb+cnt
+// (read from the leaf blocks, S values per block).
+template <typename K, typename V>
 __global__ void __launch_bounds__(256)
-range_fill_kernel(const V *__restrict__ vals, const uint64_t *__restrict__ lb,
+range_fill_kernel(const unsigned char *__restrict__ leaves, const uint64_t *__restrict__ lb,
                   const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off, uint64_t nq,
                   V *__restrict__ ids) {
+    using LG = LeafGeom<K, V>;
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < nq; i += nw) {
         const uint64_t c = cnt[i], l = lb[i], o = off[i];
-        for (uint64_t k = lane; k < c; k += 32) ids[o + k] = vals[l + k];
+        for (uint64_t k = lane; k < c; k += 32) {
+            const uint64_t p = l + k;
+            ids[o + k] = reinterpret_cast<const V *>(leaves + (p / LG::S) * LG::BS +
+                                                     kSectorBytes)[p % LG::S];
+        }
     }
 }
 
@@ -450,14 +456,19 @@ bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64
     if (nq == 0 || t->n == 0) return BT_OK;
     const unsigned grid = (unsigned)std::min<uint64_t>((nq + 7) / 8, (uint64_t)sm_count() * 8);
     count_launch();
-    if (t->val_bytes == 4)
-        range_fill_kernel<uint32_t><<<grid, 256, 0, s>>>((const uint32_t *)t->d_vals, d_lb,
-                                                         d_counts, d_offsets, nq,
-                                                         (uint32_t *)d_ids);
+    const unsigned char *lv = (const unsigned char *)t->d_leaves;
+    if (t->key_bytes == 4 && t->val_bytes == 4)
+        range_fill_kernel<uint32_t, uint32_t><<<grid, 256, 0, s>>>(lv, d_lb, d_counts, d_offsets,
+                                                                   nq, (uint32_t *)d_ids);
+    else if (t->key_bytes == 4)
+        range_fill_kernel<uint32_t, uint64_t><<<grid, 256, 0, s>>>(lv, d_lb, d_counts, d_offsets,
+                                                                   nq, (uint64_t *)d_ids);
+    else if (t->val_bytes == 4)
+        range_fill_kernel<uint64_t, uint32_t><<<grid, 256, 0, s>>>(lv, d_lb, d_counts, d_offsets,
+                                                                   nq, (uint32_t *)d_ids);
     else
-        range_fill_kernel<uint64_t><<<grid, 256, 0, s>>>((const uint64_t *)t->d_vals, d_lb,
-                                                         d_counts, d_offsets, nq,
-                                                         (uint64_t *)d_ids);
+        range_fill_kernel<uint64_t, uint64_t><<<grid, 256, 0, s>>>(lv, d_lb, d_counts, d_offsets,
+                                                                   nq, (uint64_t *)d_ids);
     BT_CUDA(cudaGetLastError());
     if (t->values_sorted) return BT_OK;
     unsigned int *flag = nullptr;

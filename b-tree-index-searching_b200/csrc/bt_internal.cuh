@@ -2,18 +2,20 @@
 //
 // Tree layout in HBM (one allocation per array, 256-byte aligned):
 //
-//   keys   K[n_sectors * S]   the sorted keys, padded with the all-ones key;
-//                             S = 32 / sizeof(key) keys form one 32-byte
-//                             DRAM sector ("leaf sector").
-//   vals   V[n_sectors * S]   the values, same positions (struct of arrays).
-//   seps   separator levels, stored root first.  Level t holds nodes of
-//                             F = 128 / sizeof(key) separators (one 128-byte
-//                             line).  A separator is the maximum key of the
-//                             node (or leaf sector) below it, as in the
-//                             reference's internal pages (BPTree.cu:54-55).
+//   leaves  the sorted keys and their values in leaf blocks.  Block b holds
+//           keys b*S .. b*S+S-1 (S = 32 / sizeof(key): one 32-byte DRAM
+//           sector) followed by the same positions' values, the block padded
+//           to a power of two (64 bytes, or 128 for 4-byte keys with 8-byte
+//           values).  A point-search hit needs one block: its key sector and
+//           value sector come in the same 64-byte DRAM access.  Unused key
+//           slots of the last block hold the all-ones key.
+//   seps    separator levels, stored root first.  Level t holds nodes of
+//           F = 128 / sizeof(key) separators (one 128-byte line).  A
+//           separator is the maximum key of the node (or leaf block) below
+//           it, as in the reference's internal pages (BPTree.cu:54-55).
 //
 // Child j of node i at level t is node i*F + j of level t+1; the children of
-// the bottom level are leaf sectors.  No pointers are stored.  A search for
+// the bottom level are leaf blocks.  No pointers are stored.  A search for
 // q <= max_key takes, at every level, the first separator >= q (lower bound)
 // or > q (upper bound); padding separators are all-ones and never win.
 #pragma once
@@ -36,9 +38,21 @@ constexpr int kMaxLevels = 24;
 // Shared-memory budget for the staged top levels of one search CTA.
 constexpr size_t kSmemTopBudget = 40 * 1024;
 
+// Leaf block geometry for key type K and value type V.
+template <typename K, typename V>
+struct LeafGeom {
+    static constexpr int S = kSectorBytes / (int)sizeof(K);  // keys per block
+    static constexpr int VB = S * (int)sizeof(V);             // value bytes per block
+    static constexpr int BS = (kSectorBytes + VB) <= 64 ? 64 : 128;  // block stride
+};
+
+inline int leaf_stride(int key_bytes, int val_bytes) {
+    const int vb = (kSectorBytes / key_bytes) * val_bytes;
+    return (kSectorBytes + vb) <= 64 ? 64 : 128;
+}
+
 struct DevTree {
-    const void *keys;
-    const void *vals;
+    const void *leaves;
     const void *seps;
     uint64_t n;
     uint64_t max_key;
@@ -57,14 +71,14 @@ struct bt_tree {
     int val_bytes;
     uint64_t n;
     uint64_t n_sectors;
-    void *d_keys;
-    void *d_vals;
+    void *d_leaves;
     void *d_seps;
     uint64_t seps_elems;
     uint64_t lvl_nodes[bt::kMaxLevels];
     uint64_t lvl_entries[bt::kMaxLevels];
     uint64_t min_key, max_key;
     int values_sorted;
+    int search_cfg;  // index into the search kernels' (lanes, slots) table
     bt::DevTree dev;
 };
 
@@ -120,6 +134,13 @@ bt_status launch_scan_u64(const uint64_t *d_in, uint64_t *d_out, uint64_t n, uin
                           cudaStream_t s);
 bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
                             const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
+
+// (lanes per query, queries per group) -> index of the search configuration
+// table in bt_search.cu, or -1.
+int search_cfg_index(int lanes, int slots);
+int default_search_cfg(int key_bytes);
+int search_cfg_lanes(int cfg);
+int search_cfg_slots(int cfg);
 
 // Partition kinds for launch_partition.
 enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2 };

@@ -12,15 +12,38 @@
 //
 // Both kernels are persistent (grid = SMs x resident CTAs), stage the top
 // separator levels into shared memory once per CTA, then loop over warp tiles.
-// The leaf stage loads the query's key sector and, speculatively, the value
-// sector of the same positions in parallel (one 32-byte DRAM sector each), so
-// a hit costs one dependent HBM round trip instead of two.
+// The leaf stage loads the whole leaf block of the query -- key sector and
+// value sector side by side, one 64-byte DRAM access -- with its chunks
+// spread over the group's lanes, so a hit costs one HBM round trip.
 #include <map>
 #include <mutex>
 
 #include "bt_search.cuh"
 
 namespace bt {
+
+// Lanes per query (G) and queries in flight per group (I) of the search
+// kernels; set per tree by bt_set_search_config / the autotuner.
+struct SearchCfg {
+    int g, i;
+};
+constexpr SearchCfg kSearchCfgs[] = {{8, 2}, {8, 4}, {4, 2}, {4, 4}, {2, 2}, {1, 2}};
+constexpr int kNumSearchCfgs = sizeof(kSearchCfgs) / sizeof(kSearchCfgs[0]);
+
+int search_cfg_index(int g, int i) {
+    for (int k = 0; k < kNumSearchCfgs; k++)
+        if (kSearchCfgs[k].g == g && kSearchCfgs[k].i == i) return k;
+    return -1;
+}
+
+int search_cfg_lanes(int cfg) { return kSearchCfgs[cfg].g; }
+int search_cfg_slots(int cfg) { return kSearchCfgs[cfg].i; }
+
+int default_search_cfg(int key_bytes) {
+    (void)key_bytes;
+    return search_cfg_index(8, 2);
+}
+
 namespace {
 
 constexpr int kThreads = 512;
@@ -34,68 +57,90 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     stage_top<K>(s_top, t);
     __syncthreads();
 
-    constexpr int S = kSectorBytes / (int)sizeof(K);
-    constexpr int LL = S >= G ? G : S;  // lanes holding part of the leaf sector
-    constexpr int LPL = S / LL;         // keys per such lane
-    constexpr int QPW = 32 / G;         // queries per warp and slot
+    using LG = LeafGeom<K, V>;
+    using LS = LeafStage<K, V, G>;
+    constexpr int QPW = 32 / G;  // queries per warp and slot
     constexpr int TILE = QPW * I;
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int gl = lane % G;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const K tmax = (K)t.max_key;
-    const K *gk = static_cast<const K *>(t.keys);
-    const V *gv = static_cast<const V *>(t.vals);
-    const bool act = gl < LL;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
 
     for (uint64_t base = warp * TILE; base < nq; base += nwarps * TILE) {
         K qv[I], qe[I];
         bool up[I];
-        uint64_t node[I];
-        bool valid[I];
+        uint32_t node[I];
 #pragma unroll
         for (int s = 0; s < I; s++) {
             const uint64_t qi = base + (uint64_t)s * QPW + grp;
-            valid[s] = qi < nq;
-            qv[s] = valid[s] ? q[qi] : (K)0;
+            qv[s] = qi < nq ? q[qi] : (K)0;
             qe[s] = qv[s] < tmax ? qv[s] : tmax;
             up[s] = false;
         }
         descend<K, G, I>(t, s_top, qe, up, node, grp, gl);
 
-        K kk[I][LPL];
-        V vv[I][LPL];
+        // the leaf block: key chunks then value chunks, chunk c on lane c % G
+        uint32_t ch[I][LS::CPL][4];
 #pragma unroll
         for (int s = 0; s < I; s++) {
+            const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
 #pragma unroll
-            for (int j = 0; j < LPL; j++) {
-                kk[s][j] = 0;
-                vv[s][j] = 0;
-            }
-            if (act) {
-                const uint64_t p = node[s] * S + (uint64_t)gl * LPL;
-                load_stream<K, LPL>(gk + p, kk[s]);
-                load_stream<V, LPL>(gv + p, vv[s]);
+            for (int j = 0; j < LS::CPL; j++) {
+                const int c = gl + j * G;
+                if (c < LS::NC) {
+                    const uint4 x = load_stream16(blk + (c < LS::NKC ? c * 16 : kSectorBytes + (c - LS::NKC) * 16));
+                    ch[s][j][0] = x.x;
+                    ch[s][j][1] = x.y;
+                    ch[s][j][2] = x.z;
+                    ch[s][j][3] = x.w;
+                }
             }
         }
 #pragma unroll
         for (int s = 0; s < I; s++) {
-            const int cnt = act ? count_below<K, LPL>(kk[s], qe[s], false) : 0;
-            int pos = group_count<G, LL, LPL>(cnt, act, grp);
-            pos = pos < S ? pos : S - 1;
-            if (gl == pos / LPL && valid[s]) {
-                const int j0 = pos % LPL;
-                K key = kk[s][0];
-                V val = vv[s][0];
+            int cnt = 0;
+            bool eq = false;
 #pragma unroll
-                for (int j = 1; j < LPL; j++)
-                    if (j == j0) {
-                        key = kk[s][j];
-                        val = vv[s][j];
+            for (int j = 0; j < LS::KCPL; j++) {
+                if (gl + j * G < LS::NKC) {
+                    cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], false);
+#pragma unroll
+                    for (int k = 0; k < LS::KPC; k++) eq |= key_at<K>(ch[s][j], k) == qv[s];
+                }
+            }
+            int pos;
+            bool found;
+            if constexpr (G == 1) {
+                pos = cnt;
+                found = eq;
+            } else {
+                pos = __shfl_sync(0xffffffffu, cnt, grp * G) + __shfl_sync(0xffffffffu, cnt, grp * G + 1);
+                found = (__ballot_sync(0xffffffffu, eq) & gmask) != 0;
+            }
+            found = found && qv[s] <= tmax;  // padding keys are all-ones
+            const uint64_t qi = base + (uint64_t)s * QPW + grp;
+            pos = pos < LG::S ? pos : LG::S - 1;
+            const int vc = LS::NKC + pos / LS::VPC;  // chunk holding the value
+            if (gl == vc % G && qi < nq) {
+                V val = 0;
+#pragma unroll
+                for (int j = 0; j < LS::CPL; j++) {
+                    if (j == vc / G) {
+                        const int w = (pos % LS::VPC) * (int)(sizeof(V) / 4);
+                        if constexpr (sizeof(V) == 4) {
+#pragma unroll
+                            for (int k = 0; k < 4; k++)
+                                if (k == w) val = ch[s][j][k];
+                        } else {
+                            val = w == 0 ? (((uint64_t)ch[s][j][1] << 32) | ch[s][j][0])
+                                         : (((uint64_t)ch[s][j][3] << 32) | ch[s][j][2]);
+                        }
                     }
-                const bool found = qv[s] <= tmax && key == qv[s];
-                const uint64_t qi = base + (uint64_t)s * QPW + grp;
+                }
                 const uint64_t dst = PERM ? (uint64_t)perm[qi] : qi;
                 out[dst] = found ? val : key_max<V>();
             }
@@ -105,7 +150,7 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
 
 // Lower bound of lo and upper bound of hi for QG queries per group (2*QG
 // descents in flight).  counts[i] = ub - lb (0 if lo > hi); lb_out[i] = lb.
-template <typename K, int G, int QG, bool PERM>
+template <typename K, typename V, int G, int QG, bool PERM>
 __global__ void __launch_bounds__(kThreads)
 bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
               const K *__restrict__ hi, const uint32_t *__restrict__ perm, uint64_t nq,
@@ -115,10 +160,9 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
     stage_top<K>(s_top, t);
     __syncthreads();
 
+    using LG = LeafGeom<K, V>;
+    using LS = LeafStage<K, V, G>;
     constexpr int I = 2 * QG;
-    constexpr int S = kSectorBytes / (int)sizeof(K);
-    constexpr int LL = S >= G ? G : S;
-    constexpr int LPL = S / LL;
     constexpr int QPW = 32 / G;
     constexpr int TILE = QPW * QG;
     const int lane = threadIdx.x & 31;
@@ -127,19 +171,18 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const K tmax = (K)t.max_key;
-    const K *gk = static_cast<const K *>(t.keys);
-    const bool act = gl < LL;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
 
     for (uint64_t base = warp * TILE; base < nq; base += nwarps * TILE) {
         K a[QG], b[QG], qe[I];
-        bool up[I], valid[QG];
-        uint64_t node[I];
+        bool up[I];
+        uint32_t node[I];
 #pragma unroll
         for (int j = 0; j < QG; j++) {
             const uint64_t qi = base + (uint64_t)j * QPW + grp;
-            valid[j] = qi < nq;
-            a[j] = valid[j] ? lo[qi] : (K)0;
-            b[j] = valid[j] ? hi[qi] : (K)0;
+            const bool v = qi < nq;
+            a[j] = v ? lo[qi] : (K)0;
+            b[j] = v ? hi[qi] : (K)0;
             // lower bound of a: a > max gives n (walk on max instead)
             qe[2 * j] = a[j] <= tmax ? a[j] : tmax;
             up[2 * j] = false;
@@ -148,23 +191,42 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
             up[2 * j + 1] = b[j] < tmax;
         }
         descend<K, G, I>(t, s_top, qe, up, node, grp, gl);
-        K kk[I][LPL];
+        uint32_t ch[I][LS::KCPL][4];
 #pragma unroll
         for (int s = 0; s < I; s++) {
+            const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
 #pragma unroll
-            for (int j = 0; j < LPL; j++) kk[s][j] = 0;
-            if (act) load_stream<K, LPL>(gk + node[s] * S + (uint64_t)gl * LPL, kk[s]);
+            for (int j = 0; j < LS::KCPL; j++) {
+                const int c = gl + j * G;
+                if (c < LS::NKC) {
+                    const uint4 x = load_stream16(blk + c * 16);
+                    ch[s][j][0] = x.x;
+                    ch[s][j][1] = x.y;
+                    ch[s][j][2] = x.z;
+                    ch[s][j][3] = x.w;
+                }
+            }
         }
 #pragma unroll
         for (int j = 0; j < QG; j++) {
-            int c0 = act ? count_below<K, LPL>(kk[2 * j], qe[2 * j], false) : 0;
-            int c1 = act ? count_below<K, LPL>(kk[2 * j + 1], qe[2 * j + 1], up[2 * j + 1]) : 0;
-            const int p0 = group_count<G, LL, LPL>(c0, act, grp);
-            const int p1 = group_count<G, LL, LPL>(c1, act, grp);
-            if (gl == 0 && valid[j]) {
-                const uint64_t lb = a[j] <= tmax ? node[2 * j] * S + (uint64_t)p0 : t.n;
-                const uint64_t ub = b[j] < tmax ? node[2 * j + 1] * S + (uint64_t)p1 : t.n;
-                const uint64_t qi = base + (uint64_t)j * QPW + grp;
+            int pos[2];
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int s = 2 * j + e;
+                int cnt = 0;
+#pragma unroll
+                for (int k = 0; k < LS::KCPL; k++)
+                    if (gl + k * G < LS::NKC) cnt += count_below<K, LS::KPC>(ch[s][k], qe[s], up[s]);
+                if constexpr (G == 1)
+                    pos[e] = cnt;
+                else
+                    pos[e] = __shfl_sync(0xffffffffu, cnt, grp * G) +
+                             __shfl_sync(0xffffffffu, cnt, grp * G + 1);
+            }
+            const uint64_t qi = base + (uint64_t)j * QPW + grp;
+            if (gl == 0 && qi < nq) {
+                const uint64_t lb = a[j] <= tmax ? (uint64_t)node[2 * j] * LG::S + pos[0] : t.n;
+                const uint64_t ub = b[j] < tmax ? (uint64_t)node[2 * j + 1] * LG::S + pos[1] : t.n;
                 const uint64_t dst = PERM ? (uint64_t)perm[qi] : qi;
                 counts[dst] = (a[j] <= b[j] && ub > lb) ? ub - lb : 0;
                 if (lb_out) lb_out[dst] = lb;
@@ -205,12 +267,9 @@ unsigned persistent_grid(const void *fn, size_t smem, uint64_t work_items, uint6
     return (unsigned)(want < 1 ? 1 : want);
 }
 
-template <typename K, typename V, bool PERM>
-bt_status point_dispatch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
-                         void *d_out, cudaStream_t s) {
-    // Lanes per query and queries in flight per group (see bt_search.cuh).
-    constexpr int G = 8;
-    constexpr int I = 2;
+template <typename K, typename V, int G, int I, bool PERM>
+bt_status point_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
+                       void *d_out, cudaStream_t s) {
     auto fn = point_kernel<K, V, G, I, PERM>;
     const size_t smem = (size_t)t->dev.smem_elems * sizeof(K);
     const unsigned grid = persistent_grid((const void *)fn, smem, nq, (kThreads / 32) * (32 / G) * I);
@@ -220,13 +279,24 @@ bt_status point_dispatch(const bt_tree *t, const void *d_q, const uint32_t *d_pe
     return BT_OK;
 }
 
-template <typename K, bool PERM>
-bt_status bounds_dispatch(const bt_tree *t, const void *d_lo, const void *d_hi,
-                          const uint32_t *d_perm, uint64_t nq, uint64_t *d_counts,
-                          uint64_t *d_lb, cudaStream_t s) {
-    constexpr int G = 8;
-    constexpr int QG = 1;
-    auto fn = bounds_kernel<K, G, QG, PERM>;
+template <typename K, typename V, bool PERM>
+bt_status point_cfg(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
+                    void *d_out, cudaStream_t s) {
+    switch (t->search_cfg) {
+        case 0: return point_launch<K, V, 8, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 1: return point_launch<K, V, 8, 4, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 2: return point_launch<K, V, 4, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 3: return point_launch<K, V, 4, 4, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 4: return point_launch<K, V, 2, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+        default: return point_launch<K, V, 1, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+    }
+}
+
+template <typename K, typename V, int G, int QG, bool PERM>
+bt_status bounds_launch(const bt_tree *t, const void *d_lo, const void *d_hi,
+                        const uint32_t *d_perm, uint64_t nq, uint64_t *d_counts, uint64_t *d_lb,
+                        cudaStream_t s) {
+    auto fn = bounds_kernel<K, V, G, QG, PERM>;
     const size_t smem = (size_t)t->dev.smem_elems * sizeof(K);
     const unsigned grid = persistent_grid((const void *)fn, smem, nq, (kThreads / 32) * (32 / G) * QG);
     count_launch();
@@ -234,6 +304,42 @@ bt_status bounds_dispatch(const bt_tree *t, const void *d_lo, const void *d_hi,
                                     d_lb);
     BT_CUDA(cudaGetLastError());
     return BT_OK;
+}
+
+template <typename K, typename V, bool PERM>
+bt_status bounds_cfg(const bt_tree *t, const void *d_lo, const void *d_hi, const uint32_t *d_perm,
+                     uint64_t nq, uint64_t *d_counts, uint64_t *d_lb, cudaStream_t s) {
+    // two descents per range query: half the point configuration's slots
+    switch (t->search_cfg) {
+        case 0: return bounds_launch<K, V, 8, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+        case 1: return bounds_launch<K, V, 8, 2, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+        case 2: return bounds_launch<K, V, 4, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+        case 3: return bounds_launch<K, V, 4, 2, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+        case 4: return bounds_launch<K, V, 2, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+        default: return bounds_launch<K, V, 1, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+    }
+}
+
+template <bool PERM>
+bt_status point_types(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
+                      void *d_out, cudaStream_t s) {
+    if (t->key_bytes == 4)
+        return t->val_bytes == 4 ? point_cfg<uint32_t, uint32_t, PERM>(t, d_q, d_perm, nq, d_out, s)
+                                 : point_cfg<uint32_t, uint64_t, PERM>(t, d_q, d_perm, nq, d_out, s);
+    return t->val_bytes == 4 ? point_cfg<uint64_t, uint32_t, PERM>(t, d_q, d_perm, nq, d_out, s)
+                             : point_cfg<uint64_t, uint64_t, PERM>(t, d_q, d_perm, nq, d_out, s);
+}
+
+template <bool PERM>
+bt_status bounds_types(const bt_tree *t, const void *d_lo, const void *d_hi, const uint32_t *d_perm,
+                       uint64_t nq, uint64_t *d_counts, uint64_t *d_lb, cudaStream_t s) {
+    if (t->key_bytes == 4)
+        return t->val_bytes == 4
+                   ? bounds_cfg<uint32_t, uint32_t, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s)
+                   : bounds_cfg<uint32_t, uint64_t, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+    return t->val_bytes == 4
+               ? bounds_cfg<uint64_t, uint32_t, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s)
+               : bounds_cfg<uint64_t, uint64_t, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
 }
 
 }  // namespace
@@ -251,19 +357,8 @@ bt_status launch_point_search(const bt_tree *t, const void *d_q, const uint32_t 
         BT_CUDA(cudaGetLastError());
         return BT_OK;
     }
-    const bool perm = d_perm != nullptr;
-    if (t->key_bytes == 4) {
-        if (t->val_bytes == 4)
-            return perm ? point_dispatch<uint32_t, uint32_t, true>(t, d_q, d_perm, nq, d_out, s)
-                        : point_dispatch<uint32_t, uint32_t, false>(t, d_q, d_perm, nq, d_out, s);
-        return perm ? point_dispatch<uint32_t, uint64_t, true>(t, d_q, d_perm, nq, d_out, s)
-                    : point_dispatch<uint32_t, uint64_t, false>(t, d_q, d_perm, nq, d_out, s);
-    }
-    if (t->val_bytes == 4)
-        return perm ? point_dispatch<uint64_t, uint32_t, true>(t, d_q, d_perm, nq, d_out, s)
-                    : point_dispatch<uint64_t, uint32_t, false>(t, d_q, d_perm, nq, d_out, s);
-    return perm ? point_dispatch<uint64_t, uint64_t, true>(t, d_q, d_perm, nq, d_out, s)
-                : point_dispatch<uint64_t, uint64_t, false>(t, d_q, d_perm, nq, d_out, s);
+    return d_perm ? point_types<true>(t, d_q, d_perm, nq, d_out, s)
+                  : point_types<false>(t, d_q, d_perm, nq, d_out, s);
 }
 
 bt_status launch_bounds(const bt_tree *t, const void *d_lo, const void *d_hi,
@@ -281,12 +376,8 @@ bt_status launch_bounds(const bt_tree *t, const void *d_lo, const void *d_hi,
         BT_CUDA(cudaGetLastError());
         return BT_OK;
     }
-    const bool perm = d_perm != nullptr;
-    if (t->key_bytes == 4)
-        return perm ? bounds_dispatch<uint32_t, true>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s)
-                    : bounds_dispatch<uint32_t, false>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
-    return perm ? bounds_dispatch<uint64_t, true>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s)
-                : bounds_dispatch<uint64_t, false>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+    return d_perm ? bounds_types<true>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s)
+                  : bounds_types<false>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
 }
 
 }  // namespace bt

@@ -1,14 +1,16 @@
 // Device-side descent shared by the point, range and forest kernels.
 //
 // A query is served by a group of G lanes of one warp.  At an internal level
-// the group reads the node's 128-byte line with one 16-byte vector load per
-// lane (F/G separators each), counts the separators below the query, and
-// combines the per-lane counts with one warp ballot and one shuffle: because
-// the line is sorted, the lanes whose whole chunk is below the query form a
-// prefix, so count = KPL * (#full lanes) + (count of the first non-full
-// lane).  The child index is node*F + count.  Each group works on I queries
-// at once (independent dependency chains) so that several line loads are in
-// flight per group.
+// the group reads the node's 128-byte line with 16-byte vector loads (F/G
+// separators per lane), counts the separators below the query, and combines
+// the per-lane counts with one warp ballot and one shuffle: because the line
+// is sorted, the lanes whose whole chunk is below the query form a prefix,
+// so count = KPL * (#full lanes) + (count of the first non-full lane).  The
+// child index is node*F + count.  Each group works on I queries at once
+// (independent dependency chains), so several line loads are in flight per
+// group.  The top levels are read from shared memory, the rest from global
+// memory (L2-resident in practice), in two separate loops so each uses its
+// native load instruction.
 //
 // The reference walks 80 KB pages by scalar binary search, one thread per
 // query, about 13 dependent 8-byte loads per level plus a leafFlag load on
@@ -20,71 +22,62 @@
 
 namespace bt {
 
-template <int BYTES>
-struct VecOf;
-template <>
-struct VecOf<4> { using T = uint32_t; };
-template <>
-struct VecOf<8> { using T = uint2; };
-template <>
-struct VecOf<16> { using T = uint4; };
-
-// Loads NK consecutive keys (NK*sizeof(K) in {4, 8, 16, 32} bytes, aligned).
-template <typename K, int NK>
-__device__ __forceinline__ void load_keys(const K *p, K (&v)[NK]) {
-    constexpr int B = NK * (int)sizeof(K);
-    if constexpr (B <= 16) {
-        using VT = typename VecOf<B>::T;
-        VT x = *reinterpret_cast<const VT *>(p);
-        memcpy(v, &x, B);
+// Loads NB bytes (4, 8, or a multiple of 16; aligned) from p into v.
+template <int NB>
+__device__ __forceinline__ void load_bytes(const void *p, uint32_t (&v)[NB / 4]) {
+    if constexpr (NB == 4) {
+        v[0] = *reinterpret_cast<const uint32_t *>(p);
+    } else if constexpr (NB == 8) {
+        uint2 x = *reinterpret_cast<const uint2 *>(p);
+        v[0] = x.x;
+        v[1] = x.y;
     } else {
-        static_assert(B % 16 == 0, "chunk must be a multiple of 16 bytes");
+        static_assert(NB % 16 == 0, "chunk must be 4, 8 or a multiple of 16 bytes");
 #pragma unroll
-        for (int i = 0; i < B / 16; i++) {
+        for (int i = 0; i < NB / 16; i++) {
             uint4 x = reinterpret_cast<const uint4 *>(p)[i];
-            memcpy(reinterpret_cast<char *>(v) + 16 * i, &x, 16);
+            v[4 * i] = x.x;
+            v[4 * i + 1] = x.y;
+            v[4 * i + 2] = x.z;
+            v[4 * i + 3] = x.w;
         }
     }
 }
 
-// Same for data in HBM that is touched once per query: read-only path, no L1
-// allocation (keeps L1 for the separator lines).
-template <typename T, int NK>
-__device__ __forceinline__ void load_stream(const T *p, T (&v)[NK]) {
-    constexpr int B = NK * (int)sizeof(T);
-    if constexpr (B == 4) {
-        uint32_t x;
-        asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(x) : "l"(p));
-        memcpy(v, &x, 4);
-    } else if constexpr (B == 8) {
-        uint2 x;
-        asm volatile("ld.global.nc.L1::no_allocate.v2.b32 {%0,%1}, [%2];"
-                     : "=r"(x.x), "=r"(x.y) : "l"(p));
-        memcpy(v, &x, 8);
+// 16-byte load of data touched once per query (leaf blocks): read-only path,
+// no L1 allocation, so L1 keeps the separator lines.
+__device__ __forceinline__ uint4 load_stream16(const void *p) {
+    uint4 x;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(x.x), "=r"(x.y), "=r"(x.z), "=r"(x.w)
+                 : "l"(p));
+    return x;
+}
+
+template <typename K>
+__device__ __forceinline__ K key_at(const uint32_t *w, int i) {
+    if constexpr (sizeof(K) == 4) {
+        return w[i];
     } else {
-        static_assert(B % 16 == 0, "chunk must be 4, 8 or a multiple of 16 bytes");
-#pragma unroll
-        for (int i = 0; i < B / 16; i++) {
-            uint4 x;
-            asm volatile("ld.global.nc.L1::no_allocate.v4.b32 {%0,%1,%2,%3}, [%4];"
-                         : "=r"(x.x), "=r"(x.y), "=r"(x.z), "=r"(x.w)
-                         : "l"(reinterpret_cast<const char *>(p) + 16 * i));
-            memcpy(reinterpret_cast<char *>(v) + 16 * i, &x, 16);
-        }
+        return ((uint64_t)w[2 * i + 1] << 32) | w[2 * i];
     }
 }
 
-// Number of keys in v below q (upper == false) or not above q (upper == true).
+// Keys among the NK packed in w that are below q (or not above q, upper).
 template <typename K, int NK>
-__device__ __forceinline__ int count_below(const K (&v)[NK], K q, bool upper) {
+__device__ __forceinline__ int count_below(const uint32_t *w, K q, bool upper) {
     int c = 0;
 #pragma unroll
-    for (int i = 0; i < NK; i++) c += upper ? (v[i] <= q) : (v[i] < q);
+    for (int i = 0; i < NK; i++) {
+        const K k = key_at<K>(w, i);
+        c += upper ? (k <= q) : (k < q);
+    }
     return c;
 }
 
 // Combine per-lane counts of a sorted chunk spread over the first ACT lanes
-// of a G-lane group (each lane holds NK keys).  All 32 lanes must call it.
+// of a G-lane group (each lane holds NK keys).  All 32 lanes must call it;
+// every lane of the group receives the result.
 template <int G, int ACT, int NK>
 __device__ __forceinline__ int group_count(int cnt, bool active, int grp) {
     if constexpr (G == 1) {
@@ -99,29 +92,38 @@ __device__ __forceinline__ int group_count(int cnt, bool active, int grp) {
     }
 }
 
-// Walks the separator levels for I queries per group.  qe[s] must satisfy
-// qe[s] <= max_key (lower) or qe[s] < max_key (upper) for the walk to stay on
-// real separators.  On return node[s] is the leaf sector index.
+// One level for I queries: node[s] <- node[s]*F + (separators of the node
+// below qe[s]).
+template <typename K, int G, int I>
+__device__ __forceinline__ void level_step(const K *__restrict__ lp, const K (&qe)[I],
+                                           const bool (&upper)[I], uint32_t (&node)[I], int grp,
+                                           int gl) {
+    constexpr int F = kLineBytes / (int)sizeof(K);
+    constexpr int KPL = F / G;
+    constexpr int NB = KPL * (int)sizeof(K);
+    uint32_t c[I][NB / 4];
+#pragma unroll
+    for (int s = 0; s < I; s++) load_bytes<NB>(lp + (size_t)node[s] * F + gl * KPL, c[s]);
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        const int cnt = count_below<K, KPL>(c[s], qe[s], upper[s]);
+        node[s] = node[s] * F + group_count<G, G, KPL>(cnt, true, grp);
+    }
+}
+
+// Walks all separator levels.  qe[s] must satisfy qe[s] <= max_key (lower
+// bound) or qe[s] < max_key (upper bound) for the walk to stay on real
+// separators.  On return node[s] is the leaf block index.
 template <typename K, int G, int I>
 __device__ __forceinline__ void descend(const DevTree &t, const K *__restrict__ s_top,
                                         const K (&qe)[I], const bool (&upper)[I],
-                                        uint64_t (&node)[I], int grp, int gl) {
-    constexpr int F = kLineBytes / (int)sizeof(K);
-    constexpr int KPL = F / G;
-    const K *gseps = static_cast<const K *>(t.seps);
+                                        uint32_t (&node)[I], int grp, int gl) {
 #pragma unroll
     for (int s = 0; s < I; s++) node[s] = 0;
-    for (int lvl = 0; lvl < t.nlevels; lvl++) {
-        const K *lp = (lvl < t.smem_levels ? s_top : gseps) + t.lvl_off[lvl];
-        K c[I][KPL];
-#pragma unroll
-        for (int s = 0; s < I; s++) load_keys<K, KPL>(lp + node[s] * F + gl * KPL, c[s]);
-#pragma unroll
-        for (int s = 0; s < I; s++) {
-            const int cnt = count_below<K, KPL>(c[s], qe[s], upper[s]);
-            node[s] = node[s] * F + group_count<G, G, KPL>(cnt, true, grp);
-        }
-    }
+    int lvl = 0;
+    for (; lvl < t.smem_levels; lvl++) level_step<K, G, I>(s_top + t.lvl_off[lvl], qe, upper, node, grp, gl);
+    const K *gseps = static_cast<const K *>(t.seps);
+    for (; lvl < t.nlevels; lvl++) level_step<K, G, I>(gseps + t.lvl_off[lvl], qe, upper, node, grp, gl);
 }
 
 // Stages the top separator levels into shared memory (16-byte copies).
@@ -132,5 +134,21 @@ __device__ __forceinline__ void stage_top(K *s_top, const DevTree &t) {
     const uint32_t n16 = (uint32_t)((t.smem_elems * sizeof(K)) / 16);
     for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
 }
+
+// Leaf stage for one leaf block: the 32-byte key sector is NKC = 2 chunks of
+// 16 bytes; the value part is NVC chunks.  Chunk c is held by lane c % G of
+// the group (CPL chunks per lane).  Returns the lower/upper-bound position
+// inside the block, and (for lower bounds) whether the key there equals q.
+template <typename K, typename V, int G>
+struct LeafStage {
+    using LG = LeafGeom<K, V>;
+    static constexpr int KPC = 16 / (int)sizeof(K);      // keys per chunk
+    static constexpr int VPC = 16 / (int)sizeof(V);      // values per chunk
+    static constexpr int NKC = kSectorBytes / 16;        // key chunks (2)
+    static constexpr int NVC = (LG::VB + 15) / 16;       // value chunks
+    static constexpr int NC = NKC + NVC;
+    static constexpr int CPL = (NC + G - 1) / G;         // chunks per lane (values too)
+    static constexpr int KCPL = (NKC + G - 1) / G;       // key chunks per lane
+};
 
 }  // namespace bt

@@ -78,7 +78,9 @@ typedef struct bt_info {
     uint64_t min_key;
     uint64_t max_key;
     int32_t device;
-    int32_t values_sorted; /* values ascend with keys (range IDs need no sort) */
+    int32_t values_sorted;      /* values ascend with keys (range IDs need no sort) */
+    uint32_t lanes_per_query;   /* search kernel configuration (see bt_set_search_config) */
+    uint32_t queries_per_group;
 } bt_info;
 
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
@@ -107,6 +109,15 @@ BT_API bt_status bt_build_host(const void *h_sorted_keys, const void *h_values, 
 BT_API bt_status bt_destroy(bt_tree *tree);
 
 BT_API bt_status bt_get_info(const bt_tree *tree, bt_info *info);
+
+/*
+ * Search-kernel configuration of a tree: lanes of a warp that serve one query
+ * (1, 2, 4 or 8) and queries each lane group keeps in flight (2 or 4).
+ * Supported pairs: (8,2) (8,4) (4,2) (4,4) (2,2) (1,2).  Results do not
+ * depend on it; speed does.  The reference has no such knob (one thread per
+ * query, BPTreeExactSearch.cu:31); the autotuner sets it.
+ */
+BT_API bt_status bt_set_search_config(bt_tree *tree, int lanes_per_query, int queries_per_group);
 
 /*
  * Point search: d_out[i] = value of key d_queries[i], or all-ones on a miss.

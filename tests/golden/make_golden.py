@@ -42,8 +42,8 @@ def main(out):
     q = g.integers(1, 1 << 32, size=2048, dtype=np.uint64)
     q[::2] = k[g.integers(0, len(k), size=1024)]
     ref.build(k, k)
-    gq, out = ref.point_grouped(q)
-    d.update(pg_keys=k, pg_q=q, pg_grouped_q=gq, pg_out=out)
+    gq, res = ref.point_grouped(q)
+    d.update(pg_keys=k, pg_q=q, pg_grouped_q=gq, pg_out=res)
     # range endpoints and counts, value = key, 3 leaves
     g, k = keys_for(3 * PAGESIZE, 3)
     r = g.integers(0, len(k), size=2048)

@@ -115,6 +115,41 @@ def test_grouping_is_a_stable_permutation(bt, cuda):
     assert np.all(np.diff(perm)[same] > 0)                  # stable inside a group
 
 
+@pytest.mark.parametrize("kt,vt", TYPES)
+@pytest.mark.parametrize("cfg", [(8, 2), (8, 4), (4, 2), (4, 4), (2, 2), (1, 2)])
+def test_every_search_config(bt, orc, cuda, kt, vt, cfg):
+    """Results do not depend on the kernel shape the autotuner picks."""
+    g = np.random.default_rng(31)
+    keys = make_keys(70001, kt, g)
+    vals = g.integers(0, np.iinfo(vt).max, size=len(keys), dtype=np.uint64).astype(vt)
+    q = queries_for(keys, kt, g, extra=20000)
+    lo = np.minimum(q, np.roll(q, 1))
+    hi = np.maximum(q, np.roll(q, 1))
+    exp = orc.point_search(keys, vals, q)
+    expc = orc.range_count(keys, lo, hi)
+    with bt.Tree.build(dev(keys, cuda), dev(vals, cuda)) as t:
+        t.set_search_config(*cfg)
+        assert (t.info.lanes_per_query, t.info.queries_per_group) == cfg
+        for mode in ("basic", "grouped"):
+            assert np.array_equal(t.point_search(dev(q, cuda), mode=mode).cpu().numpy(), exp)
+        for mode in ("basic", "2d", "zorder"):
+            got = t.range_count(dev(lo, cuda), dev(hi, cuda), mode=mode).cpu().numpy()
+            assert np.array_equal(got, expc)
+
+
+def test_autotuner_picks_a_supported_config(bt, orc, cuda):
+    import importlib
+    at = importlib.import_module("b-tree-index-searching_b200.autotune")
+    g = np.random.default_rng(5)
+    keys = make_keys(1 << 18, np.uint32, g, dense_ends=False)
+    q = g.integers(0, 1 << 32, size=1 << 18, dtype=np.uint64).astype(np.uint32)
+    with bt.Tree.build(dev(keys, cuda), dev(keys, cuda)) as t:
+        lanes, slots, ms = at.tune(t, dev(q, cuda), mode="basic", repeats=2)
+        assert (lanes, slots) in bt.Tree.SEARCH_CONFIGS and len(ms) == 6
+        got = t.point_search(dev(q, cuda)).cpu().numpy()
+    assert np.array_equal(got, orc.point_search(keys, keys, q))
+
+
 def test_wrong_query_width_rejected(bt, cuda):
     keys = np.arange(100, dtype=np.uint64)
     with bt.Tree.build(dev(keys, cuda), dev(keys, cuda)) as t:
