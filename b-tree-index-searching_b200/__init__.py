@@ -57,7 +57,7 @@ class bt_info(ctypes.Structure):
         ("device", ctypes.c_int32),
         ("values_sorted", ctypes.c_int32),
         ("lanes_per_query", ctypes.c_uint32),
-        ("queries_per_group", ctypes.c_uint32),
+        ("rounds", ctypes.c_uint32),
     ]
 
 
@@ -187,14 +187,13 @@ class Tree:
     def handle(self):
         return self._h
 
-    def set_search_config(self, lanes_per_query, queries_per_group):
+    def set_search_config(self, lanes_per_query, rounds):
         """Search kernel shape (see bt_set_search_config); results unchanged."""
         L = lib()
-        _check(L.bt_set_search_config(self._h, lanes_per_query, queries_per_group),
-               "bt_set_search_config")
+        _check(L.bt_set_search_config(self._h, lanes_per_query, rounds), "bt_set_search_config")
         _check(L.bt_get_info(self._h, ctypes.byref(self.info)), "bt_get_info")
 
-    SEARCH_CONFIGS = ((8, 2), (8, 4), (4, 2), (4, 4), (2, 2), (1, 2))
+    SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
 
     # -- point search ---------------------------------------------------
     def point_search(self, queries, mode="basic", out=None, stream=None):

@@ -1,8 +1,8 @@
 """Autotuner for the search kernels' shape.
 
 For a tree and a sample batch, times every supported (lanes per query,
-queries per lane group) configuration of the search kernels with CUDA events
-and keeps the fastest.  Results do not depend on the configuration (the tests
+rounds) configuration of the search kernels with CUDA events and keeps the
+fastest.  Results do not depend on the configuration (the tests
 check every one against the oracle), only speed does.  Decisions can be
 cached in a JSON file keyed by (keys, key width, value width, mode, batch
 size class), so a serving process tunes once per shape.
@@ -10,14 +10,15 @@ size class), so a serving process tunes once per shape.
 The reference has no tuning: one thread per query, 1024-thread blocks,
 fanout fixed at PAGESIZE = 5000 (BPTree.h:8, BPTreeExactSearch.cu:31).  Here
 the node fanout is fixed by the 128-byte line (32 u32 / 16 u64 separators);
-what is tuned is how many lanes share a query and how many queries each lane
-group keeps in flight.
+what is tuned is how many lanes share a query below the shared-memory level
+and in how many rounds a warp's 32 queries pass through those levels (that
+is, how many queries each lane group keeps in flight).
 """
 import json
 import os
 import statistics
 
-SEARCH_CONFIGS = ((8, 2), (8, 4), (4, 2), (4, 4), (2, 2), (1, 2))
+SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
 
 
 def _key(tree, mode, nq):

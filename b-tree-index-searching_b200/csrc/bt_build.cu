@@ -154,13 +154,13 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     dt.n = n;
     dt.max_key = t->max_key;
     dt.n_sectors = t->n_sectors;
-    // sl = number of top levels whose total size fits the budget; never the
-    // bottom level (the largest, and the last one a query reaches).
-    // lvl_off[sl] is the size of levels 0 .. sl-1.
+    // The deepest separator level whose real entries fit the shared-memory
+    // budget; a binary search over it resolves every level above it at once.
     int sl = 0;
-    while (sl + 1 <= L - 1 && dt.lvl_off[sl + 1] * sizeof(K) <= kSmemTopBudget) sl++;
-    dt.smem_levels = sl;
-    dt.smem_elems = (uint32_t)dt.lvl_off[sl];
+    while (sl + 1 <= L - 1 && t->lvl_entries[sl + 1] * sizeof(K) <= kSmemTopBudget) sl++;
+    dt.smem_level = sl;
+    dt.smem_entries = (uint32_t)t->lvl_entries[sl];
+    dt.smem_bytes = (uint32_t)(((t->lvl_entries[sl] * sizeof(K)) + 15) / 16 * 16);
     return BT_OK;
 }
 
@@ -253,11 +253,11 @@ bt_status bt_destroy(bt_tree *tree) {
     return BT_OK;
 }
 
-bt_status bt_set_search_config(bt_tree *t, int lanes_per_query, int queries_per_group) {
+bt_status bt_set_search_config(bt_tree *t, int lanes_per_query, int rounds) {
     using namespace bt;
     if (!t) return fail(BT_ERR_INVALID_ARGUMENT, "tree is NULL");
-    const int k = search_cfg_index(lanes_per_query, queries_per_group);
-    if (k < 0) return fail(BT_ERR_INVALID_ARGUMENT, "unsupported (lanes, slots) search configuration");
+    const int k = search_cfg_index(lanes_per_query, rounds);
+    if (k < 0) return fail(BT_ERR_INVALID_ARGUMENT, "unsupported (lanes, rounds) search configuration");
     t->search_cfg = k;
     return BT_OK;
 }
@@ -272,7 +272,7 @@ bt_status bt_get_info(const bt_tree *t, bt_info *info) {
     info->num_levels = (uint32_t)t->dev.nlevels;
     info->fanout = (uint32_t)(kLineBytes / t->key_bytes);
     info->leaf_keys = (uint32_t)(kSectorBytes / t->key_bytes);
-    info->smem_levels = (uint32_t)t->dev.smem_levels;
+    info->smem_levels = (uint32_t)(t->n ? t->dev.smem_level + 1 : 0);
     info->device_bytes = t->n_sectors * (uint64_t)leaf_stride(t->key_bytes, t->val_bytes) +
                          t->seps_elems * t->key_bytes;
     info->min_key = t->min_key;
@@ -280,7 +280,7 @@ bt_status bt_get_info(const bt_tree *t, bt_info *info) {
     info->device = t->device;
     info->values_sorted = t->values_sorted;
     info->lanes_per_query = (uint32_t)search_cfg_lanes(t->search_cfg);
-    info->queries_per_group = (uint32_t)search_cfg_slots(t->search_cfg);
+    info->rounds = (uint32_t)search_cfg_rounds(t->search_cfg);
     return BT_OK;
 }
 

@@ -35,8 +35,9 @@ constexpr int kLineBytes = 128;   // internal node size
 constexpr int kSectorBytes = 32;  // leaf sector size
 constexpr int kMaxLevels = 24;
 
-// Shared-memory budget for the staged top levels of one search CTA.
-constexpr size_t kSmemTopBudget = 40 * 1024;
+// Shared-memory budget for the separator level a search CTA stages (the
+// deepest level that fits is staged and binary-searched per query).
+constexpr size_t kSmemTopBudget = 96 * 1024;
 
 // Leaf block geometry for key type K and value type V.
 template <typename K, typename V>
@@ -59,8 +60,9 @@ struct DevTree {
     uint64_t n_sectors;
     uint64_t lvl_off[kMaxLevels];  // element offset of level t in seps (t = 0 is the root)
     int nlevels;
-    int smem_levels;               // levels 0 .. smem_levels-1 are staged in shared memory
-    uint32_t smem_elems;           // elements staged (= lvl_off[smem_levels])
+    int smem_level;                // level staged in shared memory (resolves levels 0..smem_level)
+    uint32_t smem_entries;         // its real separators
+    uint32_t smem_bytes;           // bytes staged (a multiple of 16)
 };
 
 }  // namespace bt
@@ -135,12 +137,12 @@ bt_status launch_scan_u64(const uint64_t *d_in, uint64_t *d_out, uint64_t n, uin
 bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
                             const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
 
-// (lanes per query, queries per group) -> index of the search configuration
-// table in bt_search.cu, or -1.
-int search_cfg_index(int lanes, int slots);
+// (lanes per query, rounds) -> index of the search configuration table in
+// bt_search.cu, or -1.
+int search_cfg_index(int lanes, int rounds);
 int default_search_cfg(int key_bytes);
 int search_cfg_lanes(int cfg);
-int search_cfg_slots(int cfg);
+int search_cfg_rounds(int cfg);
 
 // Partition kinds for launch_partition.
 enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2 };

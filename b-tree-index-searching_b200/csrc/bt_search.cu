@@ -10,8 +10,9 @@
 // (BtreeRangeSearch.cu:215-374 and :33-211).  With implicit leaf positions
 // the count is upper_bound(hi) - lower_bound(lo); no leaf-chain walk.
 //
-// Both kernels are persistent (grid = SMs x resident CTAs), stage the top
-// separator levels into shared memory once per CTA, then loop over warp tiles.
+// Both kernels are persistent (grid = SMs x resident CTAs), stage one
+// separator level into shared memory once per CTA, then loop over warp tiles
+// of 32 queries (see bt_search.cuh for the two-phase descent).
 // The leaf stage loads the whole leaf block of the query -- key sector and
 // value sector side by side, one 64-byte DRAM access -- with its chunks
 // spread over the group's lanes, so a hit costs one HBM round trip.
@@ -22,45 +23,51 @@
 
 namespace bt {
 
-// Lanes per query (G) and queries in flight per group (I) of the search
-// kernels; set per tree by bt_set_search_config / the autotuner.
+// Lanes per query (G) below the staged level and rounds (R) per warp tile of
+// 32 queries; each group keeps G/R queries in flight.  Set per tree by
+// bt_set_search_config / the autotuner.
 struct SearchCfg {
-    int g, i;
+    int g, r;
 };
-constexpr SearchCfg kSearchCfgs[] = {{8, 2}, {8, 4}, {4, 2}, {4, 4}, {2, 2}, {1, 2}};
+constexpr SearchCfg kSearchCfgs[] = {{8, 1}, {8, 2}, {4, 1}, {4, 2}, {2, 1}};
 constexpr int kNumSearchCfgs = sizeof(kSearchCfgs) / sizeof(kSearchCfgs[0]);
 
-int search_cfg_index(int g, int i) {
+int search_cfg_index(int g, int r) {
     for (int k = 0; k < kNumSearchCfgs; k++)
-        if (kSearchCfgs[k].g == g && kSearchCfgs[k].i == i) return k;
+        if (kSearchCfgs[k].g == g && kSearchCfgs[k].r == r) return k;
     return -1;
 }
 
 int search_cfg_lanes(int cfg) { return kSearchCfgs[cfg].g; }
-int search_cfg_slots(int cfg) { return kSearchCfgs[cfg].i; }
+int search_cfg_rounds(int cfg) { return kSearchCfgs[cfg].r; }
 
 int default_search_cfg(int key_bytes) {
     (void)key_bytes;
-    return search_cfg_index(8, 2);
+    return search_cfg_index(4, 1);
 }
 
 namespace {
 
 constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
 
-template <typename K, typename V, int G, int I, bool PERM>
+// Shared memory of a search CTA: the staged level, then (bounds kernel) 64
+// 8-byte results per warp.
+__host__ __device__ inline size_t scratch_offset(const DevTree &t) { return ((size_t)t.smem_bytes + 15) / 16 * 16; }
+
+template <typename K, typename V, int G, int R, bool PERM>
 __global__ void __launch_bounds__(kThreads)
 point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
              const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *s_top = reinterpret_cast<K *>(smem_raw);
-    stage_top<K>(s_top, t);
+    K *s_lvl = reinterpret_cast<K *>(smem_raw);
+    stage_level<K>(s_lvl, t);
     __syncthreads();
 
     using LG = LeafGeom<K, V>;
     using LS = LeafStage<K, V, G>;
-    constexpr int QPW = 32 / G;  // queries per warp and slot
-    constexpr int TILE = QPW * I;
+    constexpr int NG = 32 / G;  // lane groups per warp
+    constexpr int I = G / R;    // queries in flight per group and round
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int gl = lane % G;
@@ -70,168 +77,180 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     const K tmax = (K)t.max_key;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
 
-    for (uint64_t base = warp * TILE; base < nq; base += nwarps * TILE) {
-        K qv[I], qe[I];
-        bool up[I];
-        uint32_t node[I];
-#pragma unroll
-        for (int s = 0; s < I; s++) {
-            const uint64_t qi = base + (uint64_t)s * QPW + grp;
-            qv[s] = qi < nq ? q[qi] : (K)0;
-            qe[s] = qv[s] < tmax ? qv[s] : tmax;
-            up[s] = false;
-        }
-        descend<K, G, I>(t, s_top, qe, up, node, grp, gl);
+    for (uint64_t base = warp * 32; base < nq; base += nwarps * 32) {
+        // phase 1: one lane per query, binary search of the staged level
+        const uint64_t my = base + lane;
+        const K myq = my < nq ? q[my] : (K)0;
+        const uint32_t mynode = smem_bound<K>(s_lvl, t.smem_entries, myq < tmax ? myq : tmax, false);
 
-        // the leaf block: key chunks then value chunks, chunk c on lane c % G
-        uint32_t ch[I][LS::CPL][4];
+        // phase 2: G lanes per query through the global levels and the leaf
 #pragma unroll
-        for (int s = 0; s < I; s++) {
-            const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
+        for (int r = 0; r < R; r++) {
+            K qv[I], qe[I];
+            bool up[I];
+            uint32_t node[I];
 #pragma unroll
-            for (int j = 0; j < LS::CPL; j++) {
-                const int c = gl + j * G;
-                if (c < LS::NC) {
-                    const uint4 x = load_stream16(blk + (c < LS::NKC ? c * 16 : kSectorBytes + (c - LS::NKC) * 16));
-                    ch[s][j][0] = x.x;
-                    ch[s][j][1] = x.y;
-                    ch[s][j][2] = x.z;
-                    ch[s][j][3] = x.w;
-                }
+            for (int s = 0; s < I; s++) {
+                const int k = r * (NG * I) + s * NG + grp;  // query of the tile
+                qv[s] = __shfl_sync(0xffffffffu, myq, k);
+                node[s] = __shfl_sync(0xffffffffu, mynode, k);
+                qe[s] = qv[s] < tmax ? qv[s] : tmax;
+                up[s] = false;
             }
-        }
+            walk_global<K, G, I>(t, qe, up, node, grp, gl);
+
+            // the leaf block: key chunks then value chunks, chunk c on lane c % G
+            uint32_t ch[I][LS::CPL][4];
 #pragma unroll
-        for (int s = 0; s < I; s++) {
-            int cnt = 0;
-            bool eq = false;
-#pragma unroll
-            for (int j = 0; j < LS::KCPL; j++) {
-                if (gl + j * G < LS::NKC) {
-                    cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], false);
-#pragma unroll
-                    for (int k = 0; k < LS::KPC; k++) eq |= key_at<K>(ch[s][j], k) == qv[s];
-                }
-            }
-            int pos;
-            bool found;
-            if constexpr (G == 1) {
-                pos = cnt;
-                found = eq;
-            } else {
-                pos = __shfl_sync(0xffffffffu, cnt, grp * G) + __shfl_sync(0xffffffffu, cnt, grp * G + 1);
-                found = (__ballot_sync(0xffffffffu, eq) & gmask) != 0;
-            }
-            found = found && qv[s] <= tmax;  // padding keys are all-ones
-            const uint64_t qi = base + (uint64_t)s * QPW + grp;
-            pos = pos < LG::S ? pos : LG::S - 1;
-            const int vc = LS::NKC + pos / LS::VPC;  // chunk holding the value
-            if (gl == vc % G && qi < nq) {
-                V val = 0;
+            for (int s = 0; s < I; s++) {
+                const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
 #pragma unroll
                 for (int j = 0; j < LS::CPL; j++) {
-                    if (j == vc / G) {
-                        const int w = (pos % LS::VPC) * (int)(sizeof(V) / 4);
-                        if constexpr (sizeof(V) == 4) {
-#pragma unroll
-                            for (int k = 0; k < 4; k++)
-                                if (k == w) val = ch[s][j][k];
-                        } else {
-                            val = w == 0 ? (((uint64_t)ch[s][j][1] << 32) | ch[s][j][0])
-                                         : (((uint64_t)ch[s][j][3] << 32) | ch[s][j][2]);
-                        }
+                    const int c = gl + j * G;
+                    if (c < LS::NC) {
+                        const uint4 x = load_stream16(
+                            blk + (c < LS::NKC ? c * 16 : kSectorBytes + (c - LS::NKC) * 16));
+                        ch[s][j][0] = x.x;
+                        ch[s][j][1] = x.y;
+                        ch[s][j][2] = x.z;
+                        ch[s][j][3] = x.w;
                     }
                 }
-                const uint64_t dst = PERM ? (uint64_t)perm[qi] : qi;
-                out[dst] = found ? val : key_max<V>();
+            }
+#pragma unroll
+            for (int s = 0; s < I; s++) {
+                int cnt = 0;
+                bool eq = false;
+#pragma unroll
+                for (int j = 0; j < LS::KCPL; j++) {
+                    if (gl + j * G < LS::NKC) {
+                        cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], false);
+#pragma unroll
+                        for (int k = 0; k < LS::KPC; k++) eq |= key_at<K>(ch[s][j], k) == qv[s];
+                    }
+                }
+                const int pos0 = __shfl_sync(0xffffffffu, cnt, grp * G) +
+                                 __shfl_sync(0xffffffffu, cnt, grp * G + 1);
+                const bool found =
+                    (__ballot_sync(0xffffffffu, eq) & gmask) != 0 && qv[s] <= tmax;  // pad keys are all-ones
+                const int pos = pos0 < LG::S ? pos0 : LG::S - 1;
+                const int vc = LS::NKC + pos / LS::VPC;  // chunk holding the value
+                const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
+                if (gl == vc % G && qi < nq) {
+                    V val = 0;
+#pragma unroll
+                    for (int j = 0; j < LS::CPL; j++) {
+                        if (j == vc / G) {
+                            const int w = (pos % LS::VPC) * (int)(sizeof(V) / 4);
+                            if constexpr (sizeof(V) == 4) {
+#pragma unroll
+                                for (int k = 0; k < 4; k++)
+                                    if (k == w) val = ch[s][j][k];
+                            } else {
+                                val = w == 0 ? (((uint64_t)ch[s][j][1] << 32) | ch[s][j][0])
+                                             : (((uint64_t)ch[s][j][3] << 32) | ch[s][j][2]);
+                            }
+                        }
+                    }
+                    const uint64_t dst = PERM ? (uint64_t)perm[qi] : qi;
+                    out[dst] = found ? val : key_max<V>();
+                }
             }
         }
     }
 }
 
-// Lower bound of lo and upper bound of hi for QG queries per group (2*QG
-// descents in flight).  counts[i] = ub - lb (0 if lo > hi); lb_out[i] = lb.
-template <typename K, typename V, int G, int QG, bool PERM>
+// Lower bound of lo and upper bound of hi per query: 64 descents per warp
+// tile of 32 queries (d < 32: lower bound of query d, else upper bound of
+// query d - 32), passed in 2R rounds.  counts[i] = ub - lb (0 if lo > hi);
+// lb_out[i] = lb.
+template <typename K, typename V, int G, int R, bool PERM>
 __global__ void __launch_bounds__(kThreads)
 bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
               const K *__restrict__ hi, const uint32_t *__restrict__ perm, uint64_t nq,
               uint64_t *__restrict__ counts, uint64_t *__restrict__ lb_out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *s_top = reinterpret_cast<K *>(smem_raw);
-    stage_top<K>(s_top, t);
+    K *s_lvl = reinterpret_cast<K *>(smem_raw);
+    stage_level<K>(s_lvl, t);
     __syncthreads();
 
     using LG = LeafGeom<K, V>;
     using LS = LeafStage<K, V, G>;
-    constexpr int I = 2 * QG;
-    constexpr int QPW = 32 / G;
-    constexpr int TILE = QPW * QG;
+    constexpr int NG = 32 / G;
+    constexpr int I = G / R;
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int gl = lane % G;
+    uint64_t *res = reinterpret_cast<uint64_t *>(smem_raw + scratch_offset(t)) + (threadIdx.x >> 5) * 64;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const K tmax = (K)t.max_key;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
 
-    for (uint64_t base = warp * TILE; base < nq; base += nwarps * TILE) {
-        K a[QG], b[QG], qe[I];
-        bool up[I];
-        uint32_t node[I];
+    for (uint64_t base = warp * 32; base < nq; base += nwarps * 32) {
+        const uint64_t my = base + lane;
+        const bool v = my < nq;
+        const K a = v ? lo[my] : (K)0;
+        const K b = v ? hi[my] : (K)0;
+        // lower bound of a: a > max gives n (walk on max instead)
+        const K qa = a <= tmax ? a : tmax;
+        // upper bound of b: b >= max gives n (walk a lower bound of max instead)
+        const K qb = b < tmax ? b : tmax;
+        const bool ub_upper = b < tmax;
+        const uint32_t na = smem_bound<K>(s_lvl, t.smem_entries, qa, false);
+        const uint32_t nb = smem_bound<K>(s_lvl, t.smem_entries, qb, ub_upper);
+
 #pragma unroll
-        for (int j = 0; j < QG; j++) {
-            const uint64_t qi = base + (uint64_t)j * QPW + grp;
-            const bool v = qi < nq;
-            a[j] = v ? lo[qi] : (K)0;
-            b[j] = v ? hi[qi] : (K)0;
-            // lower bound of a: a > max gives n (walk on max instead)
-            qe[2 * j] = a[j] <= tmax ? a[j] : tmax;
-            up[2 * j] = false;
-            // upper bound of b: b >= max gives n (walk a lower bound of max instead)
-            qe[2 * j + 1] = b[j] < tmax ? b[j] : tmax;
-            up[2 * j + 1] = b[j] < tmax;
-        }
-        descend<K, G, I>(t, s_top, qe, up, node, grp, gl);
-        uint32_t ch[I][LS::KCPL][4];
+        for (int r = 0; r < 2 * R; r++) {
+            const bool which = r >= R;  // uniform per round: lower bounds first
+            K qe[I];
+            bool up[I];
+            uint32_t node[I];
 #pragma unroll
-        for (int s = 0; s < I; s++) {
-            const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
+            for (int s = 0; s < I; s++) {
+                const int k = (r % R) * (NG * I) + s * NG + grp;
+                qe[s] = __shfl_sync(0xffffffffu, which ? qb : qa, k);
+                node[s] = __shfl_sync(0xffffffffu, which ? nb : na, k);
+                up[s] = which ? __shfl_sync(0xffffffffu, ub_upper, k) : false;
+            }
+            walk_global<K, G, I>(t, qe, up, node, grp, gl);
+            uint32_t ch[I][LS::KCPL][4];
 #pragma unroll
-            for (int j = 0; j < LS::KCPL; j++) {
-                const int c = gl + j * G;
-                if (c < LS::NKC) {
-                    const uint4 x = load_stream16(blk + c * 16);
-                    ch[s][j][0] = x.x;
-                    ch[s][j][1] = x.y;
-                    ch[s][j][2] = x.z;
-                    ch[s][j][3] = x.w;
+            for (int s = 0; s < I; s++) {
+                const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
+#pragma unroll
+                for (int j = 0; j < LS::KCPL; j++) {
+                    const int c = gl + j * G;
+                    if (c < LS::NKC) {
+                        const uint4 x = load_stream16(blk + c * 16);
+                        ch[s][j][0] = x.x;
+                        ch[s][j][1] = x.y;
+                        ch[s][j][2] = x.z;
+                        ch[s][j][3] = x.w;
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int j = 0; j < QG; j++) {
-            int pos[2];
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int s = 2 * j + e;
+            for (int s = 0; s < I; s++) {
                 int cnt = 0;
 #pragma unroll
-                for (int k = 0; k < LS::KCPL; k++)
-                    if (gl + k * G < LS::NKC) cnt += count_below<K, LS::KPC>(ch[s][k], qe[s], up[s]);
-                if constexpr (G == 1)
-                    pos[e] = cnt;
-                else
-                    pos[e] = __shfl_sync(0xffffffffu, cnt, grp * G) +
-                             __shfl_sync(0xffffffffu, cnt, grp * G + 1);
-            }
-            const uint64_t qi = base + (uint64_t)j * QPW + grp;
-            if (gl == 0 && qi < nq) {
-                const uint64_t lb = a[j] <= tmax ? (uint64_t)node[2 * j] * LG::S + pos[0] : t.n;
-                const uint64_t ub = b[j] < tmax ? (uint64_t)node[2 * j + 1] * LG::S + pos[1] : t.n;
-                const uint64_t dst = PERM ? (uint64_t)perm[qi] : qi;
-                counts[dst] = (a[j] <= b[j] && ub > lb) ? ub - lb : 0;
-                if (lb_out) lb_out[dst] = lb;
+                for (int j = 0; j < LS::KCPL; j++)
+                    if (gl + j * G < LS::NKC) cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], up[s]);
+                const int pos = __shfl_sync(0xffffffffu, cnt, grp * G) +
+                                __shfl_sync(0xffffffffu, cnt, grp * G + 1);
+                if (gl == 0) res[(which ? 32 : 0) + (r % R) * (NG * I) + s * NG + grp] =
+                    (uint64_t)node[s] * LG::S + pos;
             }
         }
+        __syncwarp();
+        if (v) {
+            const uint64_t lb = a <= tmax ? res[lane] : t.n;
+            const uint64_t ub = b < tmax ? res[32 + lane] : t.n;
+            const uint64_t dst = PERM ? (uint64_t)perm[my] : my;
+            counts[dst] = (a <= b && ub > lb) ? ub - lb : 0;
+            if (lb_out) lb_out[dst] = lb;
+        }
+        __syncwarp();
     }
 }
 
@@ -267,12 +286,27 @@ unsigned persistent_grid(const void *fn, size_t smem, uint64_t work_items, uint6
     return (unsigned)(want < 1 ? 1 : want);
 }
 
-template <typename K, typename V, int G, int I, bool PERM>
+template <typename Fn>
+bt_status set_smem(Fn fn, size_t smem) {
+    static std::mutex mu;
+    static std::map<const void *, size_t> done;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = done.find((const void *)fn);
+    if (it != done.end() && it->second >= smem) return BT_OK;
+    if (smem > 48 * 1024)
+        BT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    done[(const void *)fn] = smem;
+    return BT_OK;
+}
+
+template <typename K, typename V, int G, int R, bool PERM>
 bt_status point_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
                        void *d_out, cudaStream_t s) {
-    auto fn = point_kernel<K, V, G, I, PERM>;
-    const size_t smem = (size_t)t->dev.smem_elems * sizeof(K);
-    const unsigned grid = persistent_grid((const void *)fn, smem, nq, (kThreads / 32) * (32 / G) * I);
+    auto fn = point_kernel<K, V, G, R, PERM>;
+    const size_t smem = scratch_offset(t->dev);
+    bt_status st = set_smem(fn, smem);
+    if (st != BT_OK) return st;
+    const unsigned grid = persistent_grid((const void *)fn, smem, nq, kThreads);
     count_launch();
     fn<<<grid, kThreads, smem, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out);
     BT_CUDA(cudaGetLastError());
@@ -283,22 +317,23 @@ template <typename K, typename V, bool PERM>
 bt_status point_cfg(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
                     void *d_out, cudaStream_t s) {
     switch (t->search_cfg) {
-        case 0: return point_launch<K, V, 8, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 1: return point_launch<K, V, 8, 4, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 2: return point_launch<K, V, 4, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 3: return point_launch<K, V, 4, 4, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 4: return point_launch<K, V, 2, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
-        default: return point_launch<K, V, 1, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 0: return point_launch<K, V, 8, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 1: return point_launch<K, V, 8, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 2: return point_launch<K, V, 4, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 3: return point_launch<K, V, 4, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
+        default: return point_launch<K, V, 2, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
     }
 }
 
-template <typename K, typename V, int G, int QG, bool PERM>
+template <typename K, typename V, int G, int R, bool PERM>
 bt_status bounds_launch(const bt_tree *t, const void *d_lo, const void *d_hi,
                         const uint32_t *d_perm, uint64_t nq, uint64_t *d_counts, uint64_t *d_lb,
                         cudaStream_t s) {
-    auto fn = bounds_kernel<K, V, G, QG, PERM>;
-    const size_t smem = (size_t)t->dev.smem_elems * sizeof(K);
-    const unsigned grid = persistent_grid((const void *)fn, smem, nq, (kThreads / 32) * (32 / G) * QG);
+    auto fn = bounds_kernel<K, V, G, R, PERM>;
+    const size_t smem = scratch_offset(t->dev) + (size_t)kWarps * 64 * sizeof(uint64_t);
+    bt_status st = set_smem(fn, smem);
+    if (st != BT_OK) return st;
+    const unsigned grid = persistent_grid((const void *)fn, smem, nq, kThreads);
     count_launch();
     fn<<<grid, kThreads, smem, s>>>(t->dev, (const K *)d_lo, (const K *)d_hi, d_perm, nq, d_counts,
                                     d_lb);
@@ -309,14 +344,12 @@ bt_status bounds_launch(const bt_tree *t, const void *d_lo, const void *d_hi,
 template <typename K, typename V, bool PERM>
 bt_status bounds_cfg(const bt_tree *t, const void *d_lo, const void *d_hi, const uint32_t *d_perm,
                      uint64_t nq, uint64_t *d_counts, uint64_t *d_lb, cudaStream_t s) {
-    // two descents per range query: half the point configuration's slots
     switch (t->search_cfg) {
         case 0: return bounds_launch<K, V, 8, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
         case 1: return bounds_launch<K, V, 8, 2, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
         case 2: return bounds_launch<K, V, 4, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
         case 3: return bounds_launch<K, V, 4, 2, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
-        case 4: return bounds_launch<K, V, 2, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
-        default: return bounds_launch<K, V, 1, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
+        default: return bounds_launch<K, V, 2, 1, PERM>(t, d_lo, d_hi, d_perm, nq, d_counts, d_lb, s);
     }
 }
 

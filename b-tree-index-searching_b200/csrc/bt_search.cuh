@@ -1,21 +1,25 @@
 // Device-side descent shared by the point, range and forest kernels.
 //
-// A query is served by a group of G lanes of one warp.  At an internal level
-// the group reads the node's 128-byte line with 16-byte vector loads (F/G
-// separators per lane), counts the separators below the query, and combines
-// the per-lane counts with one warp ballot and one shuffle: because the line
-// is sorted, the lanes whose whole chunk is below the query form a prefix,
-// so count = KPL * (#full lanes) + (count of the first non-full lane).  The
-// child index is node*F + count.  Each group works on I queries at once
-// (independent dependency chains), so several line loads are in flight per
-// group.  The top levels are read from shared memory, the rest from global
-// memory (L2-resident in practice), in two separate loops so each uses its
-// native load instruction.
+// Two phases per warp tile of 32 queries:
+//
+//  1. One thread per query.  The CTA stages in shared memory the deepest
+//     separator level that fits (for 2^26 u32 keys: the 8,192 maxima of the
+//     third level, 32 KB) and each lane runs a branchless binary search over
+//     it.  That single search resolves every level above the staged one and
+//     yields the node index on the first level below it; the query loads are
+//     coalesced and nothing crosses lanes.
+//  2. G lanes per query.  The remaining levels live in global memory (L2 in
+//     practice).  The group reads a node's 128-byte line with 16-byte vector
+//     loads (F/G separators per lane), counts the separators below the query,
+//     and combines the per-lane counts with one warp ballot and one shuffle:
+//     the line is sorted, so the lanes whose whole chunk is below the query
+//     form a prefix, and count = KPL * (#full lanes) + (count of the first
+//     non-full lane).  The child is node*F + count.  The warp's 32 queries
+//     pass in R rounds, each group keeping G/R queries in flight.
 //
 // The reference walks 80 KB pages by scalar binary search, one thread per
 // query, about 13 dependent 8-byte loads per level plus a leafFlag load on
-// another page per level (BPTreeExactSearch.cu:39-68).  Here each level costs
-// one coalesced line per query and the top levels come from shared memory.
+// another page per level (BPTreeExactSearch.cu:39-68).
 #pragma once
 
 #include "bt_internal.cuh"
@@ -111,28 +115,42 @@ __device__ __forceinline__ void level_step(const K *__restrict__ lp, const K (&q
     }
 }
 
-// Walks all separator levels.  qe[s] must satisfy qe[s] <= max_key (lower
-// bound) or qe[s] < max_key (upper bound) for the walk to stay on real
-// separators.  On return node[s] is the leaf block index.
+// Walks the separator levels below the staged one.  qe[s] must satisfy
+// qe[s] <= max_key (lower bound) or qe[s] < max_key (upper bound) for the walk
+// to stay on real separators.  On entry node[s] is the node index on level
+// smem_level + 1 (phase 1's result); on return it is the leaf block index.
 template <typename K, int G, int I>
-__device__ __forceinline__ void descend(const DevTree &t, const K *__restrict__ s_top,
-                                        const K (&qe)[I], const bool (&upper)[I],
-                                        uint32_t (&node)[I], int grp, int gl) {
-#pragma unroll
-    for (int s = 0; s < I; s++) node[s] = 0;
-    int lvl = 0;
-    for (; lvl < t.smem_levels; lvl++) level_step<K, G, I>(s_top + t.lvl_off[lvl], qe, upper, node, grp, gl);
+__device__ __forceinline__ void walk_global(const DevTree &t, const K (&qe)[I],
+                                            const bool (&upper)[I], uint32_t (&node)[I], int grp,
+                                            int gl) {
     const K *gseps = static_cast<const K *>(t.seps);
-    for (; lvl < t.nlevels; lvl++) level_step<K, G, I>(gseps + t.lvl_off[lvl], qe, upper, node, grp, gl);
+    for (int lvl = t.smem_level + 1; lvl < t.nlevels; lvl++)
+        level_step<K, G, I>(gseps + t.lvl_off[lvl], qe, upper, node, grp, gl);
 }
 
-// Stages the top separator levels into shared memory (16-byte copies).
+// Branchless lower (upper) bound over n >= 1 sorted keys in shared memory:
+// the first index i with s[i] >= q (s[i] > q), n if none.
 template <typename K>
-__device__ __forceinline__ void stage_top(K *s_top, const DevTree &t) {
-    const uint4 *src = static_cast<const uint4 *>(t.seps);
-    uint4 *dst = reinterpret_cast<uint4 *>(s_top);
-    const uint32_t n16 = (uint32_t)((t.smem_elems * sizeof(K)) / 16);
-    for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
+__device__ __forceinline__ uint32_t smem_bound(const K *__restrict__ s, uint32_t n, K q,
+                                               bool upper) {
+    uint32_t base = 0;
+    while (n > 1) {
+        const uint32_t half = n >> 1;
+        const K v = s[base + half];
+        base = (upper ? v <= q : v < q) ? base + half : base;
+        n -= half;
+    }
+    const K v = s[base];
+    return base + ((upper ? v <= q : v < q) ? 1u : 0u);
+}
+
+// Stages the binary-searched separator level into shared memory.
+template <typename K>
+__device__ __forceinline__ void stage_level(K *s_lvl, const DevTree &t) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(static_cast<const K *>(t.seps) +
+                                                       t.lvl_off[t.smem_level]);
+    uint4 *dst = reinterpret_cast<uint4 *>(s_lvl);
+    for (uint32_t i = threadIdx.x; i < t.smem_bytes / 16; i += blockDim.x) dst[i] = src[i];
 }
 
 // Leaf stage for one leaf block: the 32-byte key sector is NKC = 2 chunks of

@@ -314,13 +314,16 @@ def run_ours(args):
     torch.cuda.synchronize(device)
     clocks.start()
     launches0 = L.bt_kernel_launches()
+    nvtx = torch.cuda.nvtx
     for i in range(args.steps):
         flush.zero_()
+        nvtx.range_push("timed_grouped")
         ev[i][0].record(stream)
         group_into()
         ev[i][1].record(stream)
         search_grouped()
         ev[i][2].record(stream)
+        nvtx.range_pop()
     torch.cuda.synchronize(device)
     launches = L.bt_kernel_launches() - launches0
     barrier(dist, device)
@@ -338,9 +341,11 @@ def run_ours(args):
     bev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
     for i in range(args.steps):
         flush.zero_()
+        nvtx.range_push("timed_basic")
         bev[i][0].record(stream)
         search_basic()
         bev[i][1].record(stream)
+        nvtx.range_pop()
     torch.cuda.synchronize(device)
     basic_ms = max_over_ranks(statistics.mean(b[0].elapsed_time(b[1]) for b in bev), dist, device)
 

@@ -73,14 +73,14 @@ typedef struct bt_info {
     uint32_t num_levels;   /* separator levels above the leaf sectors */
     uint32_t fanout;       /* separators per internal node (one 128-byte line) */
     uint32_t leaf_keys;    /* keys per leaf sector (one 32-byte sector) */
-    uint32_t smem_levels;  /* top levels the search kernels stage in shared memory */
+    uint32_t smem_levels;  /* top levels resolved by the shared-memory binary search */
     uint64_t device_bytes; /* HBM held by the tree */
     uint64_t min_key;
     uint64_t max_key;
     int32_t device;
     int32_t values_sorted;      /* values ascend with keys (range IDs need no sort) */
     uint32_t lanes_per_query;   /* search kernel configuration (see bt_set_search_config) */
-    uint32_t queries_per_group;
+    uint32_t rounds;
 } bt_info;
 
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
@@ -111,13 +111,15 @@ BT_API bt_status bt_destroy(bt_tree *tree);
 BT_API bt_status bt_get_info(const bt_tree *tree, bt_info *info);
 
 /*
- * Search-kernel configuration of a tree: lanes of a warp that serve one query
- * (1, 2, 4 or 8) and queries each lane group keeps in flight (2 or 4).
- * Supported pairs: (8,2) (8,4) (4,2) (4,4) (2,2) (1,2).  Results do not
- * depend on it; speed does.  The reference has no such knob (one thread per
- * query, BPTreeExactSearch.cu:31); the autotuner sets it.
+ * Search-kernel configuration of a tree: lanes of a warp that share one query
+ * on the levels below shared memory (2, 4 or 8) and the number of rounds in
+ * which a warp's 32 queries pass through those levels (1 or 2; each lane
+ * group keeps lanes/rounds queries in flight).  Supported pairs: (8,1) (8,2)
+ * (4,1) (4,2) (2,1).  Results do not depend on it; speed does.  The
+ * reference has no such knob (one thread per query, BPTreeExactSearch.cu:31);
+ * the autotuner sets it.
  */
-BT_API bt_status bt_set_search_config(bt_tree *tree, int lanes_per_query, int queries_per_group);
+BT_API bt_status bt_set_search_config(bt_tree *tree, int lanes_per_query, int rounds);
 
 /*
  * Point search: d_out[i] = value of key d_queries[i], or all-ones on a miss.
