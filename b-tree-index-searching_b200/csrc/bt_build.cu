@@ -160,7 +160,8 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     while (sl + 1 <= L - 1 && t->lvl_entries[sl + 1] * sizeof(K) <= kSmemTopBudget) sl++;
     dt.smem_level = sl;
     dt.smem_entries = (uint32_t)t->lvl_entries[sl];
-    dt.smem_bytes = (uint32_t)(((t->lvl_entries[sl] * sizeof(K)) + 15) / 16 * 16);
+    // whole 128-byte bank rows, so the swizzle stays inside the staged region
+    dt.smem_bytes = (uint32_t)(((t->lvl_entries[sl] * sizeof(K)) + 127) / 128 * 128);
     return BT_OK;
 }
 

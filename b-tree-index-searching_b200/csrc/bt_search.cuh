@@ -128,29 +128,43 @@ __device__ __forceinline__ void walk_global(const DevTree &t, const K (&qe)[I],
         level_step<K, G, I>(gseps + t.lvl_off[lvl], qe, upper, node, grp, gl);
 }
 
-// Branchless lower (upper) bound over n >= 1 sorted keys in shared memory:
-// the first index i with s[i] >= q (s[i] > q), n if none.
+// Shared-memory slot of sorted element p.  A binary search over 2^k
+// elements probes positions that differ by multiples of large powers of two,
+// which in a plain array all fall into one bank (a 32-way conflict per
+// probe).  XOR-ing the bank bits with two higher bit fields spreads every
+// such probe set over distinct banks.  It only permutes elements within each
+// row of one bank width, so it is a bijection on [0, n).
+template <typename K>
+__device__ __forceinline__ uint32_t swz(uint32_t p) {
+    constexpr int B = sizeof(K) == 4 ? 5 : 4;  // log2(elements per bank row)
+    constexpr uint32_t M = (1u << B) - 1u;
+    return p ^ (((p >> B) ^ (p >> (2 * B))) & M);
+}
+
+// Branchless lower (upper) bound over n >= 1 sorted keys in shared memory
+// (stored swizzled): the first index i with s[i] >= q (s[i] > q), n if none.
 template <typename K>
 __device__ __forceinline__ uint32_t smem_bound(const K *__restrict__ s, uint32_t n, K q,
                                                bool upper) {
     uint32_t base = 0;
     while (n > 1) {
         const uint32_t half = n >> 1;
-        const K v = s[base + half];
+        const K v = s[swz<K>(base + half)];
         base = (upper ? v <= q : v < q) ? base + half : base;
         n -= half;
     }
-    const K v = s[base];
+    const K v = s[swz<K>(base)];
     return base + ((upper ? v <= q : v < q) ? 1u : 0u);
 }
 
-// Stages the binary-searched separator level into shared memory.
+// Stages the binary-searched separator level into shared memory, swizzled.
+// The staged region is padded to whole bank rows with all-ones keys.
 template <typename K>
 __device__ __forceinline__ void stage_level(K *s_lvl, const DevTree &t) {
-    const uint4 *src = reinterpret_cast<const uint4 *>(static_cast<const K *>(t.seps) +
-                                                       t.lvl_off[t.smem_level]);
-    uint4 *dst = reinterpret_cast<uint4 *>(s_lvl);
-    for (uint32_t i = threadIdx.x; i < t.smem_bytes / 16; i += blockDim.x) dst[i] = src[i];
+    const K *src = static_cast<const K *>(t.seps) + t.lvl_off[t.smem_level];
+    const uint32_t n = t.smem_bytes / sizeof(K);
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x)
+        s_lvl[swz<K>(i)] = i < t.smem_entries ? src[i] : key_max<K>();
 }
 
 // Leaf stage for one leaf block: the 32-byte key sector is NKC = 2 chunks of
