@@ -61,25 +61,36 @@ __device__ __forceinline__ uint32_t group_key(K a, K b, const GroupKeyParams &p)
     return spread16((uint32_t)x) | (spread16((uint32_t)y) << 1);
 }
 
+// Digit histogram of one tile: per-warp shared-memory histograms (atomics
+// only collide inside a warp), summed per digit at the end.
 template <typename K, bool HAS_B>
 __global__ void __launch_bounds__(kPT)
 part_hist_kernel(const K *__restrict__ a, const K *__restrict__ b, uint64_t n, GroupKeyParams gp,
                  int pass, uint32_t *__restrict__ counts, uint64_t ntiles) {
-    __shared__ uint32_t h[256];
-    for (int i = threadIdx.x; i < 256; i += kPT) h[i] = 0;
+    __shared__ uint32_t h[kPWarps][256];
+    for (int i = threadIdx.x; i < kPWarps * 256; i += kPT) (&h[0][0])[i] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
     const uint64_t t0 = (uint64_t)blockIdx.x * kPTile;
+    K av[kIPL], bv[kIPL];
 #pragma unroll
     for (int j = 0; j < kIPL; j++) {
         const uint64_t i = t0 + (uint64_t)j * kPT + threadIdx.x;
-        uint32_t d = 0xFFFFFFFFu;
-        if (i < n) d = (group_key<K>(a[i], HAS_B ? b[i] : (K)0, gp) >> (8 * pass)) & 0xFFu;
-        const unsigned m = __match_any_sync(0xffffffffu, d);
-        if (d != 0xFFFFFFFFu && lane == __ffs(m) - 1) atomicAdd(&h[d], (uint32_t)__popc(m));
+        av[j] = i < n ? a[i] : (K)0;
+        bv[j] = (HAS_B && i < n) ? b[i] : (K)0;
+    }
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        const uint64_t i = t0 + (uint64_t)j * kPT + threadIdx.x;
+        if (i < n) atomicAdd(&h[w][(group_key<K>(av[j], bv[j], gp) >> (8 * pass)) & 0xFFu], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < 256; d += kPT) counts[(uint64_t)d * ntiles + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < 256; d += kPT) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int ww = 0; ww < kPWarps; ww++) c += h[ww][d];
+        counts[(uint64_t)d * ntiles + blockIdx.x] = c;
+    }
 }
 
 // Exclusive scan of 256 values held one per thread by threads 0..255.
@@ -255,8 +266,21 @@ scan_down_kernel(const T *__restrict__ in, uint64_t n, const T *__restrict__ off
         *grand_total = total + (offs ? offs[blockIdx.x] : (T)0);
 }
 
+// Scratch elements scan_run needs for n inputs (block sums and offsets of
+// every recursion level).
+uint64_t scan_ws_elems(uint64_t n) {
+    uint64_t total = 0;
+    while (n > (uint64_t)kSTile) {
+        n = (n + kSTile - 1) / kSTile;
+        total += 2 * n;
+    }
+    return total;
+}
+
+// Exclusive scan d_out = scan(d_in) with caller-provided scratch (ws of
+// scan_ws_elems(n) elements); *d_total (optional) receives the sum.
 template <typename T>
-bt_status scan_impl(const T *d_in, T *d_out, uint64_t n, T *d_total, cudaStream_t s) {
+bt_status scan_run(const T *d_in, T *d_out, uint64_t n, T *d_total, T *ws, cudaStream_t s) {
     if (n == 0) {
         if (d_total) BT_CUDA(cudaMemsetAsync(d_total, 0, sizeof(T), s));
         return BT_OK;
@@ -268,26 +292,28 @@ bt_status scan_impl(const T *d_in, T *d_out, uint64_t n, T *d_total, cudaStream_
         BT_CUDA(cudaGetLastError());
         return BT_OK;
     }
-    T *sums = nullptr, *offs = nullptr;
-    bt_status st = ws_alloc((void **)&sums, nb * sizeof(T), s);
-    if (st != BT_OK) return st;
-    st = ws_alloc((void **)&offs, nb * sizeof(T), s);
-    if (st != BT_OK) {
-        ws_free(sums, s);
-        return st;
-    }
+    T *sums = ws, *offs = ws + nb;
     count_launch();
     scan_reduce_kernel<T><<<(unsigned)nb, kST, 0, s>>>(d_in, n, sums);
-    st = scan_impl<T>(sums, offs, nb, nullptr, s);
-    if (st == BT_OK) {
-        count_launch();
-        scan_down_kernel<T><<<(unsigned)nb, kST, 0, s>>>(d_in, n, offs, d_out, d_total);
-    }
-    ws_free(sums, s);
-    ws_free(offs, s);
+    bt_status st = scan_run<T>(sums, offs, nb, nullptr, ws + 2 * nb, s);
     if (st != BT_OK) return st;
+    count_launch();
+    scan_down_kernel<T><<<(unsigned)nb, kST, 0, s>>>(d_in, n, offs, d_out, d_total);
     BT_CUDA(cudaGetLastError());
     return BT_OK;
+}
+
+template <typename T>
+bt_status scan_impl(const T *d_in, T *d_out, uint64_t n, T *d_total, cudaStream_t s) {
+    const uint64_t we = scan_ws_elems(n);
+    T *ws = nullptr;
+    if (we) {
+        bt_status st = ws_alloc((void **)&ws, we * sizeof(T), s);
+        if (st != BT_OK) return st;
+    }
+    bt_status st = scan_run<T>(d_in, d_out, n, d_total, ws, s);
+    ws_free(ws, s);
+    return st;
 }
 
 // -------------------------------------------------------- partition host --
@@ -311,25 +337,42 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
     const uint64_t ntiles = (nq + kPTile - 1) / kPTile;
     if (ntiles * 256 >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "batch too large");
 
-    uint32_t *counts = nullptr;
-    bt_status st = ws_alloc((void **)&counts, ntiles * 256 * sizeof(uint32_t), s);
+    // One workspace: digit counts, scan scratch and, for multi-pass sorts,
+    // ping-pong copies of the payload.
+    const uint64_t ncounts = ntiles * 256;
+    const uint64_t scan_we = scan_ws_elems(ncounts);
+    const size_t pp_bytes = passes > 1 ? 2 * nq * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t)) : 0;
+    const size_t ws_bytes = (ncounts + scan_we) * sizeof(uint32_t) + 256 + pp_bytes;
+    unsigned char *ws = nullptr;
+    bt_status st = ws_alloc((void **)&ws, ws_bytes, s);
     if (st != BT_OK) return st;
-    // ping-pong buffers for multi-pass sorts
+    uint32_t *counts = reinterpret_cast<uint32_t *>(ws);
+    uint32_t *scan_ws = counts + ncounts;
+    unsigned char *pp = ws + ((ncounts + scan_we) * sizeof(uint32_t) + 255) / 256 * 256;
     K *ta[2] = {nullptr, nullptr}, *tb[2] = {nullptr, nullptr};
     uint32_t *tp[2] = {nullptr, nullptr};
     if (passes > 1) {
-        for (int i = 0; i < 2 && st == BT_OK; i++) {
-            st = ws_alloc((void **)&ta[i], nq * sizeof(K), s);
-            if (st == BT_OK && HAS_B) st = ws_alloc((void **)&tb[i], nq * sizeof(K), s);
-            if (st == BT_OK) st = ws_alloc((void **)&tp[i], nq * sizeof(uint32_t), s);
+        for (int i = 0; i < 2; i++) {
+            ta[i] = reinterpret_cast<K *>(pp);
+            pp += nq * sizeof(K);
+            if (HAS_B) {
+                tb[i] = reinterpret_cast<K *>(pp);
+                pp += nq * sizeof(K);
+            }
+            tp[i] = reinterpret_cast<uint32_t *>(pp);
+            pp += nq * sizeof(uint32_t);
         }
     }
     const size_t smem = (size_t)kPTile * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t) + 1);
     auto scat = part_scatter_kernel<K, HAS_B>;
-    if (st == BT_OK) {
+    static bool attr_done[64] = {};  // per device, per instantiation
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
         cudaError_t e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaFuncSetAttribute");
+        else if (dev >= 0 && dev < 64) attr_done[dev] = true;
     }
     const K *ia = d_a, *ib = d_b;
     const uint32_t *ip = nullptr;
@@ -340,7 +383,7 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
         uint32_t *op = last ? out_perm : tp[p & 1];
         count_launch();
         part_hist_kernel<K, HAS_B><<<(unsigned)ntiles, kPT, 0, s>>>(ia, ib, nq, gp, p, counts, ntiles);
-        st = scan_impl<uint32_t>(counts, counts, ntiles * 256, nullptr, s);
+        st = scan_run<uint32_t>(counts, counts, ncounts, nullptr, scan_ws, s);
         if (st != BT_OK) break;
         count_launch();
         scat<<<(unsigned)ntiles, kPT, smem, s>>>(ia, ib, ip, nq, gp, p, counts, ntiles, oa, ob, op);
@@ -350,12 +393,7 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
         ib = ob;
         ip = op;
     }
-    ws_free(counts, s);
-    for (int i = 0; i < 2; i++) {
-        ws_free(ta[i], s);
-        ws_free(tb[i], s);
-        ws_free(tp[i], s);
-    }
+    ws_free(ws, s);
     return st;
 }
 

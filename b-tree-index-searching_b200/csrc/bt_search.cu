@@ -72,12 +72,20 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     const int grp = lane / G;
     const int gl = lane % G;
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const K tmax = (K)t.max_key;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    // Grouped input (PERM): each CTA takes one contiguous run of warp tiles,
+    // so a CTA works one key range and its warps share node lines in L1.
+    // Ungrouped input: warp tiles are strided over the whole grid.
+    const uint64_t ntiles = (nq + 31) / 32;
+    const uint64_t per_cta = PERM ? (ntiles + gridDim.x - 1) / gridDim.x : 0;
+    const uint64_t t_begin = PERM ? blockIdx.x * per_cta + (threadIdx.x >> 5)
+                                  : (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t t_end = PERM ? min(ntiles, (blockIdx.x + 1) * per_cta) : ntiles;
+    const uint64_t t_step = PERM ? (blockDim.x >> 5) : ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
-    for (uint64_t base = warp * 32; base < nq; base += nwarps * 32) {
+    for (uint64_t tile = t_begin; tile < t_end; tile += t_step) {
+        const uint64_t base = tile * 32;
         // phase 1: one lane per query, binary search of the staged level
         const uint64_t my = base + lane;
         const K myq = my < nq ? q[my] : (K)0;
@@ -182,12 +190,18 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
     const int grp = lane / G;
     const int gl = lane % G;
     uint64_t *res = reinterpret_cast<uint64_t *>(smem_raw + scratch_offset(t)) + (threadIdx.x >> 5) * 64;
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     const K tmax = (K)t.max_key;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    // tile assignment as in point_kernel (CTA-blocked for grouped input)
+    const uint64_t ntiles = (nq + 31) / 32;
+    const uint64_t per_cta = PERM ? (ntiles + gridDim.x - 1) / gridDim.x : 0;
+    const uint64_t t_begin = PERM ? blockIdx.x * per_cta + (threadIdx.x >> 5)
+                                  : (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t t_end = PERM ? min(ntiles, (blockIdx.x + 1) * per_cta) : ntiles;
+    const uint64_t t_step = PERM ? (blockDim.x >> 5) : ((uint64_t)gridDim.x * blockDim.x) >> 5;
 
-    for (uint64_t base = warp * 32; base < nq; base += nwarps * 32) {
+    for (uint64_t tile = t_begin; tile < t_end; tile += t_step) {
+        const uint64_t base = tile * 32;
         const uint64_t my = base + lane;
         const bool v = my < nq;
         const K a = v ? lo[my] : (K)0;
@@ -265,7 +279,8 @@ __global__ void fill_kernel(V *out, uint64_t n, V v) {
 std::mutex g_occ_mu;
 std::map<std::pair<const void *, size_t>, int> g_occ;
 
-// Resident CTAs per SM for a kernel at a given dynamic shared memory size.
+// Resident CTAs per SM for a kernel at a given dynamic shared memory size
+// (all devices this library runs on are B200s of one kind).
 int occupancy(const void *fn, size_t smem) {
     std::lock_guard<std::mutex> lk(g_occ_mu);
     auto key = std::make_pair(fn, smem);
@@ -286,16 +301,21 @@ unsigned persistent_grid(const void *fn, size_t smem, uint64_t work_items, uint6
     return (unsigned)(want < 1 ? 1 : want);
 }
 
+// Raises a kernel's dynamic shared-memory limit when needed (function
+// attributes are per device; the largest size set so far is remembered).
 template <typename Fn>
 bt_status set_smem(Fn fn, size_t smem) {
     static std::mutex mu;
-    static std::map<const void *, size_t> done;
+    static std::map<std::pair<int, const void *>, size_t> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lk(mu);
-    auto it = done.find((const void *)fn);
+    const auto key = std::make_pair(dev, (const void *)fn);
+    auto it = done.find(key);
     if (it != done.end() && it->second >= smem) return BT_OK;
     if (smem > 48 * 1024)
         BT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    done[(const void *)fn] = smem;
+    done[key] = smem;
     return BT_OK;
 }
 
