@@ -83,6 +83,7 @@ _PROTOS = {
     "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
     "bt_kernel_launches": (ctypes.c_uint64, []),
     "bt_set_search_config": (_I, [_P, _I, _I]),
+    "bt_point_search_grouped_noalloc": (_I, [_P, _P, _U64, _P, _P]),
 }
 
 

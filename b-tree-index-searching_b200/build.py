@@ -23,6 +23,7 @@ SOURCES = [
     "bt_group.cu",
     "bt_capi.cu",
     "bt_compat.cu",
+    "bt_noalloc.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -397,6 +397,33 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
     return st;
 }
 
+// Single-pass point partition into caller-provided memory (no allocation):
+// counts and scan scratch come from `ws` (partition_ws_bytes bytes).
+template <typename K>
+bt_status partition_point_prealloc(const bt_tree *t, const K *d_q, uint64_t nq, K *out_q,
+                                   uint32_t *out_perm, unsigned char *ws, cudaStream_t s) {
+    GroupKeyParams gp;
+    gp.kind = kPartPoint;
+    gp.cbits = kPointGroupBits;
+    gp.shift = std::max(0, bitlen64(t->max_key) - gp.cbits);
+    const uint64_t ntiles = (nq + kPTile - 1) / kPTile;
+    const uint64_t ncounts = ntiles * 256;
+    uint32_t *counts = reinterpret_cast<uint32_t *>(ws);
+    uint32_t *scan_ws = counts + ncounts;
+    const size_t smem = (size_t)kPTile * (sizeof(K) + sizeof(uint32_t) + 1);
+    auto scat = part_scatter_kernel<K, false>;
+    BT_CUDA(cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    count_launch();
+    part_hist_kernel<K, false><<<(unsigned)ntiles, kPT, 0, s>>>(d_q, nullptr, nq, gp, 0, counts, ntiles);
+    bt_status st = scan_run<uint32_t>(counts, counts, ncounts, nullptr, scan_ws, s);
+    if (st != BT_OK) return st;
+    count_launch();
+    scat<<<(unsigned)ntiles, kPT, smem, s>>>(d_q, nullptr, nullptr, nq, gp, 0, counts, ntiles, out_q,
+                                             nullptr, out_perm);
+    BT_CUDA(cudaGetLastError());
+    return BT_OK;
+}
+
 // --------------------------------------------------------- range fill ----
 
 // One warp per query: ids[off .. off+cnt) = values of positions lb .. lb+cnt
@@ -482,6 +509,22 @@ bt_status launch_partition(const bt_tree *t, int kind, const void *d_a, const vo
                                                (uint64_t *)d_out_b, d_perm, s)
               : partition_impl<uint64_t, false>(t, kind, (const uint64_t *)d_a, nullptr, nq,
                                                 (uint64_t *)d_out_a, nullptr, d_perm, s);
+}
+
+size_t partition_point_ws_bytes(uint64_t nq) {
+    const uint64_t ncounts = ((nq + kPTile - 1) / kPTile) * 256;
+    return (ncounts + scan_ws_elems(ncounts)) * sizeof(uint32_t);
+}
+
+bt_status launch_partition_point_prealloc(const bt_tree *t, const void *d_q, uint64_t nq,
+                                          void *out_q, uint32_t *out_perm, void *ws,
+                                          cudaStream_t s) {
+    if (nq == 0) return BT_OK;
+    if (t->key_bytes == 4)
+        return partition_point_prealloc<uint32_t>(t, (const uint32_t *)d_q, nq, (uint32_t *)out_q,
+                                                  out_perm, (unsigned char *)ws, s);
+    return partition_point_prealloc<uint64_t>(t, (const uint64_t *)d_q, nq, (uint64_t *)out_q,
+                                              out_perm, (unsigned char *)ws, s);
 }
 
 bt_status launch_scan_u64(const uint64_t *d_in, uint64_t *d_out, uint64_t n, uint64_t *d_total,

@@ -134,6 +134,12 @@ bt_status launch_partition(const bt_tree *t, int kind, const void *d_a, const vo
                            cudaStream_t s);
 bt_status launch_scan_u64(const uint64_t *d_in, uint64_t *d_out, uint64_t n, uint64_t *d_total,
                           cudaStream_t s);
+// Point-query partition into caller memory: ws must hold
+// partition_point_ws_bytes(nq) bytes; nothing is allocated.
+size_t partition_point_ws_bytes(uint64_t nq);
+bt_status launch_partition_point_prealloc(const bt_tree *t, const void *d_q, uint64_t nq,
+                                          void *out_q, uint32_t *out_perm, void *ws,
+                                          cudaStream_t s);
 bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
                             const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
 

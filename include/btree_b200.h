@@ -156,6 +156,21 @@ BT_API bt_status bt_point_search_grouped_batch(const bt_tree *tree, const void *
                                                void *stream);
 
 /*
+ * Grouped point search that allocates no device memory (no counterpart in
+ * the reference).  Same results as bt_point_search(BT_POINT_GROUPED), for
+ * callers that cannot let a library allocate -- a process whose device
+ * memory is reserved by its own allocator, or a latency-critical path where
+ * an allocation could block.  Its scratch is a fixed 4 MiB array inside the
+ * library (present on every GPU that loads it, until exit), so nq is limited
+ * to 262144 per call (larger batches: BT_ERR_INVALID_ARGUMENT).  All calls on
+ * a device share that array: calls that overlap on the GPU race.  The first
+ * call on each device looks up the array's address; make it before any
+ * stream capture.
+ */
+BT_API bt_status bt_point_search_grouped_noalloc(const bt_tree *tree, const void *d_queries,
+                                                 uint64_t nq, void *d_out, void *stream);
+
+/*
  * Range count over inclusive intervals [d_lo[i], d_hi[i]]: d_counts[i] = number
  * of keys k with lo <= k <= hi (0 when lo > hi).  Replaces
  * kernelSearchingKeyRangeGroupStateTwo + kernelGenerateSearchResult
