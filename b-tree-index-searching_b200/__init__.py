@@ -61,6 +61,20 @@ class bt_info(ctypes.Structure):
     ]
 
 
+class bt_learned_config(ctypes.Structure):
+    _fields_ = [("num_segments", ctypes.c_uint32), ("hidden", ctypes.c_uint32),
+                ("iterations", ctypes.c_uint32), ("sample_stride", ctypes.c_uint32),
+                ("learning_rate", ctypes.c_float)]
+
+
+class bt_learned_report(ctypes.Structure):
+    _fields_ = [("root_loss_initial", ctypes.c_float), ("root_loss_final", ctypes.c_float),
+                ("num_segments", ctypes.c_uint32), ("model_level", ctypes.c_uint32),
+                ("keys_per_entry", ctypes.c_uint64), ("eps_mean", ctypes.c_double),
+                ("eps_max", ctypes.c_uint64), ("window_lines_mean", ctypes.c_double),
+                ("train_ms", ctypes.c_double)]
+
+
 _lib = None
 
 _P = ctypes.c_void_p
@@ -84,6 +98,11 @@ _PROTOS = {
     "bt_kernel_launches": (ctypes.c_uint64, []),
     "bt_set_search_config": (_I, [_P, _I, _I]),
     "bt_point_search_grouped_noalloc": (_I, [_P, _P, _U64, _P, _P]),
+    "bt_learned_train": (_I, [_P, ctypes.POINTER(bt_learned_config), _P,
+                              ctypes.POINTER(bt_learned_report)]),
+    "bt_point_search_learned": (_I, [_P, _P, _U64, _P, _P]),
+    "bt_learned_last_stats": (_I, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "bt_mlp_loss_grad": (_I, [_P, ctypes.c_uint32, _P, _P, _U64, _P, _P, _P]),
 }
 
 
@@ -223,6 +242,35 @@ class Tree:
                                       out.ctypes.data_as(_P), _stream_ptr(stream)),
                "bt_point_search_host")
         return out
+
+    # -- learned position model -------------------------------------------
+    def learned_train(self, num_segments=65536, hidden=16, iterations=400, sample_stride=0,
+                      learning_rate=0.01, stream=None):
+        """Train the two-stage model on this tree's keys; returns the report
+        as a dict (losses, error bounds, window size, training time)."""
+        cfg = bt_learned_config(num_segments, hidden, iterations, sample_stride, learning_rate)
+        rep = bt_learned_report()
+        _check(lib().bt_learned_train(self._h, ctypes.byref(cfg), _stream_ptr(stream),
+                                      ctypes.byref(rep)), "bt_learned_train")
+        return {k: getattr(rep, k) for k, _ in bt_learned_report._fields_}
+
+    def point_search_learned(self, queries, out=None, stream=None):
+        """Point search through the learned model (same results as point_search)."""
+        import torch
+        n = len(queries)
+        if out is None:
+            out = torch.empty(n, dtype=_torch_dtype(self.value_bytes), device=queries.device)
+        _check(lib().bt_point_search_learned(self._h, _P(queries.data_ptr()), n,
+                                             _P(out.data_ptr()), _stream_ptr(stream)),
+               "bt_point_search_learned")
+        return out
+
+    def learned_last_stats(self):
+        """(queries answered through the model window, queries that fell back)."""
+        w, f = _U64(), _U64()
+        _check(lib().bt_learned_last_stats(self._h, ctypes.byref(w), ctypes.byref(f)),
+               "bt_learned_last_stats")
+        return w.value, f.value
 
     def group(self, queries, stream=None):
         """The grouping step alone: (grouped queries, caller index per slot)."""

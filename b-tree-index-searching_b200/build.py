@@ -24,6 +24,7 @@ SOURCES = [
     "bt_capi.cu",
     "bt_compat.cu",
     "bt_noalloc.cu",
+    "bt_learned.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -173,6 +173,7 @@ bt_status build_k(bt_tree *t, const void *dk, const void *dv, cudaStream_t s) {
 
 void free_tree(bt_tree *t) {
     if (!t) return;
+    if (t->learned) free_learned(t->learned);
     if (t->d_leaves) cudaFree(t->d_leaves);
     if (t->d_seps) cudaFree(t->d_seps);
     delete t;

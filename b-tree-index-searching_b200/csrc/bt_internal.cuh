@@ -65,6 +65,36 @@ struct DevTree {
     uint32_t smem_bytes;           // bytes staged (a multiple of 16)
 };
 
+// One leaf model of the learned index (32 bytes): the segment's keys are
+// ranks r_lo .. next segment's r_lo - 1; rank ~ r_lo + icpt + slope * (key -
+// base), within eps of the truth for every key of the segment.
+struct SegParam {
+    uint64_t base;
+    float slope;
+    float icpt;
+    uint32_t r_lo;
+    uint32_t eps;
+    uint32_t pad[2];
+};
+
+constexpr int kMaxHidden = 32;
+
+// Device view of a trained learned index.
+struct LearnedDev {
+    const float *mlp;      // 3*hidden+1 root parameters
+    const SegParam *seg;   // num_segments leaf models
+    unsigned long long *stats;  // [windowed, fallback] of the last search
+    uint64_t kmin;
+    float xscale;
+    int hidden;
+    uint32_t nseg;
+    int level;             // separator level scanned in the window
+    uint64_t kpe;          // keys per entry of that level
+    uint64_t level_entries;
+};
+
+struct LearnedState;
+
 }  // namespace bt
 
 struct bt_tree {
@@ -80,8 +110,9 @@ struct bt_tree {
     uint64_t lvl_entries[bt::kMaxLevels];
     uint64_t min_key, max_key;
     int values_sorted;
-    int search_cfg;  // index into the search kernels' (lanes, slots) table
+    int search_cfg;  // index into the search kernels' (lanes, rounds) table
     bt::DevTree dev;
+    bt::LearnedState *learned;  // trained learned index, or null
 };
 
 namespace bt {
@@ -149,6 +180,8 @@ int search_cfg_index(int lanes, int rounds);
 int default_search_cfg(int key_bytes);
 int search_cfg_lanes(int cfg);
 int search_cfg_rounds(int cfg);
+
+void free_learned(bt::LearnedState *s);
 
 // Partition kinds for launch_partition.
 enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2 };

@@ -198,6 +198,72 @@ BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *
                               const void *h_hi, uint64_t nq, uint64_t *h_counts,
                               void *stream);
 
+/* ---- learned position model (north-star extension; the reference has no
+ * counterpart: its descent is always the page walk of
+ * BPTreeExactSearch.cu:39-68) ------------------------------------------ */
+
+/*
+ * A two-stage FP32 model over the tree's (key, rank) pairs:
+ *  - root: a monotone MLP x -> y (1 input, `hidden` ReLU units, 1 output;
+ *    input weights and output weights kept >= 0), x the key normalised to
+ *    [0, 1], y the rank normalised to [0, 1); it routes a key to one of
+ *    `num_segments` leaf models (segment = floor(y * num_segments)).  Trained
+ *    on the GPU by full-batch gradient descent (Adam) on MSE with this
+ *    library's own forward/backward kernels, on every `sample_stride`-th key;
+ *  - leaves: per segment, rank = segment's first rank + intercept + slope *
+ *    (key - segment's first key), fitted by least squares on the GPU; its max
+ *    error eps over the segment's keys is computed exactly with the same FP32
+ *    arithmetic the search uses.
+ * The search predicts a rank window and scans it on the separator level one
+ * above the bottom (one separator per leaf node), then descends normally;
+ * a query whose lower bound is not provably inside the window takes the
+ * full tree descent, so results never depend on the model (the tree stays
+ * both the fallback and the judge).
+ */
+typedef struct bt_learned_config {
+    uint32_t num_segments;  /* leaf models (default 65536) */
+    uint32_t hidden;        /* root hidden units, 1..32 (default 16) */
+    uint32_t iterations;    /* root training steps (default 400) */
+    uint32_t sample_stride; /* train the root on every k-th key (default: n / 2^20) */
+    float learning_rate;    /* Adam step size (default 0.01) */
+} bt_learned_config;
+
+typedef struct bt_learned_report {
+    float root_loss_initial;  /* MSE of the root before training */
+    float root_loss_final;    /* ... and after */
+    uint32_t num_segments;
+    uint32_t model_level;     /* separator level the window is scanned on */
+    uint64_t keys_per_entry;  /* keys under one separator of that level */
+    double eps_mean;          /* mean segment error bound, in keys */
+    uint64_t eps_max;
+    double window_lines_mean; /* mean 128-byte lines a window spans */
+    double train_ms;          /* device time of the whole training */
+} bt_learned_report;
+
+/* Train the model for `tree` (replacing a previous one).  cfg may be NULL
+ * for defaults; report may be NULL.  Synchronizes `stream`. */
+BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, void *stream,
+                                  bt_learned_report *report);
+
+/* Point search through the learned model (same results as bt_point_search).
+ * BT_ERR_INVALID_ARGUMENT if the tree has no trained model. */
+BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
+                                         void *d_out, void *stream);
+
+/* Counters of the last learned search on this tree: queries answered through
+ * the window and queries that took the full descent. */
+BT_API bt_status bt_learned_last_stats(const bt_tree *tree, uint64_t *windowed, uint64_t *fallback);
+
+/*
+ * The root model's training kernels, exposed so their gradients can be
+ * checked: for params p (3*hidden+1 floats: w1[hidden], b1[hidden],
+ * w2[hidden], b2) and n points (x[i], y[i]) in device memory, writes
+ * loss = mean((f(x)-y)^2) to d_loss[0] and dloss/dp to d_grad (device).
+ */
+BT_API bt_status bt_mlp_loss_grad(const float *d_params, uint32_t hidden, const float *d_x,
+                                  const float *d_y, uint64_t n, float *d_loss, float *d_grad,
+                                  void *stream);
+
 /* Number of kernel launches this library has issued in this process (all
  * devices, all threads).  Lets a caller count the device work behind a call. */
 BT_API uint64_t bt_kernel_launches(void);
