@@ -25,9 +25,9 @@ def test_mlp_gradient_kernel_matches_cpu(bt, cuda, H):
     loss_d = torch.zeros(1, dtype=torch.float32, device=cuda)
     grad_d = torch.zeros(3 * H + 1, dtype=torch.float32, device=cuda)
     P = ctypes.c_void_p
-    st = bt.lib().bt_mlp_loss_grad(P(dev(p, cuda).data_ptr()), H, P(dev(x, cuda).data_ptr()),
-                                   P(dev(y, cuda).data_ptr()), n, P(loss_d.data_ptr()),
-                                   P(grad_d.data_ptr()),
+    dp, dx, dy = dev(p, cuda), dev(x, cuda), dev(y, cuda)  # keep the buffers alive
+    st = bt.lib().bt_mlp_loss_grad(P(dp.data_ptr()), H, P(dx.data_ptr()), P(dy.data_ptr()), n,
+                                   P(loss_d.data_ptr()), P(grad_d.data_ptr()),
                                    P(torch.cuda.current_stream().cuda_stream))
     assert st == 0
     torch.cuda.synchronize()
