@@ -75,6 +75,18 @@ class bt_learned_report(ctypes.Structure):
                 ("train_ms", ctypes.c_double)]
 
 
+class bt_server_config(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("memory_budget_bytes", ctypes.c_uint64),
+                ("max_batch", ctypes.c_uint32), ("mode", ctypes.c_int32)]
+
+
+class bt_server_stats(ctypes.Structure):
+    _fields_ = [("slots", ctypes.c_uint32), ("max_in_flight", ctypes.c_uint32),
+                ("completed", ctypes.c_uint64), ("jobs", ctypes.c_uint64)]
+
+
+SERVE_MODES = {"basic": 0, "grouped": 1, "learned": 2}
+
 _lib = None
 
 _P = ctypes.c_void_p
@@ -103,6 +115,12 @@ _PROTOS = {
     "bt_point_search_learned": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_last_stats": (_I, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "bt_mlp_loss_grad": (_I, [_P, ctypes.c_uint32, _P, _P, _U64, _P, _P, _P]),
+    "bt_server_create": (_I, [_P, ctypes.POINTER(bt_server_config), ctypes.POINTER(_P)]),
+    "bt_server_submit": (_I, [_P, _P, _U64, _P, ctypes.POINTER(_U64)]),
+    "bt_server_wait": (_I, [_P, _U64, ctypes.POINTER(ctypes.c_double)]),
+    "bt_server_get_stats": (_I, [_P, ctypes.POINTER(bt_server_stats)]),
+    "bt_server_destroy": (_I, [_P]),
+    "bt_server_replay": (_I, [_P, _U64, _P, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
 }
 
 
@@ -342,6 +360,81 @@ class Tree:
                                  ids_capacity, ctypes.byref(total), _stream_ptr(stream)),
                "bt_range_search")
         return counts, offsets, ids[: total.value]
+
+
+class Server:
+    """Continuous-batching request loop over one tree (see bt_server_create).
+    Requests are numpy arrays; keep them (and the outputs) alive until done."""
+
+    def __init__(self, tree, mode="basic", slots=8, memory_budget_bytes=256 << 20,
+                 max_batch=65536):
+        self.tree = tree
+        cfg = bt_server_config(slots, memory_budget_bytes, max_batch, SERVE_MODES[mode])
+        h = ctypes.c_void_p()
+        _check(lib().bt_server_create(tree.handle, ctypes.byref(cfg), ctypes.byref(h)),
+               "bt_server_create")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, queries, out=None):
+        """Queue one request; returns (ticket, out array)."""
+        queries = np.ascontiguousarray(queries)
+        if out is None:
+            out = np.empty(len(queries), dtype=np.uint32 if self.tree.value_bytes == 4 else np.uint64)
+        t = _U64()
+        _check(lib().bt_server_submit(self._h, queries.ctypes.data_as(_P), len(queries),
+                                      out.ctypes.data_as(_P), ctypes.byref(t)), "bt_server_submit")
+        self._keep[t.value] = (queries, out)
+        return t.value, out
+
+    def wait(self, ticket):
+        """Block until answered; returns the latency in microseconds."""
+        lat = ctypes.c_double()
+        _check(lib().bt_server_wait(self._h, ticket, ctypes.byref(lat)), "bt_server_wait")
+        self._keep.pop(ticket, None)
+        return lat.value
+
+    def stats(self):
+        s = bt_server_stats()
+        _check(lib().bt_server_get_stats(self._h, ctypes.byref(s)), "bt_server_get_stats")
+        return {k: getattr(s, k) for k, _ in bt_server_stats._fields_}
+
+    def replay(self, queries, arrival_us, outs=None):
+        """Submit each request at its arrival time (us after start), wait for
+        all; returns (latencies_us array, wall_us, outs)."""
+        n = len(queries)
+        queries = [np.ascontiguousarray(q) for q in queries]
+        if outs is None:
+            vt = np.uint32 if self.tree.value_bytes == 4 else np.uint64
+            outs = [np.empty(len(q), dtype=vt) for q in queries]
+        nq = (ctypes.c_uint64 * n)(*[len(q) for q in queries])
+        qp = (ctypes.c_void_p * n)(*[q.ctypes.data for q in queries])
+        op = (ctypes.c_void_p * n)(*[o.ctypes.data for o in outs])
+        arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        lat = np.empty(n, dtype=np.float64)
+        wall = ctypes.c_double()
+        _check(lib().bt_server_replay(self._h, n, nq, qp, op, arr.ctypes.data_as(_P),
+                                      lat.ctypes.data_as(_P), ctypes.byref(wall)),
+               "bt_server_replay")
+        return lat, wall.value, outs
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().bt_server_destroy(self._h)
+        self._h = None
+        self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def version():

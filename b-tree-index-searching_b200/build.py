@@ -25,6 +25,7 @@ SOURCES = [
     "bt_compat.cu",
     "bt_noalloc.cu",
     "bt_learned.cu",
+    "bt_server.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -48,6 +48,11 @@ def parse_args(argv=None):
     p.add_argument("--queries-log2", type=int, default=24)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-log2", type=int, default=22)
+    p.add_argument("--no-learned", action="store_true",
+                   help="skip the learned-index + serving section (2^28 u64 keys)")
+    p.add_argument("--learned-keys-log2", type=int, default=28)
+    p.add_argument("--serve-requests", type=int, default=3000)
+    p.add_argument("--serve-rate", type=float, default=20000.0, help="requests per second")
     return p.parse_args(argv)
 
 
@@ -253,6 +258,110 @@ def run_reference(args):
     return 0
 
 
+# ------------------------------------------ learned index + serving --------
+
+def learned_section(args, device, bt, flush):
+    """2^28 unique u64 keys (cumulative sum of
+    floor(lognormal(4, 2)) + 1 gaps), value = rank; FP32 two-stage model with
+    2^16 leaf segments trained on the GPU.  Reports the plain and the learned
+    batched point-search throughput on a 2^24-query batch (90% hits uniform
+    over ranks, 10% uniform in [min, max]) and p50/p99 latency of a Poisson
+    request loop with batch sizes round(2^U), U ~ uniform[0, 16]."""
+    import torch
+    wl = importlib.import_module(PKG + ".workloads")
+    at = importlib.import_module(PKG + ".autotune")
+    n = 1 << args.learned_keys_log2
+    keys = wl.lognormal_keys(n)
+    vals = np.arange(n, dtype=np.uint64)
+    g = wl.rng(wl.KEY_SEED + 7)
+    nq = 1 << args.queries_log2
+    q = keys[g.integers(0, n, size=nq)]
+    miss = g.random(nq) < 0.10
+    q[miss] = g.integers(int(keys[0]), int(keys[-1]) + 1, size=int(miss.sum()), dtype=np.uint64)
+    stream = torch.cuda.current_stream(device)
+    tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
+    rep = tree.learned_train(num_segments=1 << 16, hidden=16, iterations=400)
+    dq = torch.from_numpy(q).to(device)
+    out = torch.empty(nq, dtype=torch.uint64, device=device)
+
+    def timed(fn, steps):
+        ts = []
+        for _ in range(steps):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.mean(ts)
+
+    lanes_p, rounds_p, _ = at.tune(tree, dq, mode="basic", repeats=3)
+    plain_ms = timed(lambda: tree.point_search(dq, mode="basic", out=out, stream=stream), args.steps)
+    plain_res = out.cpu().numpy()
+    learned_ms = {}
+    for cfg in tree.SEARCH_CONFIGS:  # the autotuner's choice for the learned kernel
+        tree.set_search_config(*cfg)
+        learned_ms[cfg] = timed(lambda: tree.point_search_learned(dq, out=out, stream=stream), 2)
+    best = min(learned_ms, key=learned_ms.get)
+    tree.set_search_config(*best)
+    l_ms = timed(lambda: tree.point_search_learned(dq, out=out, stream=stream), args.steps)
+    learned_res = out.cpu().numpy()
+    windowed, fallback = tree.learned_last_stats()
+    hits = int(np.count_nonzero(learned_res != np.uint64(0xFFFFFFFFFFFFFFFF)))
+    from oracle.oracle import Oracle
+    sample = slice(0, 1 << 20)
+    exact = bool(np.array_equal(learned_res, plain_res)) and bool(
+        np.array_equal(learned_res[sample], Oracle().point_search(keys, vals, q[sample])))
+    alg = nq * (8 + 8 + 32) + hits * 32
+    peak, _ = measured_peak()
+
+    # request loop: Poisson arrivals, log-uniform batch sizes, pinned buffers
+    sizes = np.rint(2.0 ** g.uniform(0, 16, size=args.serve_requests)).astype(np.int64)
+    reqs = []
+    for m in sizes:
+        r = keys[g.integers(0, n, size=m)]
+        mm = g.random(m) < 0.10
+        r[mm] = g.integers(int(keys[0]), int(keys[-1]) + 1, size=int(mm.sum()), dtype=np.uint64)
+        reqs.append(torch.from_numpy(r).pin_memory().numpy())
+    outs = [torch.empty(len(r), dtype=torch.uint64).pin_memory().numpy() for r in reqs]
+    arrivals = np.cumsum(g.exponential(1e6 / args.serve_rate, size=len(reqs)))
+    serving = {}
+    for mode in ("basic", "learned"):
+        tree.set_search_config(*(best if mode == "learned" else (lanes_p, rounds_p)))
+        with bt.Server(tree, mode=mode, slots=8, memory_budget_bytes=512 << 20) as srv:
+            srv.replay(reqs[:200], arrivals[:200] - arrivals[0], outs[:200])  # warm-up
+            lat, wall, _ = srv.replay(reqs, arrivals - arrivals[0], outs)
+            st = srv.stats()
+        serving[mode] = {"p50_us": float(np.percentile(lat, 50)),
+                         "p99_us": float(np.percentile(lat, 99)),
+                         "mean_us": float(lat.mean()),
+                         "queries_per_s": float(sizes.sum() / (wall / 1e6)),
+                         "max_in_flight": st["max_in_flight"], "slots": st["slots"]}
+    tree.close()
+    return {
+        "workload": (f"2^{args.learned_keys_log2} unique u64 keys = cumsum(floor(lognormal(4,2))+1), "
+                     f"value = rank; batch of 2^{args.queries_log2} queries, 90% hits uniform over "
+                     "ranks, 10% uniform in [min, max]"),
+        "plain": {"value": nq / (plain_ms / 1e3), "unit": "queries/s", "ms": plain_ms,
+                  "lanes_per_query": lanes_p, "rounds": rounds_p},
+        "learned": {"value": nq / (l_ms / 1e3), "unit": "queries/s", "ms": l_ms,
+                    "lanes_per_query": best[0], "rounds": best[1],
+                    "windowed": windowed, "fallback": fallback,
+                    "roofline": {"bound": "hbm", "achieved": alg / (l_ms / 1e3) / 1e9,
+                                 "peak": peak, "unit": "GB/s",
+                                 "frac": alg / (l_ms / 1e3) / 1e9 / peak}},
+        "learned_over_plain": plain_ms / l_ms,
+        "exact": exact,
+        "model": {k: rep[k] for k in ("root_loss_initial", "root_loss_final", "eps_mean",
+                                      "eps_max", "window_lines_mean", "train_ms",
+                                      "keys_per_entry")},
+        "serving": {"requests": int(len(reqs)), "rate_per_s": args.serve_rate,
+                    "batch_sizes": "round(2^U), U ~ uniform[0,16]", **serving},
+    }
+
+
 # ------------------------------------------------------------ GPU leg -------
 
 def run_ours(args):
@@ -376,6 +485,10 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
 
+    learned = None
+    if world == 1 and not args.no_learned:
+        learned = learned_section(args, device, bt, flush)
+
     line = None
     if rank == 0:
         cpu = None
@@ -414,6 +527,7 @@ def run_ours(args):
                          "basic": {"lanes_per_query": b_lanes, "queries_per_group": b_slots,
                                    "ms": b_ms}},
             "checked_vs_oracle": checked,
+            "learned_index": learned,
         }
         print(json.dumps(line), flush=True)
     tree.close()

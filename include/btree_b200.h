@@ -264,6 +264,60 @@ BT_API bt_status bt_mlp_loss_grad(const float *d_params, uint32_t hidden, const 
                                   const float *d_y, uint64_t n, float *d_loss, float *d_grad,
                                   void *stream);
 
+/* ---- continuous-batching request loop (north-star extension; the reference
+ * runs one synchronous batch per host call, BPTreeExactSearch.cu:409-484) */
+
+typedef struct bt_server bt_server;
+
+typedef enum bt_serve_mode {
+    BT_SERVE_BASIC = 0,   /* bt_point_search basic */
+    BT_SERVE_GROUPED = 1, /* bt_point_search grouped */
+    BT_SERVE_LEARNED = 2  /* bt_point_search_learned (needs a trained model) */
+} bt_serve_mode;
+
+typedef struct bt_server_config {
+    uint32_t slots;               /* concurrent device jobs wanted (default 8) */
+    uint64_t memory_budget_bytes; /* device memory for job buffers (default 256 MiB) */
+    uint32_t max_batch;           /* queries per job; larger requests are split (default 65536) */
+    int32_t mode;                 /* bt_serve_mode */
+} bt_server_config;
+
+typedef struct bt_server_stats {
+    uint32_t slots;          /* slots the memory budget admitted */
+    uint32_t max_in_flight;  /* most jobs on the device at once so far */
+    uint64_t completed;      /* requests completed */
+    uint64_t jobs;           /* device jobs issued */
+} bt_server_stats;
+
+/*
+ * A server answering point-query requests on one tree.  A worker thread
+ * admits requests chunk by chunk into free slots -- each slot a stream with
+ * its own device buffers, the number of slots bounded by the memory budget --
+ * as soon as one frees up, so requests that arrive while others run are
+ * admitted at once and their copies and kernels overlap on the device.
+ * Host buffers must stay valid until the request completes; pinned host
+ * memory lets the copies run asynchronously.
+ */
+BT_API bt_status bt_server_create(const bt_tree *tree, const bt_server_config *cfg,
+                                  bt_server **out);
+/* Queue a request (non-blocking); *ticket identifies it. */
+BT_API bt_status bt_server_submit(bt_server *srv, const void *h_queries, uint64_t nq, void *h_out,
+                                  uint64_t *ticket);
+/* Block until the request is answered; *latency_us = submit-to-completion
+ * time.  Each ticket can be waited for once. */
+BT_API bt_status bt_server_wait(bt_server *srv, uint64_t ticket, double *latency_us);
+BT_API bt_status bt_server_get_stats(bt_server *srv, bt_server_stats *stats);
+/* Waits for all outstanding work, then frees the server. */
+BT_API bt_status bt_server_destroy(bt_server *srv);
+/*
+ * Load generator: submits nreq requests at their arrival times (arrival_us,
+ * microseconds after the call starts, ascending), waits for all, and fills
+ * latency_us[i]; *wall_us receives the total time.
+ */
+BT_API bt_status bt_server_replay(bt_server *srv, uint64_t nreq, const uint64_t *nq,
+                                  const void *const *h_queries, void *const *h_outs,
+                                  const double *arrival_us, double *latency_us, double *wall_us);
+
 /* Number of kernel launches this library has issued in this process (all
  * devices, all threads).  Lets a caller count the device work behind a call. */
 BT_API uint64_t bt_kernel_launches(void);
