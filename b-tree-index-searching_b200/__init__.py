@@ -115,6 +115,12 @@ _PROTOS = {
     "bt_point_search_learned": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_last_stats": (_I, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "bt_mlp_loss_grad": (_I, [_P, ctypes.c_uint32, _P, _P, _U64, _P, _P, _P]),
+    "bt_forest_build": (_I, [_P, _P, _P, ctypes.c_uint32, _I, _I, _P, ctypes.POINTER(_P)]),
+    "bt_forest_destroy": (_I, [_P]),
+    "bt_forest_plan_create": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, ctypes.c_uint32,
+                                   ctypes.POINTER(_P)]),
+    "bt_forest_plan_run": (_I, [_P, _P]),
+    "bt_forest_plan_destroy": (_I, [_P]),
     "bt_server_create": (_I, [_P, ctypes.POINTER(bt_server_config), ctypes.POINTER(_P)]),
     "bt_server_submit": (_I, [_P, _P, _U64, _P, ctypes.POINTER(_U64)]),
     "bt_server_wait": (_I, [_P, _U64, ctypes.POINTER(ctypes.c_double)]),
@@ -360,6 +366,84 @@ class Tree:
                                  ids_capacity, ctypes.byref(total), _stream_ptr(stream)),
                "bt_range_search")
         return counts, offsets, ids[: total.value]
+
+
+class Forest:
+    """Many independent trees built and searched together (bt_forest_*)."""
+
+    def __init__(self, keys, values, offsets, stream=None):
+        """keys/values: CUDA tensors holding every tree's sorted keys back to
+        back; offsets: numpy u64 array of num_trees+1 boundaries."""
+        off = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self.num_trees = len(off) - 1
+        self.key_bytes, self.value_bytes = keys.element_size(), values.element_size()
+        keys, values = keys.contiguous(), values.contiguous()
+        h = ctypes.c_void_p()
+        _check(lib().bt_forest_build(_P(keys.data_ptr()), _P(values.data_ptr()),
+                                     off.ctypes.data_as(_P), self.num_trees, self.key_bytes,
+                                     self.value_bytes, _stream_ptr(stream), ctypes.byref(h)),
+               "bt_forest_build")
+        self._h = h
+
+    def plan(self, queries, q_offsets, out, lo=None, hi=None, r_offsets=None, counts=None,
+             lanes_per_query=4, rounds=1, tile=1024):
+        return ForestPlan(self, queries, q_offsets, out, lo, hi, r_offsets, counts,
+                          lanes_per_query, rounds, tile)
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().bt_forest_destroy(self._h)
+        self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ForestPlan:
+    """A captured forest search (CUDA graph) over fixed buffers."""
+
+    def __init__(self, forest, queries, q_offsets, out, lo, hi, r_offsets, counts, lanes, rounds,
+                 tile):
+        qo = np.ascontiguousarray(q_offsets, dtype=np.uint64)
+        ro = None if r_offsets is None else np.ascontiguousarray(r_offsets, dtype=np.uint64)
+        self._keep = (forest, queries, out, lo, hi, counts)
+        ptr = lambda t: None if t is None else _P(t.data_ptr())  # noqa: E731
+        h = ctypes.c_void_p()
+        _check(lib().bt_forest_plan_create(forest._h, ptr(queries), qo.ctypes.data_as(_P), ptr(out),
+                                           ptr(lo), ptr(hi),
+                                           None if ro is None else ro.ctypes.data_as(_P),
+                                           ptr(counts), lanes, rounds, tile, ctypes.byref(h)),
+               "bt_forest_plan_create")
+        self._h = h
+
+    def run(self, stream=None):
+        _check(lib().bt_forest_plan_run(self._h, _stream_ptr(stream)), "bt_forest_plan_run")
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            lib().bt_forest_plan_destroy(self._h)
+        self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Server:

@@ -26,6 +26,7 @@ SOURCES = [
     "bt_noalloc.cu",
     "bt_learned.cu",
     "bt_server.cu",
+    "bt_forest.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -66,15 +66,16 @@ struct DevTree {
 };
 
 // One leaf model of the learned index (32 bytes): the segment's keys are
-// ranks r_lo .. next segment's r_lo - 1; rank ~ r_lo + icpt + slope * (key -
-// base), within eps of the truth for every key of the segment.
+// ranks r_lo .. r_lo + cnt - 1; rank ~ r_lo + clamp(icpt + slope * (key -
+// base), 0, cnt), within eps of the truth for every key of the segment.
 struct SegParam {
     uint64_t base;
     float slope;
     float icpt;
     uint32_t r_lo;
     uint32_t eps;
-    uint32_t pad[2];
+    uint32_t cnt;
+    uint32_t pad;
 };
 
 constexpr int kMaxHidden = 32;

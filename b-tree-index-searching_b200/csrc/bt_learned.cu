@@ -68,10 +68,15 @@ __device__ __forceinline__ uint32_t root_segment(const float *p, int H, uint32_t
     return f >= (float)nseg ? nseg - 1 : (uint32_t)f;
 }
 
-// Relative rank predicted by a leaf model for a key (FP32, round to nearest).
+// Relative rank predicted by a leaf model for a key (FP32, round to
+// nearest), clamped to the segment's rank range [0, cnt]: a key in the gap
+// after the segment's last key (lognormal gaps can be 10^6 wide) must not be
+// extrapolated along the line, its lower bound is at most the next segment's
+// first rank.
 __device__ __forceinline__ float leaf_pred(const SegParam &s, uint64_t key) {
     const uint64_t d = key > s.base ? key - s.base : 0ull;
-    return __fadd_rn(s.icpt, __fmul_rn(s.slope, __ull2float_rn(d)));
+    const float p = __fadd_rn(s.icpt, __fmul_rn(s.slope, __ull2float_rn(d)));
+    return fminf(fmaxf(p, 0.f), (float)s.cnt);
 }
 
 template <typename K, typename V>
@@ -191,7 +196,8 @@ __global__ void fit_kernel(const unsigned char *__restrict__ leaves, uint64_t n,
         SegParam sp;
         sp.base = a < n ? (uint64_t)leaf_key<K, V>(leaves, a) : (uint64_t)leaf_key<K, V>(leaves, n - 1);
         sp.r_lo = a;
-        sp.pad[0] = sp.pad[1] = 0;
+        sp.cnt = b - a;
+        sp.pad = 0;
         double sx = 0, sy = 0, sxx = 0, sxy = 0;
         for (uint32_t i = a + lane; i < b; i += 32) {
             const uint64_t k = (uint64_t)leaf_key<K, V>(leaves, i);
@@ -231,7 +237,7 @@ __global__ void fit_kernel(const unsigned char *__restrict__ leaves, uint64_t n,
 // --------------------------------------------------------------- search ---
 
 constexpr int kThreads = 256;
-constexpr int kMaxWindowLines = 4;
+constexpr int kMaxWindowLines = 8;
 
 // Full descent for one query by one thread (the fallback): binary search in
 // each node line from global memory, then the leaf block.
@@ -268,7 +274,6 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     __syncthreads();
 
     using LG = LeafGeom<K, V>;
-    using LS = LeafStage<K, V, G>;
     constexpr int F = kLineBytes / (int)sizeof(K);
     constexpr int KPL = F / G;
     constexpr int NG = 32 / G;
@@ -276,7 +281,6 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int gl = lane % G;
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
     uint8_t *bad = s_bad + (threadIdx.x & ~31);
     const K tmax = (K)t.max_key;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
@@ -364,61 +368,10 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             for (int lvl = m.level + 1; lvl < t.nlevels; lvl++)
                 level_step<K, G, I>(static_cast<const K *>(t.seps) + t.lvl_off[lvl], qe, up, node,
                                     grp, gl);
-            // leaf block, as in point_kernel
-            uint32_t ch[I][LS::CPL][4];
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
-#pragma unroll
-                for (int j = 0; j < LS::CPL; j++) {
-                    const int c = gl + j * G;
-                    if (c < LS::NC) {
-                        const uint4 x = load_stream16(
-                            blk + (c < LS::NKC ? c * 16 : kSectorBytes + (c - LS::NKC) * 16));
-                        ch[s][j][0] = x.x;
-                        ch[s][j][1] = x.y;
-                        ch[s][j][2] = x.z;
-                        ch[s][j][3] = x.w;
-                    }
-                }
-            }
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                int c2 = 0;
-                bool eq = false;
-#pragma unroll
-                for (int j = 0; j < LS::KCPL; j++) {
-                    if (gl + j * G < LS::NKC) {
-                        c2 += count_below<K, LS::KPC>(ch[s][j], qe[s], false);
-#pragma unroll
-                        for (int k = 0; k < LS::KPC; k++) eq |= key_at<K>(ch[s][j], k) == qv[s];
-                    }
-                }
-                const int pos0 = __shfl_sync(0xffffffffu, c2, grp * G) +
-                                 __shfl_sync(0xffffffffu, c2, grp * G + 1);
-                const bool found = (__ballot_sync(0xffffffffu, eq) & gmask) != 0 && qv[s] <= tmax;
-                const int pos = pos0 < LG::S ? pos0 : LG::S - 1;
-                const int vc = LS::NKC + pos / LS::VPC;
+            leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
                 const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                if (gl == vc % G && qi < nq && !sbad[s]) {
-                    V val = 0;
-#pragma unroll
-                    for (int j = 0; j < LS::CPL; j++) {
-                        if (j == vc / G) {
-                            const int w = (pos % LS::VPC) * (int)(sizeof(V) / 4);
-                            if constexpr (sizeof(V) == 4) {
-#pragma unroll
-                                for (int k = 0; k < 4; k++)
-                                    if (k == w) val = ch[s][j][k];
-                            } else {
-                                val = w == 0 ? (((uint64_t)ch[s][j][1] << 32) | ch[s][j][0])
-                                             : (((uint64_t)ch[s][j][3] << 32) | ch[s][j][2]);
-                            }
-                        }
-                    }
-                    out[qi] = found ? val : key_max<V>();
-                }
-            }
+                return (qi < nq && !sbad[s]) ? out + qi : nullptr;
+            });
         }
         __syncwarp();
         // fallback: the owning lane runs the full descent for its own query

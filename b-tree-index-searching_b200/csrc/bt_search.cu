@@ -64,14 +64,11 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     stage_level<K>(s_lvl, t);
     __syncthreads();
 
-    using LG = LeafGeom<K, V>;
-    using LS = LeafStage<K, V, G>;
     constexpr int NG = 32 / G;  // lane groups per warp
     constexpr int I = G / R;    // queries in flight per group and round
     const int lane = threadIdx.x & 31;
     const int grp = lane / G;
     const int gl = lane % G;
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
     const K tmax = (K)t.max_key;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
     // Grouped input (PERM): each CTA takes one contiguous run of warp tiles,
@@ -106,64 +103,11 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
                 up[s] = false;
             }
             walk_global<K, G, I>(t, qe, up, node, grp, gl);
-
-            // the leaf block: key chunks then value chunks, chunk c on lane c % G
-            uint32_t ch[I][LS::CPL][4];
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
-#pragma unroll
-                for (int j = 0; j < LS::CPL; j++) {
-                    const int c = gl + j * G;
-                    if (c < LS::NC) {
-                        const uint4 x = load_stream16(
-                            blk + (c < LS::NKC ? c * 16 : kSectorBytes + (c - LS::NKC) * 16));
-                        ch[s][j][0] = x.x;
-                        ch[s][j][1] = x.y;
-                        ch[s][j][2] = x.z;
-                        ch[s][j][3] = x.w;
-                    }
-                }
-            }
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                int cnt = 0;
-                bool eq = false;
-#pragma unroll
-                for (int j = 0; j < LS::KCPL; j++) {
-                    if (gl + j * G < LS::NKC) {
-                        cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], false);
-#pragma unroll
-                        for (int k = 0; k < LS::KPC; k++) eq |= key_at<K>(ch[s][j], k) == qv[s];
-                    }
-                }
-                const int pos0 = __shfl_sync(0xffffffffu, cnt, grp * G) +
-                                 __shfl_sync(0xffffffffu, cnt, grp * G + 1);
-                const bool found =
-                    (__ballot_sync(0xffffffffu, eq) & gmask) != 0 && qv[s] <= tmax;  // pad keys are all-ones
-                const int pos = pos0 < LG::S ? pos0 : LG::S - 1;
-                const int vc = LS::NKC + pos / LS::VPC;  // chunk holding the value
+            leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
                 const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                if (gl == vc % G && qi < nq) {
-                    V val = 0;
-#pragma unroll
-                    for (int j = 0; j < LS::CPL; j++) {
-                        if (j == vc / G) {
-                            const int w = (pos % LS::VPC) * (int)(sizeof(V) / 4);
-                            if constexpr (sizeof(V) == 4) {
-#pragma unroll
-                                for (int k = 0; k < 4; k++)
-                                    if (k == w) val = ch[s][j][k];
-                            } else {
-                                val = w == 0 ? (((uint64_t)ch[s][j][1] << 32) | ch[s][j][0])
-                                             : (((uint64_t)ch[s][j][3] << 32) | ch[s][j][2]);
-                            }
-                        }
-                    }
-                    const uint64_t dst = PERM ? (uint64_t)perm[qi] : qi;
-                    out[dst] = found ? val : key_max<V>();
-                }
-            }
+                if (qi >= nq) return nullptr;
+                return out + (PERM ? (uint64_t)perm[qi] : qi);
+            });
         }
     }
 }
@@ -183,7 +127,6 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
     __syncthreads();
 
     using LG = LeafGeom<K, V>;
-    using LS = LeafStage<K, V, G>;
     constexpr int NG = 32 / G;
     constexpr int I = G / R;
     const int lane = threadIdx.x & 31;
@@ -228,33 +171,13 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
                 up[s] = which ? __shfl_sync(0xffffffffu, ub_upper, k) : false;
             }
             walk_global<K, G, I>(t, qe, up, node, grp, gl);
-            uint32_t ch[I][LS::KCPL][4];
+            int pos[I];
+            leaf_bound<K, V, G, I>(leaves, node, qe, up, grp, gl, pos);
 #pragma unroll
-            for (int s = 0; s < I; s++) {
-                const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
-#pragma unroll
-                for (int j = 0; j < LS::KCPL; j++) {
-                    const int c = gl + j * G;
-                    if (c < LS::NKC) {
-                        const uint4 x = load_stream16(blk + c * 16);
-                        ch[s][j][0] = x.x;
-                        ch[s][j][1] = x.y;
-                        ch[s][j][2] = x.z;
-                        ch[s][j][3] = x.w;
-                    }
-                }
-            }
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                int cnt = 0;
-#pragma unroll
-                for (int j = 0; j < LS::KCPL; j++)
-                    if (gl + j * G < LS::NKC) cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], up[s]);
-                const int pos = __shfl_sync(0xffffffffu, cnt, grp * G) +
-                                __shfl_sync(0xffffffffu, cnt, grp * G + 1);
-                if (gl == 0) res[(which ? 32 : 0) + (r % R) * (NG * I) + s * NG + grp] =
-                    (uint64_t)node[s] * LG::S + pos;
-            }
+            for (int s = 0; s < I; s++)
+                if (gl == 0)
+                    res[(which ? 32 : 0) + (r % R) * (NG * I) + s * NG + grp] =
+                        (uint64_t)node[s] * LG::S + pos[s];
         }
         __syncwarp();
         if (v) {

@@ -183,4 +183,118 @@ struct LeafStage {
     static constexpr int KCPL = (NKC + G - 1) / G;       // key chunks per lane
 };
 
+// Leaf stage of I point queries.  Each query's leaf block (key chunks, then
+// value chunks) is loaded by its lane group with 16-byte streaming loads, the
+// lower-bound slot and the match are found, and the lane holding the value
+// writes it -- or all-ones on a miss -- to dst(s); dst returns null to skip
+// a slot.  leaves points at leaf block 0 of the tree; node[s] is the block.
+template <typename K, typename V, int G, int I, typename Dst>
+__device__ __forceinline__ void leaf_point(const unsigned char *__restrict__ leaves,
+                                           const uint32_t (&node)[I], const K (&qv)[I],
+                                           const K (&qe)[I], K tmax, int grp, int gl, Dst dst) {
+    using LG = LeafGeom<K, V>;
+    using LS = LeafStage<K, V, G>;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
+    uint32_t ch[I][LS::CPL][4];
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
+#pragma unroll
+        for (int j = 0; j < LS::CPL; j++) {
+            const int c = gl + j * G;
+            if (c < LS::NC) {
+                const uint4 x =
+                    load_stream16(blk + (c < LS::NKC ? c * 16 : kSectorBytes + (c - LS::NKC) * 16));
+                ch[s][j][0] = x.x;
+                ch[s][j][1] = x.y;
+                ch[s][j][2] = x.z;
+                ch[s][j][3] = x.w;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        int cnt = 0;
+        bool eq = false;
+#pragma unroll
+        for (int j = 0; j < LS::KCPL; j++) {
+            if (gl + j * G < LS::NKC) {
+                cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], false);
+#pragma unroll
+                for (int k = 0; k < LS::KPC; k++) eq |= key_at<K>(ch[s][j], k) == qv[s];
+            }
+        }
+        int pos0;
+        bool found;
+        if constexpr (G == 1) {
+            pos0 = cnt;
+            found = eq;
+        } else {
+            pos0 = __shfl_sync(0xffffffffu, cnt, grp * G) + __shfl_sync(0xffffffffu, cnt, grp * G + 1);
+            found = (__ballot_sync(0xffffffffu, eq) & gmask) != 0;
+        }
+        found = found && qv[s] <= tmax;  // padding keys are all-ones
+        const int pos = pos0 < LG::S ? pos0 : LG::S - 1;
+        const int vc = LS::NKC + pos / LS::VPC;  // chunk holding the value
+        if (gl == vc % G) {
+            V *d = dst(s);
+            if (d) {
+                V val = 0;
+#pragma unroll
+                for (int j = 0; j < LS::CPL; j++) {
+                    if (j == vc / G) {
+                        const int w = (pos % LS::VPC) * (int)(sizeof(V) / 4);
+                        if constexpr (sizeof(V) == 4) {
+#pragma unroll
+                            for (int k = 0; k < 4; k++)
+                                if (k == w) val = ch[s][j][k];
+                        } else {
+                            val = w == 0 ? (((uint64_t)ch[s][j][1] << 32) | ch[s][j][0])
+                                         : (((uint64_t)ch[s][j][3] << 32) | ch[s][j][2]);
+                        }
+                    }
+                }
+                *d = found ? val : key_max<V>();
+            }
+        }
+    }
+}
+
+// Lower (upper, per slot) bound slot inside each query's leaf block, keys
+// only; every lane of the group receives pos[s].
+template <typename K, typename V, int G, int I>
+__device__ __forceinline__ void leaf_bound(const unsigned char *__restrict__ leaves,
+                                           const uint32_t (&node)[I], const K (&qe)[I],
+                                           const bool (&up)[I], int grp, int gl, int (&pos)[I]) {
+    using LG = LeafGeom<K, V>;
+    using LS = LeafStage<K, V, G>;
+    uint32_t ch[I][LS::KCPL][4];
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
+#pragma unroll
+        for (int j = 0; j < LS::KCPL; j++) {
+            const int c = gl + j * G;
+            if (c < LS::NKC) {
+                const uint4 x = load_stream16(blk + c * 16);
+                ch[s][j][0] = x.x;
+                ch[s][j][1] = x.y;
+                ch[s][j][2] = x.z;
+                ch[s][j][3] = x.w;
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < LS::KCPL; j++)
+            if (gl + j * G < LS::NKC) cnt += count_below<K, LS::KPC>(ch[s][j], qe[s], up[s]);
+        if constexpr (G == 1)
+            pos[s] = cnt;
+        else
+            pos[s] = __shfl_sync(0xffffffffu, cnt, grp * G) + __shfl_sync(0xffffffffu, cnt, grp * G + 1);
+    }
+}
+
 }  // namespace bt

@@ -264,6 +264,44 @@ BT_API bt_status bt_mlp_loss_grad(const float *d_params, uint32_t hidden, const 
                                   const float *d_y, uint64_t n, float *d_loss, float *d_grad,
                                   void *stream);
 
+/* ---- batched forest of uneven trees (north-star extension; in the
+ * reference each tree is its own genBPlusTree + search host calls) ------ */
+
+typedef struct bt_forest bt_forest;
+typedef struct bt_forest_plan bt_forest_plan;
+
+/*
+ * Build num_trees independent trees at once.  Tree t's keys (sorted
+ * ascending) and values are d_keys/d_values[h_offsets[t] .. h_offsets[t+1]),
+ * device memory; h_offsets is a host array of num_trees+1 entries.  Empty
+ * trees are allowed.  All trees share one leaf array and one separator array
+ * (same layout as a single tree) plus a per-tree descriptor table.
+ */
+BT_API bt_status bt_forest_build(const void *d_keys, const void *d_values, const uint64_t *h_offsets,
+                                 uint32_t num_trees, int key_bytes, int value_bytes, void *stream,
+                                 bt_forest **out);
+BT_API bt_status bt_forest_destroy(bt_forest *forest);
+
+/*
+ * A reusable search plan over fixed buffers: point queries of tree t are
+ * d_queries[h_q_offsets[t] .. h_q_offsets[t+1]) with results in d_out at the
+ * same positions; range queries of tree t are [d_lo[i], d_hi[i]] for i in
+ * h_r_offsets[t] .. h_r_offsets[t+1] with counts in d_counts[i] (h_r_offsets
+ * may be NULL for no ranges).  The plan cuts every tree's queries into work
+ * items of `tile` queries and records one persistent kernel launch, in which
+ * warps take items from a device queue, as a CUDA graph (captured on a
+ * private stream when the plan is made).  lanes_per_query / rounds as in
+ * bt_set_search_config.
+ */
+BT_API bt_status bt_forest_plan_create(const bt_forest *forest, const void *d_queries,
+                                       const uint64_t *h_q_offsets, void *d_out, const void *d_lo,
+                                       const void *d_hi, const uint64_t *h_r_offsets,
+                                       uint64_t *d_counts, int lanes_per_query, int rounds,
+                                       uint32_t tile, bt_forest_plan **out);
+/* Launch the plan's graph on `stream` (asynchronous). */
+BT_API bt_status bt_forest_plan_run(bt_forest_plan *plan, void *stream);
+BT_API bt_status bt_forest_plan_destroy(bt_forest_plan *plan);
+
 /* ---- continuous-batching request loop (north-star extension; the reference
  * runs one synchronous batch per host call, BPTreeExactSearch.cu:409-484) */
 
