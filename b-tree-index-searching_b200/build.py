@@ -27,6 +27,7 @@ SOURCES = [
     "bt_learned.cu",
     "bt_server.cu",
     "bt_forest.cu",
+    "bt_rect.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -552,6 +552,12 @@ bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64
                                                                    nq, (uint64_t *)d_ids);
     BT_CUDA(cudaGetLastError());
     if (t->values_sorted) return BT_OK;
+    return launch_segment_sort(t, d_counts, d_offsets, nq, d_ids, s);
+}
+
+bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
+                              uint64_t nq, void *d_ids, cudaStream_t s) {
+    if (nq == 0) return BT_OK;
     unsigned int *flag = nullptr;
     bt_status st = ws_alloc((void **)&flag, sizeof(unsigned int), s);
     if (st != BT_OK) return st;

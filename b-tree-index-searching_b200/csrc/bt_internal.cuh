@@ -174,6 +174,9 @@ bt_status launch_partition_point_prealloc(const bt_tree *t, const void *d_q, uin
                                           cudaStream_t s);
 bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
                             const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
+// Sorts each segment ids[offsets[i] .. + counts[i]) ascending (value width of t).
+bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
+                              uint64_t nseg, void *d_ids, cudaStream_t s);
 
 // (lanes per query, rounds) -> index of the search configuration table in
 // bt_search.cu, or -1.

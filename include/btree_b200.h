@@ -193,6 +193,22 @@ BT_API bt_status bt_range_search(const bt_tree *tree, int mode, const void *d_lo
                           uint64_t nq, uint64_t *d_counts, uint64_t *d_offsets, void *d_ids,
                           uint64_t ids_capacity, uint64_t *h_total, void *stream);
 
+/*
+ * Rectangle search over 2-D points (north-star extension; the reference only
+ * reorders 1-D range queries by a Z-order of (start, end), zOrder2d.cu:27-54).
+ * The tree's keys are 32-bit Morton codes of (x, y) in u16 (x in the even
+ * bits, y in the odd bits), its values point IDs; rectangle i is
+ * [x0,x1] x [y0,y1] inclusive.  Outputs as bt_range_search: counts, offsets
+ * and, for each rectangle, the IDs of the points inside sorted ascending.
+ * Scans the Z interval [Z(x0,y0), Z(x1,y1)] and jumps over runs of keys
+ * outside the box with the BIGMIN computation of Tropf & Herzog (1981).
+ * BT_ERR_INVALID_ARGUMENT unless the tree has 4-byte keys.
+ */
+BT_API bt_status bt_rect_search(const bt_tree *tree, const uint16_t *d_x0, const uint16_t *d_y0,
+                                const uint16_t *d_x1, const uint16_t *d_y1, uint64_t nr,
+                                uint64_t *d_counts, uint64_t *d_offsets, void *d_ids,
+                                uint64_t ids_capacity, uint64_t *h_total, void *stream);
+
 /* Range count with host buffers (pipelined like bt_point_search_host). */
 BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *h_lo,
                               const void *h_hi, uint64_t nq, uint64_t *h_counts,
