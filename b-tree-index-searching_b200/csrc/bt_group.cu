@@ -22,6 +22,7 @@
 // A pass is stable, so the order is deterministic (the reference's in-block
 // atomicAdd scatter is not, grouping.cu:451-452).
 #include <algorithm>
+#include <vector>
 
 #include "bt_internal.cuh"
 
@@ -449,7 +450,8 @@ range_fill_kernel(const unsigned char *__restrict__ leaves, const uint64_t *__re
 
 // Sorts each query's ID segment when values do not ascend with keys.
 // Segments up to kSortCap values are sorted by one CTA with an in-shared-
-// memory bitonic network; longer segments are reported as unsupported.
+// memory bitonic network; longer ones are listed and sorted afterwards, one
+// CTA each, by a bitonic network over a padded copy in global memory.
 constexpr int kSortCap = 4096;
 
 template <typename V>
@@ -488,6 +490,48 @@ segment_sort_kernel(const uint64_t *__restrict__ cnt, const uint64_t *__restrict
         for (uint32_t k = threadIdx.x; k < c; k += blockDim.x) seg[k] = buf[k];
         __syncthreads();
     }
+}
+
+// Segments longer than kSortCap: list them (index, offset, count).
+__global__ void list_long_segments(const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off,
+                                   uint64_t nq, unsigned int *__restrict__ n_long,
+                                   uint64_t *__restrict__ list, unsigned int max_list) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nq;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        if (cnt[i] > (uint64_t)kSortCap) {
+            const unsigned int k = atomicAdd(n_long, 1u);
+            if (k < max_list) {
+                list[2 * k] = off[i];
+                list[2 * k + 1] = cnt[i];
+            }
+        }
+    }
+}
+
+// One CTA sorts one long segment: copy into a power-of-two scratch padded
+// with all-ones, bitonic network in global (L2-resident) memory, copy back.
+template <typename V>
+__global__ void __launch_bounds__(1024)
+long_segment_sort(V *__restrict__ ids, uint64_t off, uint64_t c, V *__restrict__ tmp, uint64_t p2) {
+    for (uint64_t k = threadIdx.x; k < p2; k += blockDim.x) tmp[k] = k < c ? ids[off + k] : key_max<V>();
+    __syncthreads();
+    for (uint64_t size = 2; size <= p2; size <<= 1) {
+        for (uint64_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint64_t k = threadIdx.x; k < p2; k += blockDim.x) {
+                const uint64_t partner = k ^ stride;
+                if (partner > k) {
+                    const bool asc = (k & size) == 0;
+                    const V x = tmp[k], y = tmp[partner];
+                    if ((x > y) == asc) {
+                        tmp[k] = y;
+                        tmp[partner] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (uint64_t k = threadIdx.x; k < c; k += blockDim.x) ids[off + k] = tmp[k];
 }
 
 }  // namespace
@@ -572,10 +616,53 @@ bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const 
                                                          flag);
     unsigned int h = 0;
     BT_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, s));
-    ws_free(flag, s);
     BT_CUDA(cudaStreamSynchronize(s));
-    if (h) return fail(BT_ERR_NOT_SUPPORTED, "a range hit more than 4096 keys whose values are not ascending; ID sort for such ranges is not built");
-    return BT_OK;
+    if (!h) {
+        ws_free(flag, s);
+        return BT_OK;
+    }
+    // some segments exceed the shared-memory sort: list and sort them one CTA each
+    const unsigned int max_list = 1u << 16;
+    uint64_t *d_list = nullptr;
+    st = ws_alloc((void **)&d_list, 2 * (size_t)max_list * sizeof(uint64_t), s);
+    if (st != BT_OK) {
+        ws_free(flag, s);
+        return st;
+    }
+    BT_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), s));
+    count_launch();
+    list_long_segments<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 4096), 256, 0, s>>>(
+        d_counts, d_offsets, nq, flag, d_list, max_list);
+    unsigned int n_long = 0;
+    BT_CUDA(cudaMemcpyAsync(&n_long, flag, sizeof(n_long), cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaStreamSynchronize(s));
+    ws_free(flag, s);
+    if (n_long > max_list) {
+        ws_free(d_list, s);
+        return fail(BT_ERR_NOT_SUPPORTED, "more than 65536 result sets exceed 4096 unsorted values");
+    }
+    std::vector<uint64_t> list(2 * (size_t)n_long);
+    BT_CUDA(cudaMemcpyAsync(list.data(), d_list, list.size() * sizeof(uint64_t),
+                            cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaStreamSynchronize(s));
+    ws_free(d_list, s);
+    const size_t vb = (size_t)t->val_bytes;
+    for (unsigned int k = 0; k < n_long && st == BT_OK; k++) {
+        const uint64_t off = list[2 * k], c = list[2 * k + 1];
+        uint64_t p2 = 1;
+        while (p2 < c) p2 <<= 1;
+        void *tmp = nullptr;
+        st = ws_alloc(&tmp, p2 * vb, s);
+        if (st != BT_OK) break;
+        count_launch();
+        if (vb == 4)
+            long_segment_sort<uint32_t><<<1, 1024, 0, s>>>((uint32_t *)d_ids, off, c, (uint32_t *)tmp, p2);
+        else
+            long_segment_sort<uint64_t><<<1, 1024, 0, s>>>((uint64_t *)d_ids, off, c, (uint64_t *)tmp, p2);
+        ws_free(tmp, s);
+    }
+    BT_CUDA(cudaGetLastError());
+    return st;
 }
 
 }  // namespace bt

@@ -97,3 +97,19 @@ def test_range_host_pipeline(bt, orc, cuda):
     with bt.Tree.build(keys, keys) as t:
         for mode in MODES:
             assert np.array_equal(t.range_count(lo, hi, mode=mode), exp), mode
+
+
+def test_range_ids_long_unsorted_segments(bt, orc, cuda):
+    """Result sets longer than the shared-memory sort (4096 values) whose
+    values do not ascend with the keys."""
+    g = np.random.default_rng(33)
+    keys = np.unique(g.integers(0, 1 << 32, size=200000, dtype=np.uint64)).astype(np.uint32)
+    vals = g.permutation(len(keys)).astype(np.uint32)
+    lo = np.array([0, keys[10], keys[5000], 7], dtype=np.uint32)
+    hi = np.array([0xFFFFFFFF, keys[9000], keys[5100], 9], dtype=np.uint32)
+    ec, eo, ei = orc.range_search(keys, vals, lo, hi)
+    assert ec.max() > 4096
+    with bt.Tree.build(dev(keys, cuda), dev(vals, cuda)) as t:
+        c, o, ids = t.range_search(dev(lo, cuda), dev(hi, cuda))
+    assert np.array_equal(c.cpu().numpy(), ec)
+    assert np.array_equal(ids.cpu().numpy(), ei)
