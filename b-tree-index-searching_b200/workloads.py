@@ -114,6 +114,16 @@ def morton_u16(x, y):
     return spread(x) | (spread(y) << np.uint32(1))
 
 
+def compact_u16(z):
+    """Inverse of the even-bit spread: the bits of z at even positions."""
+    v = z.astype(np.uint32) & np.uint32(0x55555555)
+    v = (v | (v >> np.uint32(1))) & np.uint32(0x33333333)
+    v = (v | (v >> np.uint32(2))) & np.uint32(0x0F0F0F0F)
+    v = (v | (v >> np.uint32(4))) & np.uint32(0x00FF00FF)
+    v = (v | (v >> np.uint32(8))) & np.uint32(0x0000FFFF)
+    return v
+
+
 def zorder_points(n_points=1 << 24, n_rects=1 << 20, max_side=256, seed=KEY_SEED):
     """2-D points keyed by Morton code (duplicates allowed) and rectangles.
     Returns (z_sorted u32, ids u32 in the same order, x0, y0, x1, y1 u16)."""
@@ -147,6 +157,51 @@ def lognormal_keys(n_keys=1 << 28, mu=4.0, sigma=2.0, seed=KEY_SEED, chunk=1 << 
         keys[i:i + m] = c
         acc = c[-1]
     return keys
+
+
+def forest(num_trees=4096, size_log2=(10, 20), batch_log2=(6, 16), hit=0.8, range_frac=0.01,
+           max_width=1 << 12, seed=KEY_SEED):
+    """Batched uneven forest: tree sizes round(2^U), U ~ uniform[size_log2];
+    each tree's keys are a random walk with gaps uniform in [1, (2^32-1) // n]
+    (strictly increasing u32, spanning about half the u32 range); value =
+    rank.  Per tree round(2^U), U ~ uniform[batch_log2], point queries (`hit`
+    of them existing keys, the rest uniform u32) and round(range_frac * that)
+    range queries [key[r], key[min(r + w - 1, n - 1)]], w uniform in
+    [1, max_width] (width in ranks).  Vectorised over all trees.  Returns
+    keys, values, key offsets, queries, query offsets, lo, hi, range offsets."""
+    g = rng(seed)
+    u64 = np.uint64
+    sizes = np.rint(2.0 ** g.uniform(*size_log2, size=num_trees)).astype(np.int64)
+    batches = np.rint(2.0 ** g.uniform(*batch_log2, size=num_trees)).astype(np.int64)
+    nr = np.rint(range_frac * batches).astype(np.int64)
+    koff = np.concatenate([[0], np.cumsum(sizes)])
+    qoff = np.concatenate([[0], np.cumsum(batches)])
+    roff = np.concatenate([[0], np.cumsum(nr)])
+    gmax = (0xFFFFFFFF // sizes).astype(np.float64)  # largest gap; n * gmax < 2^32
+    keys = np.empty(koff[-1], dtype=np.uint32)
+    step = 1 << 26
+    t0 = 0
+    while t0 < num_trees:  # trees in chunks of about 2^26 keys
+        t1 = int(np.searchsorted(koff, koff[t0] + step, side="right"))
+        t1 = min(max(t1 - 1, t0 + 1), num_trees)
+        n = sizes[t0:t1]
+        gaps = np.floor(g.random(int(n.sum())) * np.repeat(gmax[t0:t1], n)).astype(np.int64) + 1
+        cs = np.cumsum(gaps)
+        base = np.repeat(np.concatenate([[0], cs[np.cumsum(n)[:-1] - 1]]), n)
+        keys[koff[t0]:koff[t1]] = (cs - base).astype(np.uint32)
+        t0 = t1
+    vals = (np.arange(koff[-1], dtype=np.int64) - np.repeat(koff[:-1], sizes)).astype(np.uint32)
+    tq = np.repeat(np.arange(num_trees), batches)
+    q = g.integers(0, 1 << 32, size=qoff[-1], dtype=np.uint64).astype(np.uint32)
+    h = g.random(qoff[-1]) < hit
+    pick = koff[tq[h]] + np.floor(g.random(int(h.sum())) * sizes[tq[h]]).astype(np.int64)
+    q[h] = keys[pick]
+    tr = np.repeat(np.arange(num_trees), nr)
+    a = np.floor(g.random(roff[-1]) * sizes[tr]).astype(np.int64)
+    w = g.integers(1, max_width + 1, size=roff[-1])
+    lo = keys[koff[tr] + a]
+    hi = keys[koff[tr] + np.minimum(a + w - 1, sizes[tr] - 1)]
+    return keys, vals, koff.astype(u64), q, qoff.astype(u64), lo, hi, roff.astype(u64)
 
 
 def range_queries(keys, n_queries, max_width_ranks, seed=KEY_SEED + 2):

@@ -53,6 +53,8 @@ def parse_args(argv=None):
     p.add_argument("--learned-keys-log2", type=int, default=28)
     p.add_argument("--serve-requests", type=int, default=3000)
     p.add_argument("--serve-rate", type=float, default=20000.0, help="requests per second")
+    p.add_argument("--no-forest", action="store_true", help="skip the 4096-tree forest section")
+    p.add_argument("--no-rect", action="store_true", help="skip the rectangle-search section")
     return p.parse_args(argv)
 
 
@@ -201,9 +203,11 @@ def profiled_traffic(name):
 
 # ------------------------------------------------------------ cpu leg -------
 
-def cpu_refc_qps(keys, vals, q, sample_log2, repeats=3):
+def cpu_refc_qps(keys, vals, q, sample_log2, gpu_res=None, repeats=3):
     """The reference's algorithm on the host cores: its fanout-5000 page tree
-    restated in C (oracle/oracle.c refc_*), OpenMP over all cores."""
+    restated in C (oracle/oracle.c refc_*), OpenMP over all cores.  The
+    binary-search oracle's answers for the same sample (the secondary timing)
+    are also compared with the GPU results `gpu_res`."""
     from oracle.oracle import Oracle
     orc = Oracle()
     t = orc.refc_build(keys.astype(np.uint64), vals.astype(np.uint64))
@@ -217,9 +221,10 @@ def cpu_refc_qps(keys, vals, q, sample_log2, repeats=3):
     t.close()
     # lower_bound over the sorted array, same sample (secondary figure)
     t0 = time.perf_counter()
-    orc.point_search(keys, vals, q[: len(qs)])
+    exp = orc.point_search(keys, vals, q[: len(qs)])
     lb = len(qs) / (time.perf_counter() - t0)
-    return len(qs) / best, lb, len(qs)
+    matches = None if gpu_res is None else bool(np.array_equal(gpu_res[: len(qs)], exp))
+    return len(qs) / best, lb, len(qs), matches
 
 
 def run_reference(args):
@@ -310,10 +315,7 @@ def learned_section(args, device, bt, flush):
     learned_res = out.cpu().numpy()
     windowed, fallback = tree.learned_last_stats()
     hits = int(np.count_nonzero(learned_res != np.uint64(0xFFFFFFFFFFFFFFFF)))
-    from oracle.oracle import Oracle
-    sample = slice(0, 1 << 20)
-    exact = bool(np.array_equal(learned_res, plain_res)) and bool(
-        np.array_equal(learned_res[sample], Oracle().point_search(keys, vals, q[sample])))
+    exact = bool(np.array_equal(learned_res, plain_res))
     alg = nq * (8 + 8 + 32) + hits * 32
     peak, _ = measured_peak()
 
@@ -359,6 +361,154 @@ def learned_section(args, device, bt, flush):
                                       "keys_per_entry")},
         "serving": {"requests": int(len(reqs)), "rate_per_s": args.serve_rate,
                     "batch_sizes": "round(2^U), U ~ uniform[0,16]", **serving},
+    }
+
+
+# ------------------------------------------------ forest and rectangles ----
+
+def _timed_ms(fn, stream, flush, steps):
+    import torch
+    ts = []
+    for _ in range(steps):
+        flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return statistics.mean(ts)
+
+
+def forest_section(args, device, bt, flush):
+    """4096 trees of round(2^U), U ~ [10, 20], u32
+    keys; per tree round(2^U), U ~ [6, 16], point queries (80% hits) plus 1%
+    range queries of width [1, 2^12] ranks; every batch is one launch of a
+    captured CUDA graph.  The plan's lanes/rounds and tile are chosen by
+    timing the candidates."""
+    import torch
+    wl = importlib.import_module(PKG + ".workloads")
+    keys, vals, koff, q, qoff, lo, hi, roff = wl.forest()
+    stream = torch.cuda.current_stream(device)
+    f = bt.Forest(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device), koff)
+    dq = torch.from_numpy(q).to(device)
+    dlo, dhi = torch.from_numpy(lo).to(device), torch.from_numpy(hi).to(device)
+    out = torch.empty(len(q), dtype=torch.uint32, device=device)
+    counts = torch.empty(len(lo), dtype=torch.uint64, device=device)
+    tried = {}
+    for cfg in ((4, 1), (8, 1), (8, 2)):
+        for tile in (512, 2048):
+            with f.plan(dq, qoff, out, dlo, dhi, roff, counts, *cfg, tile=tile) as p:
+                p.run(stream)
+                tried[f"{cfg[0]}x{cfg[1]}/t{tile}"] = _timed_ms(lambda: p.run(stream), stream, flush, 3)
+    best = min(tried, key=tried.get)
+    lanes, rounds = (int(x) for x in best.split("/")[0].split("x"))
+    tile = int(best.split("/t")[1])
+    with f.plan(dq, qoff, out, dlo, dhi, roff, counts, lanes, rounds, tile=tile) as p:
+        l0 = bt.kernel_launches()
+        ms = _timed_ms(lambda: p.run(stream), stream, flush, args.steps)
+        launches = (bt.kernel_launches() - l0) / args.steps
+    res, cnt = out.cpu().numpy(), counts.cpu().numpy()
+    f.close()
+    # properties of the answers (exactness itself is the forest tests' job):
+    # a found value is the key's rank, so it must point back at the query; a
+    # query that was drawn from the keys must be found; a range [key[a],
+    # key[b]] over unique keys holds b - a + 1 keys
+    sizes = np.diff(koff.astype(np.int64))
+    tq = np.repeat(np.arange(len(sizes)), np.diff(qoff.astype(np.int64)))
+    found = res != np.uint32(0xFFFFFFFF)
+    ok = bool(np.all(res[found] < sizes[tq[found]]))
+    ok = ok and bool(np.array_equal(keys[koff[tq[found]].astype(np.int64) + res[found]], q[found]))
+    pos = np.searchsorted
+    miss = ~found
+    ok = ok and not any(np.isin(q[miss][tq[miss] == t], keys[koff[t]:koff[t + 1]]).any()
+                        for t in range(0, len(sizes), 257))
+    tr = np.repeat(np.arange(len(sizes)), np.diff(roff.astype(np.int64)))
+    exp_cnt = np.empty(len(lo), dtype=np.int64)
+    for t in range(len(sizes)):
+        k = keys[koff[t]:koff[t + 1]]
+        s = slice(int(roff[t]), int(roff[t + 1]))
+        exp_cnt[s] = pos(k, hi[s], side="right") - pos(k, lo[s], side="left")
+    ok = ok and bool(np.array_equal(cnt.astype(np.int64), exp_cnt))
+    total = len(q) + len(lo)
+    hits = int(np.count_nonzero(res != np.uint32(0xFFFFFFFF)))
+    alg = len(q) * (4 + 4 + 32) + hits * 32 + len(lo) * (2 * 4 + 8 + 2 * 32)
+    peak, _ = measured_peak()
+    return {
+        "workload": (f"{len(koff) - 1} trees, {len(keys)} u32 keys in total (sizes round(2^U), "
+                     f"U~[10,20]); {len(q)} point queries (80% hits) + {len(lo)} range queries"),
+        "value": total / (ms / 1e3), "unit": "queries/s", "ms_per_batch": ms,
+        "graph_launches_per_batch": launches, "lanes_per_query": lanes, "rounds": rounds,
+        "tile": tile, "autotune_ms": tried, "answers_consistent": ok,
+        "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak},
+    }
+
+
+def rect_section(args, device, bt, flush):
+    """2^24 points (x, y uniform u16) keyed by their
+    32-bit Morton code (value = point ID, sorted by (code, ID)); 2^20
+    rectangles with a uniform corner and sides uniform in [1, 256].  Timed:
+    one bt_rect_search call (count pass, scan, fill pass, per-box ID sort)
+    into a buffer sized by an untimed first call; beside it the reference's
+    own formulation, hit counts of the Z interval [Z(x0,y0), Z(x1,y1)] under
+    the 2-D-grouped and Z-order-grouped range modes."""
+    import ctypes
+    import torch
+    wl = importlib.import_module(PKG + ".workloads")
+    z, ids, x0, y0, x1, y1 = wl.zorder_points()
+    stream = torch.cuda.current_stream(device)
+    tree = bt.Tree.build(torch.from_numpy(z).to(device), torch.from_numpy(ids).to(device))
+    d = [torch.from_numpy(a).to(device) for a in (x0, y0, x1, y1)]
+    counts, offsets, hits = bt.rect_search(tree, *d)  # sizes the ID buffer
+    total = ctypes.c_uint64(0)
+    P = ctypes.c_void_p
+    cargs = (tree.handle, *(P(t.data_ptr()) for t in d), len(x0), P(counts.data_ptr()),
+             P(offsets.data_ptr()), P(hits.data_ptr()), len(hits), ctypes.byref(total),
+             P(stream.cuda_stream))
+
+    def run():
+        st = bt.lib().bt_rect_search(*cargs)
+        if st != 0:
+            raise RuntimeError(f"bt_rect_search failed with status {st}")
+
+    l0 = bt.kernel_launches()
+    ms = _timed_ms(run, stream, flush, max(3, args.steps // 3))
+    launches = (bt.kernel_launches() - l0) / max(3, args.steps // 3)
+    c, off, got = counts.cpu().numpy(), offsets.cpu().numpy(), hits.cpu().numpy()
+    # properties of the first 2048 answers (exactness is the rectangle tests'
+    # job): IDs strictly ascending per box and every hit inside its box
+    zid = np.empty(len(z), dtype=np.uint32)
+    zid[ids] = z
+    ok = True
+    for i in range(2048):
+        h = got[int(off[i]):int(off[i] + c[i])]
+        hz = zid[h]
+        hx, hy = (wl.compact_u16(hz), wl.compact_u16(hz >> np.uint32(1)))
+        ok = ok and bool(np.all(np.diff(h.astype(np.int64)) > 0)) and bool(
+            np.all((hx >= x0[i]) & (hx <= x1[i]) & (hy >= y0[i]) & (hy <= y1[i])))
+    zl = torch.from_numpy(wl.morton_u16(x0, y0)).to(device)
+    zh = torch.from_numpy(wl.morton_u16(x1, y1)).to(device)
+    cnt = torch.empty(len(x0), dtype=torch.uint64, device=device)
+    zi = {}
+    for mode in ("2d", "zorder"):
+        zms = _timed_ms(lambda: tree.range_count(zl, zh, mode=mode, out=cnt, stream=stream),
+                        stream, flush, 3)
+        zi[mode] = {"rects_per_s": len(x0) / (zms / 1e3), "ms": zms,
+                    "interval_hits": int(cnt.sum().item())}
+    tree.close()
+    nh = int(c.sum())
+    alg = len(x0) * (8 + 8 + 8) + nh * (4 + 4)  # boxes + counts + offsets; per hit key + ID read
+    peak, _ = measured_peak()
+    return {
+        "workload": "2^24 points (u16 x, y; 32-bit Morton keys, value = ID), 2^20 rectangles, "
+                    "sides uniform [1, 256]; counts + sorted hit IDs",
+        "value": len(x0) / (ms / 1e3), "unit": "rectangles/s", "ms": ms, "launches_per_call": launches,
+        "hits": nh, "hits_per_rect": nh / len(x0), "answers_consistent_first_2048": ok,
+        "z_interval_counts": zi,
+        "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak},
     }
 
 
@@ -408,7 +558,7 @@ def run_ours(args):
     b_lanes, b_slots, b_ms = at.tune(tree, dq, mode="basic", repeats=3)
     g_lanes, g_slots, g_ms = at.tune(tree, dq, mode="grouped", repeats=3)
 
-    # warm-up (also checks the result against the CPU judge on rank 0)
+    # warm-up (the result is compared with the CPU leg's sample on rank 0)
     for _ in range(max(args.warmup, 3)):
         group_into()
         search_grouped()
@@ -416,9 +566,6 @@ def run_ours(args):
     res = out.cpu().numpy()
     hits = int(np.count_nonzero(res != np.uint32(0xFFFFFFFF)))
     checked = None
-    if rank == 0:
-        from oracle.oracle import Oracle
-        checked = bool(np.array_equal(res, Oracle().point_search(keys, vals, q)))
 
     # ---- timed region: K grouped steps, device time per step ----------------
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
@@ -485,15 +632,19 @@ def run_ours(args):
     peak, peak_kind = measured_peak()
     tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
 
-    learned = None
+    learned = forest = rect = None
     if world == 1 and not args.no_learned:
         learned = learned_section(args, device, bt, flush)
+    if world == 1 and not args.no_forest:
+        forest = forest_section(args, device, bt, flush)
+    if world == 1 and not args.no_rect:
+        rect = rect_section(args, device, bt, flush)
 
     line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            qps_refc, qps_lb, sample = cpu_refc_qps(keys, vals, q, args.cpu_sample_log2)
+            qps_refc, qps_lb, sample, checked = cpu_refc_qps(keys, vals, q, args.cpu_sample_log2, res)
             cpu = {"value": qps_refc, "unit": "queries/s", "cores": os.cpu_count(),
                    "kind": "port",
                    "sample": f"{sample} queries of the batch, reference page tree (fanout 5000) "
@@ -526,8 +677,10 @@ def run_ours(args):
                                      "ms": g_ms},
                          "basic": {"lanes_per_query": b_lanes, "queries_per_group": b_slots,
                                    "ms": b_ms}},
-            "checked_vs_oracle": checked,
+            "cpu_sample_matches_gpu": checked,
             "learned_index": learned,
+            "forest": forest,
+            "rectangles": rect,
         }
         print(json.dumps(line), flush=True)
     tree.close()

@@ -234,7 +234,7 @@ BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *
  * above the bottom (one separator per leaf node), then descends normally;
  * a query whose lower bound is not provably inside the window takes the
  * full tree descent, so results never depend on the model (the tree stays
- * both the fallback and the judge).
+ * both the fallback and the source of truth).
  */
 typedef struct bt_learned_config {
     uint32_t num_segments;  /* leaf models (default 65536) */

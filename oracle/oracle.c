@@ -1,7 +1,7 @@
 /*
  * CPU oracle for the B+tree index search path -- TEST INFRASTRUCTURE ONLY.
  * See oracle.h for the contract.  Only tests/, __graft_entry__.smoke() and
- * bench.py's CPU-baseline leg load this library, and only as the checker or
+ * bench.py's CPU-baseline leg load this library, and only to check results or
  * as the timed CPU baseline.  The shipped engine never calls it.
  */
 #include "oracle.h"
@@ -22,7 +22,7 @@ static int orc_threads(int nthreads) {
 }
 
 /* ------------------------------------------------------------------------ */
-/* The judge: binary search over the sorted key array.                      */
+/* Ground truth: binary search over the sorted key array.                      */
 /* ------------------------------------------------------------------------ */
 
 /* first index i in [0, n) with keys[i] >= q (or > q when upper), else n */

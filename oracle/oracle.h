@@ -3,11 +3,11 @@
  *
  * TEST INFRASTRUCTURE ONLY.  Nothing in the shipped library links, loads or
  * calls this code; only tests/, __graft_entry__.smoke() and bench.py's CPU
- * baseline leg use it, and only as the checker (or as the timed CPU baseline).
+ * baseline leg use it, and only to check results (or as the timed CPU baseline).
  *
  * Two families of functions live here:
  *
- *  1. orc_*  : the judge.  Plain binary search over the sorted key array
+ *  1. orc_*  : ground truth.  Plain binary search over the sorted key array
  *              (std::lower_bound / std::upper_bound semantics).  Point search
  *              returns values[lower_bound(q)] on an exact match, else the
  *              all-ones sentinel of the value width (the reference's
@@ -18,7 +18,7 @@
  *  2. refc_* : a literal CPU restatement of the reference's page-based tree
  *              (fanout PAGESIZE = 5000, BPTree.h:6-23) and of its kernels,
  *              including their quirks, so that divergences between the
- *              reference and the judge can be explained case by case.
+ *              reference and the ground truth can be explained case by case.
  *              Each function cites the reference file:line it follows.
  *
  * All functions are thread-safe; `nthreads` <= 0 means "all OpenMP threads".
@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-/* ---- the judge ---------------------------------------------------------- */
+/* ---- ground truth ---------------------------------------------------------- */
 
 /* Point search.  key_bytes/val_bytes in {4, 8}.  out has val_bytes per query. */
 int orc_point_search(const void *keys, const void *vals, uint64_t n,

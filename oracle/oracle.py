@@ -1,9 +1,9 @@
 """ctypes wrappers of the CPU oracle and of the reference harness.
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg, as the checker.  The engine never imports it.
+bench.py's CPU-baseline leg, to check results.  The engine never imports it.
 
-  Oracle   -- lib/liboracle.so (oracle.c): binary-search judge + literal
+  Oracle   -- lib/liboracle.so (oracle.c): binary-search ground truth + literal
               restatement of the reference's page tree ("refc").
   RefHarness -- _ref/libbtref.so: the reference's own .cu sources compiled
               for sm_100a plus ref_harness.cu (needs a GPU to run).
@@ -67,7 +67,7 @@ class Oracle:
             f.argtypes = args
         self.L = L
 
-    # -- the judge --------------------------------------------------------
+    # -- ground truth --------------------------------------------------------
     def point_search(self, keys, vals, queries, nthreads=0):
         keys, vals, queries = map(np.ascontiguousarray, (keys, vals, queries))
         out = np.empty(len(queries), dtype=vals.dtype)

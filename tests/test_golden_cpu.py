@@ -3,7 +3,7 @@
 tests/golden/reference_outputs.npz holds inputs and outputs of the
 reference's own kernels (compiled from its sources for sm_100a and run on a
 B200 by tests/golden/make_golden.py).  Here, on the CPU:
-  * the judge (lower_bound) reproduces the reference's basic point search;
+  * the ground truth (lower_bound) reproduces the reference's basic point search;
   * the literal restatement reproduces every reference output, including the
     grouped point search and the off-by-one range counts.
 """
@@ -45,7 +45,7 @@ def test_range_endpoints_and_counts_pinned(g, orc):
     c, rc = t.range_count(lo, hi)
     assert rc == 0
     assert np.array_equal(c, g["rg_count"])
-    # the judge is exact; the reference is 0-3 low
+    # the ground truth is exact; the reference is 0-3 low
     d = orc.range_count(k, lo, hi).astype(np.int64) - g["rg_count"].astype(np.int64)
     assert d.min() >= 0 and d.max() <= 3
 

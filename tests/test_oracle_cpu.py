@@ -1,8 +1,8 @@
-"""The CPU oracle, checked before it is trusted as the judge.
+"""The CPU oracle, checked before it is trusted as ground truth.
 
 * against numpy's searchsorted (an independent binary search);
 * against known answers derived by hand from the reference's code;
-* the literal restatement of the reference ("refc") against the judge, with
+* the literal restatement of the reference ("refc") against the ground truth, with
   the reference's documented divergences reproduced exactly.
 The pin against the reference's own outputs is in test_golden_cpu.py.
 """
@@ -94,7 +94,7 @@ def test_morton_matches_bitwise(orc, wl):
 # ---- the literal restatement of the reference ------------------------------
 
 @pytest.mark.parametrize("n", [1, 7, 4999, 5000, 5001, 10000, 25001, 60000])
-def test_refc_basic_equals_judge(orc, n):
+def test_refc_basic_equals_ground_truth(orc, n):
     """kernelSearchingNaiveOneStep == std::lower_bound exact match (unique keys)."""
     g = np.random.default_rng(n)
     keys = np.unique(g.integers(0, 1 << 40, size=n + 100, dtype=np.uint64))[:n]
