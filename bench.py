@@ -499,7 +499,9 @@ def rect_section(args, device, bt, flush):
                     "interval_hits": int(cnt.sum().item())}
     tree.close()
     nh = int(c.sum())
-    alg = len(x0) * (8 + 8 + 8) + nh * (4 + 4)  # boxes + counts + offsets; per hit key + ID read
+    # per box: its corners (8 B), count and offset out (16 B), one 32-byte
+    # key sector for the descent; per hit: key read, ID read, ID write
+    alg = len(x0) * (8 + 16 + 32) + nh * (4 + 4 + 4)
     peak, _ = measured_peak()
     return {
         "workload": "2^24 points (u16 x, y; 32-bit Morton keys, value = ID), 2^20 rectangles, "
