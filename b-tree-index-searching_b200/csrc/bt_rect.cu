@@ -1,17 +1,22 @@
 // Rectangle search over Z-ordered 2-D points (declared in btree_b200.h).
 //
-// Keys are 32-bit Morton codes z = interleave(x, y) (x in the even bits).
-// Every point of the box [x0,x1] x [y0,y1] has its code in
-// [zmin, zmax] = [Z(x0,y0), Z(x1,y1)] (interleaving is monotone in each
-// coordinate), but that interval also holds many points outside the box.
-// One warp per rectangle scans the sorted keys 32 at a time from
-// lower_bound(zmin), tests each decoded (x, y) against the box, and when the
-// window's last key lies outside the box jumps to lower_bound(BIGMIN) --
-// BIGMIN being the smallest code above it that lies inside the box (Tropf &
-// Herzog, "Multidimensional range search in dynamically balanced trees",
-// 1981) -- so long outside runs cost one descent instead of a scan.  A count
-// pass, an exclusive scan and a fill pass produce CSR output; the IDs of each
-// box are then sorted.
+// Keys are 32-bit Morton codes z = interleave(x, y) (x in the even bits).  An
+// aligned square cell of side 2^c ([X, X + 2^c) x [Y, Y + 2^c), X and Y
+// multiples of 2^c) holds exactly the codes of one interval
+// [Z(X,Y), Z(X,Y) + 4^c), so its points are one contiguous run of the sorted
+// keys.  Each box [x0,x1] x [y0,y1] is covered by the aligned cells of the
+// smallest c that needs at most 16 of them; one warp per box finds the run
+// of every cell with 32 descents in one round (lanes 0-15: lower bound of a
+// cell's first code, lanes 16-31: upper bound of its last), the same
+// two-phase descent as the point search.  Cells inside the box count their
+// whole run; the runs of the cells on the box's edge are scanned by the warp
+// together, 32 keys at a time, testing each decoded (x, y).  A count pass
+// (which also stores every cell's run), an exclusive scan and a fill pass
+// produce CSR output; the IDs of each box are then sorted.
+//
+// About 1.3x the box's area in codes is scanned; the alternative of scanning
+// [Z(x0,y0), Z(x1,y1)] and jumping over outside stretches (BIGMIN, Tropf &
+// Herzog 1981) pays one dependent root-to-leaf descent per jump.
 #include <algorithm>
 
 #include "bt_search.cuh"
@@ -19,7 +24,9 @@
 namespace bt {
 namespace {
 
-constexpr int kRThreads = 256;
+constexpr int kRThreads = 512;
+constexpr int kRWarps = kRThreads / 32;
+constexpr int kMaxCells = 16;
 
 __device__ __forceinline__ uint32_t compact16(uint32_t v) {
     v &= 0x55555555u;
@@ -45,103 +52,186 @@ __device__ __forceinline__ bool in_box(uint32_t z, uint32_t x0, uint32_t y0, uin
     return x >= x0 && x <= x1 && y >= y0 && y <= y1;
 }
 
-// Smallest Morton code > z inside the box [zmin, zmax] (both corners' codes),
-// or 0xFFFFFFFF if there is none; z must lie inside [zmin, zmax] and outside
-// the box.  Bits are visited from the top; at each bit the (z, zmin, zmax)
-// pattern decides whether the box lies entirely above z in that subtree, splits
-// it (narrowing zmin or zmax to one half of the dimension), or ends the walk.
-__device__ uint32_t bigmin(uint32_t z, uint32_t zmin, uint32_t zmax) {
-    uint32_t best = 0xFFFFFFFFu;
-    for (int b = 31; b >= 0; b--) {
-        const uint32_t m = 1u << b;
-        const uint32_t low = ((b & 1) ? 0xAAAAAAAAu : 0x55555555u) & (m - 1u);  // lower bits, same dim
-        const int zb = (z & m) != 0, lb = (zmin & m) != 0, hb = (zmax & m) != 0;
-        if (!zb && !lb && hb) {
-            best = (zmin | m) & ~low;   // the upper half starts here
-            zmax = (zmax & ~m) | low;   // keep looking in the lower half
-        } else if (!zb && lb && hb) {
-            return zmin;                // the whole box is above z here
-        } else if (zb && !lb && !hb) {
-            return best;                // z is above the box here
-        } else if (zb && !lb && hb) {
-            zmin = (zmin | m) & ~low;   // continue in the upper half
-        } else if (lb && !hb) {
-            return best;                // empty box in this dimension
-        }
+// The cover of one box: cells of side 2^c, nx per row; cell j of the lane.
+struct Cell {
+    uint32_t zs, ze;  // first and last code of the cell
+    bool valid;       // j < number of cells
+    bool full;        // the cell lies inside the box
+};
+
+__device__ __forceinline__ Cell box_cell(uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, int j) {
+    int c = 0;
+    uint32_t nx = x1 - x0 + 1, ny = y1 - y0 + 1;
+    while ((uint64_t)nx * ny > (uint64_t)kMaxCells) {  // c = 16 gives one cell
+        c++;
+        nx = (x1 >> c) - (x0 >> c) + 1;
+        ny = (y1 >> c) - (y0 >> c) + 1;
     }
-    return best;
+    Cell cell;
+    cell.valid = (uint32_t)j < nx * ny;
+    const uint32_t X = ((x0 >> c) + (uint32_t)j % nx) << c;
+    const uint32_t Y = ((y0 >> c) + (uint32_t)j / nx) << c;
+    const uint32_t side = (1u << c) - 1u;  // c <= 16
+    cell.zs = spread16d(X) | (spread16d(Y) << 1);
+    cell.ze = (uint32_t)((uint64_t)cell.zs + (1ull << (2 * c)) - 1ull);
+    cell.full = X >= x0 && X + side <= x1 && Y >= y0 && Y + side <= y1;
+    return cell;
 }
 
-// First position with key >= q (q <= max key) by the whole warp: the lanes
-// binary-search the staged level together (same path), then walk the global
-// levels with all 32 lanes on one node line, then the leaf block.
-template <typename V>
-__device__ __forceinline__ uint64_t warp_lower_bound(const DevTree &t, const uint32_t *s_lvl,
-                                                     uint32_t q) {
+// Lanes 0-15 receive the first key position of cell `lane`, lanes 16-31 the
+// position after the last key of cell `lane - 16`: lower bounds of the
+// cells' first codes and upper bounds of their last codes, 32 descents in
+// one round (G lanes per descent, G/1 descents per group).
+template <typename V, int G>
+__device__ __forceinline__ uint64_t cell_bounds(const DevTree &t, const uint32_t *s_lvl,
+                                                uint64_t *res, const Cell &cell, int lane) {
+    using LG = LeafGeom<uint32_t, V>;
+    constexpr int NG = 32 / G;
+    constexpr int I = G;
+    const int grp = lane / G, gl = lane % G;
     const uint32_t tmax = (uint32_t)t.max_key;
-    if (q > tmax) return t.n;
-    uint32_t qe[1] = {q};
-    bool up[1] = {false};
-    uint32_t node[1] = {smem_bound<uint32_t>(s_lvl, t.smem_entries, q, false)};
-    const int lane = threadIdx.x & 31;
-    walk_global<uint32_t, 32, 1>(t, qe, up, node, 0, lane);
-    int pos[1];
-    leaf_bound<uint32_t, V, 32, 1>(static_cast<const unsigned char *>(t.leaves), node, qe, up, 0,
-                                   lane, pos);
-    return (uint64_t)node[0] * LeafGeom<uint32_t, V>::S + pos[0];
+    const bool upper_lane = lane >= kMaxCells;
+    // lower bound of a: a > max gives n; upper bound of b: b >= max gives n
+    const uint32_t a = upper_lane ? cell.ze : cell.zs;
+    const bool beyond = upper_lane ? a >= tmax : a > tmax;
+    const bool up = upper_lane && a < tmax;
+    const uint32_t qa = a < tmax ? a : tmax;
+    const uint32_t nd = smem_bound<uint32_t>(s_lvl, t.smem_entries, qa, up);
+    uint32_t qe[I], node[I];
+    bool ups[I];
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        const int k = s * NG + grp;
+        qe[s] = __shfl_sync(0xffffffffu, qa, k);
+        node[s] = __shfl_sync(0xffffffffu, nd, k);
+        ups[s] = __shfl_sync(0xffffffffu, (int)up, k) != 0;
+    }
+    walk_global<uint32_t, G, I>(t, qe, ups, node, grp, gl);
+    int pos[I];
+    leaf_bound<uint32_t, V, G, I>(static_cast<const unsigned char *>(t.leaves), node, qe, ups, grp,
+                                  gl, pos);
+#pragma unroll
+    for (int s = 0; s < I; s++)
+        if (gl == 0) res[s * NG + grp] = (uint64_t)node[s] * LG::S + pos[s];
+    __syncwarp();
+    const uint64_t r = beyond ? t.n : res[lane];
+    __syncwarp();
+    return r;
 }
 
-// FILL = false: counts[i] = points in box i.  FILL = true: write their IDs
-// at ids[offsets[i] ..] (in key order; sorted afterwards).
-template <typename V, bool FILL>
-__global__ void __launch_bounds__(kRThreads)
-rect_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
-            const uint16_t *__restrict__ y0s, const uint16_t *__restrict__ x1s,
-            const uint16_t *__restrict__ y1s, uint64_t nr, uint64_t *__restrict__ counts,
-            const uint64_t *__restrict__ offsets, V *__restrict__ ids) {
+// Exclusive prefix sum over the warp.
+__device__ __forceinline__ uint64_t warp_excl_scan(uint64_t v, int lane, uint64_t &total) {
+    uint64_t x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint64_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+// Cell (0..15) whose run holds item k of the concatenated runs, given each
+// lane's exclusive offset `off` (cells past the last hold offset = total).
+__device__ __forceinline__ int find_cell(uint64_t off, uint64_t k) {
+    int j = 0;
+#pragma unroll
+    for (int step = kMaxCells / 2; step >= 1; step >>= 1) {
+        const uint64_t o = __shfl_sync(0xffffffffu, off, j + step);
+        if (o <= k) j += step;
+    }
+    return j;
+}
+
+__device__ __forceinline__ uint32_t key_at_pos(const unsigned char *leaves, uint64_t p, int S, int BS) {
+    return reinterpret_cast<const uint32_t *>(leaves + (p / S) * BS)[p % S];
+}
+
+// Count pass: counts[i] = points in box i; runs[i * 16 + j] = (first key
+// position, length) of cell j's run (positions fit 32 bits: n < 2^32).
+template <typename V>
+__global__ void __launch_bounds__(kRThreads, 2)
+rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
+                  const uint16_t *__restrict__ y0s, const uint16_t *__restrict__ x1s,
+                  const uint16_t *__restrict__ y1s, uint64_t nr, uint64_t *__restrict__ counts,
+                  uint2 *__restrict__ runs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t *s_lvl = reinterpret_cast<uint32_t *>(smem_raw);
+    uint64_t *res = reinterpret_cast<uint64_t *>(smem_raw + (((size_t)t.smem_bytes + 15) / 16 * 16)) +
+                    (threadIdx.x >> 5) * 32;
     stage_level<uint32_t>(s_lvl, t);
     __syncthreads();
     using LG = LeafGeom<uint32_t, V>;
     const int lane = threadIdx.x & 31;
+    const int j = lane % kMaxCells;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    const unsigned lt = (1u << lane) - 1u;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nr;
          i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
         const uint32_t x0 = x0s[i], y0 = y0s[i], x1 = x1s[i], y1 = y1s[i];
-        uint64_t c = 0;
-        if (x0 <= x1 && y0 <= y1 && t.n > 0) {
-            const uint32_t zmin = spread16d(x0) | (spread16d(y0) << 1);
-            const uint32_t zmax = spread16d(x1) | (spread16d(y1) << 1);
-            const uint64_t base_out = FILL ? offsets[i] : 0;
-            uint64_t pos = warp_lower_bound<V>(t, s_lvl, zmin);
-            while (pos < t.n) {
-                const uint64_t p = pos + lane;
-                const bool valid = p < t.n;
-                const uint32_t k = valid ? reinterpret_cast<const uint32_t *>(
-                                               leaves + (p / LG::S) * LG::BS)[p % LG::S]
-                                         : 0xFFFFFFFFu;
-                const bool in_range = valid && k <= zmax;
-                const bool inside = in_range && in_box(k, x0, y0, x1, y1);
-                const unsigned hit = __ballot_sync(0xffffffffu, inside);
-                if (FILL && inside)
-                    ids[base_out + c + __popc(hit & lt)] = reinterpret_cast<const V *>(
-                        leaves + (p / LG::S) * LG::BS + kSectorBytes)[p % LG::S];
-                c += __popc(hit);
-                if (__ballot_sync(0xffffffffu, in_range) != 0xffffffffu) break;  // past zmax or n
-                const uint32_t last = __shfl_sync(0xffffffffu, k, 31);
-                if (hit >> 31) {  // the window ends inside the box: keep scanning
-                    pos += 32;
-                    continue;
-                }
-                const uint32_t bm = bigmin(last, zmin, zmax);
-                if (bm == 0xFFFFFFFFu || bm > zmax) break;
-                // bm > last, so the new position is past this window
-                pos = warp_lower_bound<V>(t, s_lvl, bm);
-            }
+        if (x0 > x1 || y0 > y1) {  // empty box (warp-uniform)
+            if (lane == 0) counts[i] = 0;
+            if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2(0u, 0u);
+            continue;
         }
-        if (!FILL && lane == 0) counts[i] = c;
+        const Cell cell = box_cell(x0, y0, x1, y1, j);
+        const uint64_t b = cell_bounds<V, 4>(t, s_lvl, res, cell, lane);
+        const uint64_t ub = __shfl_sync(0xffffffffu, b, lane + kMaxCells);
+        const uint64_t len = (lane < kMaxCells && cell.valid && ub > b) ? ub - b : 0;
+        uint64_t total;
+        // whole runs of the cells inside the box; edge cells are scanned
+        warp_excl_scan(cell.full ? len : 0, lane, total);
+        uint64_t c = total;
+        uint64_t P;
+        const uint64_t poff = warp_excl_scan(cell.full ? 0 : len, lane, P);
+        for (uint64_t base = 0; base < P; base += 32) {
+            const uint64_t k = base + lane;
+            const int jc = find_cell(poff, k);
+            const uint64_t lb_j = __shfl_sync(0xffffffffu, b, jc);
+            const uint64_t off_j = __shfl_sync(0xffffffffu, poff, jc);
+            const bool inside =
+                k < P && in_box(key_at_pos(leaves, lb_j + (k - off_j), LG::S, LG::BS), x0, y0, x1, y1);
+            c += __popc(__ballot_sync(0xffffffffu, inside));
+        }
+        if (lane == 0) counts[i] = c;
+        if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2((uint32_t)b, (uint32_t)len);
+    }
+}
+
+// Fill pass: the IDs of box i's points at ids[offsets[i] ..], cell by cell
+// (sorted afterwards).
+template <typename V>
+__global__ void __launch_bounds__(kRThreads)
+rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
+                 const uint16_t *__restrict__ y0s, const uint16_t *__restrict__ x1s,
+                 const uint16_t *__restrict__ y1s, uint64_t nr, const uint2 *__restrict__ runs,
+                 const uint64_t *__restrict__ offsets, V *__restrict__ ids) {
+    using LG = LeafGeom<uint32_t, V>;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nr;
+         i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        const uint32_t x0 = x0s[i], y0 = y0s[i], x1 = x1s[i], y1 = y1s[i];
+        if (x0 > x1 || y0 > y1) continue;
+        const Cell cell = box_cell(x0, y0, x1, y1, lane % kMaxCells);
+        const uint2 run = lane < kMaxCells ? runs[i * kMaxCells + lane] : make_uint2(0u, 0u);
+        uint64_t T;
+        const uint64_t off = warp_excl_scan(run.y, lane, T);
+        uint64_t out = offsets[i];
+        for (uint64_t base = 0; base < T; base += 32) {
+            const uint64_t k = base + lane;
+            const int jc = find_cell(off, k);
+            const uint64_t p = (uint64_t)__shfl_sync(0xffffffffu, run.x, jc) +
+                               (k - __shfl_sync(0xffffffffu, off, jc));
+            const bool full = __shfl_sync(0xffffffffu, (int)cell.full, jc) != 0;
+            const bool inside =
+                k < T && (full || in_box(key_at_pos(leaves, p, LG::S, LG::BS), x0, y0, x1, y1));
+            const unsigned hit = __ballot_sync(0xffffffffu, inside);
+            if (inside)
+                ids[out + __popc(hit & lt)] =
+                    reinterpret_cast<const V *>(leaves + (p / LG::S) * LG::BS + kSectorBytes)[p % LG::S];
+            out += __popc(hit);
+        }
     }
 }
 
@@ -149,40 +239,54 @@ template <typename V>
 bt_status rect_impl(const bt_tree *t, const uint16_t *x0, const uint16_t *y0, const uint16_t *x1,
                     const uint16_t *y1, uint64_t nr, uint64_t *counts, uint64_t *offsets,
                     void *ids, uint64_t cap, uint64_t *h_total, cudaStream_t s) {
-    const size_t smem = t->dev.smem_bytes;
-    auto kc = rect_kernel<V, false>;
-    auto kf = rect_kernel<V, true>;
-    if (smem > 48 * 1024) {
+    const size_t smem = ((size_t)t->dev.smem_bytes + 15) / 16 * 16 + (size_t)kRWarps * 32 * sizeof(uint64_t);
+    auto kc = rect_count_kernel<V>;
+    auto kf = rect_fill_kernel<V>;
+    if (smem > 48 * 1024)
         BT_CUDA(cudaFuncSetAttribute(kc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        BT_CUDA(cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
     int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, kRThreads, smem);
     const unsigned grid = (unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>((nr + 7) / 8, (uint64_t)sm_count() * std::max(per_sm, 1)));
-    count_launch();
-    kc<<<grid, kRThreads, smem, s>>>(t->dev, x0, y0, x1, y1, nr, counts, nullptr, nullptr);
-    BT_CUDA(cudaGetLastError());
+        1, std::min<uint64_t>((nr + kRWarps - 1) / kRWarps, (uint64_t)sm_count() * std::max(per_sm, 1)));
+    uint2 *runs = nullptr;
     uint64_t *d_total = nullptr;
-    bt_status st = ws_alloc((void **)&d_total, sizeof(uint64_t), s);
+    bt_status st = ws_alloc((void **)&runs, nr * kMaxCells * sizeof(uint2), s);
     if (st != BT_OK) return st;
-    st = launch_scan_u64(counts, offsets, nr, d_total, s);
+    st = ws_alloc((void **)&d_total, sizeof(uint64_t), s);
+    if (st != BT_OK) {
+        ws_free(runs, s);
+        return st;
+    }
+    count_launch();
+    kc<<<grid, kRThreads, smem, s>>>(t->dev, x0, y0, x1, y1, nr, counts, runs);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) st = cuda_fail(e, "rectangle count pass");
+    if (st == BT_OK) st = launch_scan_u64(counts, offsets, nr, d_total, s);
     uint64_t total = 0;
     if (st == BT_OK) {
-        cudaError_t e = cudaMemcpyAsync(&total, d_total, sizeof(total), cudaMemcpyDeviceToHost, s);
+        e = cudaMemcpyAsync(&total, d_total, sizeof(total), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_fail(e, "rectangle total read-back");
     }
+    if (st == BT_OK) {
+        *h_total = total;
+        if (total > cap) {
+            st = fail(BT_ERR_CAPACITY, "ids_capacity is below the total hit count");
+        } else if (total > 0 && !ids) {
+            st = fail(BT_ERR_INVALID_ARGUMENT, "ids is NULL");
+        } else if (total > 0) {
+            const unsigned fgrid = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>((nr + kRWarps - 1) / kRWarps, (uint64_t)sm_count() * 4));
+            count_launch();
+            kf<<<fgrid, kRThreads, 0, s>>>(t->dev, x0, y0, x1, y1, nr, runs, offsets, (V *)ids);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) st = cuda_fail(e, "rectangle fill pass");
+            if (st == BT_OK) st = launch_segment_sort(t, counts, offsets, nr, ids, s);
+        }
+    }
     ws_free(d_total, s);
-    if (st != BT_OK) return st;
-    *h_total = total;
-    if (total > cap) return fail(BT_ERR_CAPACITY, "ids_capacity is below the total hit count");
-    if (total == 0) return BT_OK;
-    if (!ids) return fail(BT_ERR_INVALID_ARGUMENT, "ids is NULL");
-    count_launch();
-    kf<<<grid, kRThreads, smem, s>>>(t->dev, x0, y0, x1, y1, nr, counts, offsets, (V *)ids);
-    BT_CUDA(cudaGetLastError());
-    return launch_segment_sort(t, counts, offsets, nr, ids, s);
+    ws_free(runs, s);
+    return st;
 }
 
 }  // namespace
@@ -200,6 +304,8 @@ bt_status bt_rect_search(const bt_tree *t, const uint16_t *x0, const uint16_t *y
     *h_total = 0;
     if (t->key_bytes != 4)
         return fail(BT_ERR_INVALID_ARGUMENT, "rectangle search needs 32-bit Morton-code keys");
+    if (t->n >= (1ull << 32))
+        return fail(BT_ERR_NOT_SUPPORTED, "rectangle search needs fewer than 2^32 points");
     if (nr == 0) return BT_OK;
     if (!x0 || !y0 || !x1 || !y1 || !counts || !offsets)
         return fail(BT_ERR_INVALID_ARGUMENT, "a rectangle or output array is NULL");
@@ -207,6 +313,12 @@ bt_status bt_rect_search(const bt_tree *t, const uint16_t *x0, const uint16_t *y
     BT_CUDA(cudaGetDevice(&prev));
     if (prev != t->device) BT_CUDA(cudaSetDevice(t->device));
     cudaStream_t s = (cudaStream_t)stream;
+    if (t->n == 0) {  // no points: every box is empty
+        cudaError_t e = cudaMemsetAsync(counts, 0, nr * sizeof(uint64_t), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(offsets, 0, nr * sizeof(uint64_t), s);
+        if (prev != t->device) cudaSetDevice(prev);
+        return e == cudaSuccess ? BT_OK : cuda_fail(e, "rectangle search on an empty tree");
+    }
     const bt_status st =
         t->val_bytes == 4 ? rect_impl<uint32_t>(t, x0, y0, x1, y1, nr, counts, offsets, ids, cap, h_total, s)
                           : rect_impl<uint64_t>(t, x0, y0, x1, y1, nr, counts, offsets, ids, cap, h_total, s);

@@ -42,3 +42,42 @@ def test_rect_search_needs_32bit_keys(bt, cuda):
         u = torch.zeros(1, dtype=torch.uint16, device=cuda)
         with pytest.raises(bt.BTreeError):
             bt.rect_search(t, u, u, u, u)
+
+
+@pytest.mark.parametrize("side_log2", [0, 2, 5, 8, 11, 14, 16])
+def test_rect_search_box_sizes(bt, orc, wl, cuda, side_log2):
+    """Boxes whose sides reach 2^side_log2 (cell sizes from 1 to the whole
+    grid), over points with duplicated coordinates."""
+    g = np.random.default_rng(side_log2 + 100)
+    n = 1 << 18
+    x = g.integers(0, 1 << 16, size=n).astype(np.uint16)
+    y = g.integers(0, 1 << 16, size=n).astype(np.uint16)
+    x[: n // 8], y[: n // 8] = x[n // 8: n // 4], y[n // 8: n // 4]  # duplicate points
+    z = wl.morton_u16(x, y)
+    ids = np.arange(n, dtype=np.uint32)
+    o = np.lexsort((ids, z))
+    zs, idss = z[o], ids[o]
+    nr = 3000 if side_log2 < 14 else 200
+    x0 = g.integers(0, 1 << 16, size=nr)
+    y0 = g.integers(0, 1 << 16, size=nr)
+    x1 = np.minimum(x0 + g.integers(0, 1 << side_log2, size=nr), 65535)
+    y1 = np.minimum(y0 + g.integers(0, 1 << side_log2, size=nr), 65535)
+    x0, y0, x1, y1 = (a.astype(np.uint16) for a in (x0, y0, x1, y1))
+    ec, eo, ei = orc.rect_search(zs, idss, x0, y0, x1, y1)
+    with bt.Tree.build(dev(zs, cuda), dev(idss, cuda)) as t:
+        c, off, got = bt.rect_search(t, dev(x0, cuda), dev(y0, cuda), dev(x1, cuda), dev(y1, cuda))
+    assert np.array_equal(c.cpu().numpy(), ec)
+    assert np.array_equal(off.cpu().numpy(), eo)
+    assert np.array_equal(got.cpu().numpy(), ei)
+
+
+def test_rect_search_empty_tree_and_inverted_boxes(bt, cuda):
+    u = lambda v: dev(np.array(v, dtype=np.uint16), cuda)  # noqa: E731
+    z = np.zeros(0, dtype=np.uint32)
+    with bt.Tree.build(dev(z, cuda), dev(z, cuda)) as t:
+        c, off, got = bt.rect_search(t, u([0, 5]), u([0, 5]), u([65535, 9]), u([65535, 9]))
+        assert c.cpu().numpy().tolist() == [0, 0] and got.numel() == 0
+    z = np.arange(0, 1 << 20, 7, dtype=np.uint32)
+    with bt.Tree.build(dev(z, cuda), dev(z, cuda)) as t:
+        c, off, got = bt.rect_search(t, u([10, 3]), u([0, 8]), u([9, 3]), u([65535, 2]))
+        assert c.cpu().numpy().tolist() == [0, 0] and got.numel() == 0
