@@ -448,24 +448,89 @@ range_fill_kernel(const unsigned char *__restrict__ leaves, const uint64_t *__re
     }
 }
 
-// Sorts each query's ID segment when values do not ascend with keys.
-// Segments up to kSortCap values are sorted by one CTA with an in-shared-
-// memory bitonic network; longer ones are listed and sorted afterwards, one
-// CTA each, by a bitonic network over a padded copy in global memory.
+// Sorts each query's ID segment when values do not ascend with keys, in
+// three tiers by length.  Up to kWarpSortCap values: one warp copies the
+// segment to shared memory and every value's final slot is its rank (values
+// below it, plus equal values before it -- stable), written straight back.
+// Up to kSortCap: one CTA per segment, bitonic network in shared memory; the
+// warp pass lists these segments.  Longer: listed afterwards and sorted one
+// CTA each by a bitonic network over a padded copy in global memory.
+constexpr int kWarpSortCap = 256;
 constexpr int kSortCap = 4096;
+constexpr unsigned int kMedListCap = 1u << 16;
+constexpr int kWSortThreads = 256;
 
+// Rank of each of the lane's M values (value index lane + 32 m) among the c
+// values of b; writes each to seg[rank].
+template <typename V, int M>
+__device__ __forceinline__ void rank_scatter(const V *b, uint32_t c, int lane, V *seg) {
+    V v[M];
+    uint32_t r[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) {
+        const uint32_t e = lane + 32u * m;
+        v[m] = e < c ? b[e] : (V)0;
+        r[m] = 0;
+    }
+    for (uint32_t j = 0; j < c; j++) {
+        const V w = b[j];  // same address for the whole warp: a broadcast
+#pragma unroll
+        for (int m = 0; m < M; m++)
+            r[m] += (w < v[m]) | ((w == v[m]) & (j < lane + 32u * m));
+    }
+#pragma unroll
+    for (int m = 0; m < M; m++)
+        if (lane + 32u * m < c) seg[r[m]] = v[m];
+}
+
+// stat[0]: segments of kWarpSortCap < c <= kSortCap (listed in med_list up
+// to kMedListCap); stat[1]: set if a segment is longer than kSortCap.
+template <typename V>
+__global__ void __launch_bounds__(kWSortThreads)
+warp_segment_sort_kernel(const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off,
+                         uint64_t nq, V *__restrict__ ids, unsigned int *__restrict__ stat,
+                         uint64_t *__restrict__ med_list) {
+    __shared__ V buf[kWSortThreads / 32][kWarpSortCap];
+    const int lane = threadIdx.x & 31;
+    V *b = buf[threadIdx.x >> 5];
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nq; i += nw) {
+        const uint64_t c = cnt[i];
+        if (c < 2) continue;
+        if (c > (uint64_t)kWarpSortCap) {
+            if (lane == 0) {
+                if (c > (uint64_t)kSortCap) {
+                    atomicOr(&stat[1], 1u);
+                } else {
+                    const unsigned int k = atomicAdd(&stat[0], 1u);
+                    if (k < kMedListCap) med_list[k] = i;
+                }
+            }
+            continue;
+        }
+        V *seg = ids + off[i];
+        for (uint32_t k = lane; k < (uint32_t)c; k += 32) b[k] = seg[k];
+        __syncwarp();
+        const uint32_t cc = (uint32_t)c;
+        if (cc <= 32) rank_scatter<V, 1>(b, cc, lane, seg);
+        else if (cc <= 64) rank_scatter<V, 2>(b, cc, lane, seg);
+        else if (cc <= 128) rank_scatter<V, 4>(b, cc, lane, seg);
+        else rank_scatter<V, 8>(b, cc, lane, seg);
+        __syncwarp();
+    }
+}
+
+// One CTA per medium segment: the listed ones (list != null, n entries), or
+// every segment with kWarpSortCap < c <= kSortCap (list == null, n = nq).
 template <typename V>
 __global__ void __launch_bounds__(512)
 segment_sort_kernel(const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off,
-                    uint64_t nq, V *__restrict__ ids, unsigned int *__restrict__ too_long) {
+                    const uint64_t *__restrict__ list, uint64_t n, V *__restrict__ ids) {
     __shared__ V buf[kSortCap];
-    for (uint64_t i = blockIdx.x; i < nq; i += gridDim.x) {
+    for (uint64_t li = blockIdx.x; li < n; li += gridDim.x) {
+        const uint64_t i = list ? list[li] : li;
         const uint64_t c = cnt[i];
-        if (c < 2) continue;
-        if (c > kSortCap) {
-            if (threadIdx.x == 0) atomicOr(too_long, 1u);
-            continue;
-        }
+        if (c <= (uint64_t)kWarpSortCap || c > (uint64_t)kSortCap) continue;
         uint32_t p2 = 1;
         while (p2 < c) p2 <<= 1;
         V *seg = ids + off[i];
@@ -602,22 +667,45 @@ bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64
 bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
                               uint64_t nq, void *d_ids, cudaStream_t s) {
     if (nq == 0) return BT_OK;
-    unsigned int *flag = nullptr;
-    bt_status st = ws_alloc((void **)&flag, sizeof(unsigned int), s);
+    unsigned int *stat = nullptr;
+    uint64_t *med = nullptr;
+    bt_status st = ws_alloc((void **)&stat, 2 * sizeof(unsigned int), s);
     if (st != BT_OK) return st;
-    BT_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), s));
-    const unsigned g2 = (unsigned)std::min<uint64_t>(nq, (uint64_t)sm_count() * 4);
+    st = ws_alloc((void **)&med, kMedListCap * sizeof(uint64_t), s);
+    if (st != BT_OK) {
+        ws_free(stat, s);
+        return st;
+    }
+    BT_CUDA(cudaMemsetAsync(stat, 0, 2 * sizeof(unsigned int), s));
+    const unsigned gw = (unsigned)std::min<uint64_t>((nq + kWSortThreads / 32 - 1) / (kWSortThreads / 32),
+                                                     (uint64_t)sm_count() * 8);
     count_launch();
     if (t->val_bytes == 4)
-        segment_sort_kernel<uint32_t><<<g2, 512, 0, s>>>(d_counts, d_offsets, nq, (uint32_t *)d_ids,
-                                                         flag);
+        warp_segment_sort_kernel<uint32_t><<<gw, kWSortThreads, 0, s>>>(d_counts, d_offsets, nq,
+                                                                        (uint32_t *)d_ids, stat, med);
     else
-        segment_sort_kernel<uint64_t><<<g2, 512, 0, s>>>(d_counts, d_offsets, nq, (uint64_t *)d_ids,
-                                                         flag);
-    unsigned int h = 0;
-    BT_CUDA(cudaMemcpyAsync(&h, flag, sizeof(h), cudaMemcpyDeviceToHost, s));
+        warp_segment_sort_kernel<uint64_t><<<gw, kWSortThreads, 0, s>>>(d_counts, d_offsets, nq,
+                                                                        (uint64_t *)d_ids, stat, med);
+    unsigned int h[2] = {0, 0};
+    BT_CUDA(cudaMemcpyAsync(h, stat, sizeof(h), cudaMemcpyDeviceToHost, s));
     BT_CUDA(cudaStreamSynchronize(s));
-    if (!h) {
+    if (h[0] > 0) {
+        // medium segments: the list, or (if it overflowed) every segment
+        const bool listed = h[0] <= kMedListCap;
+        const uint64_t n = listed ? h[0] : nq;
+        const unsigned g2 = (unsigned)std::min<uint64_t>(n, (uint64_t)sm_count() * 4);
+        count_launch();
+        if (t->val_bytes == 4)
+            segment_sort_kernel<uint32_t><<<g2, 512, 0, s>>>(d_counts, d_offsets, listed ? med : nullptr,
+                                                             n, (uint32_t *)d_ids);
+        else
+            segment_sort_kernel<uint64_t><<<g2, 512, 0, s>>>(d_counts, d_offsets, listed ? med : nullptr,
+                                                             n, (uint64_t *)d_ids);
+        BT_CUDA(cudaGetLastError());
+    }
+    ws_free(med, s);
+    unsigned int *flag = stat;
+    if (!h[1]) {
         ws_free(flag, s);
         return BT_OK;
     }

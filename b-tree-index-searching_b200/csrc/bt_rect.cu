@@ -183,14 +183,21 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
         uint64_t c = total;
         uint64_t P;
         const uint64_t poff = warp_excl_scan(cell.full ? 0 : len, lane, P);
-        for (uint64_t base = 0; base < P; base += 32) {
-            const uint64_t k = base + lane;
-            const int jc = find_cell(poff, k);
-            const uint64_t lb_j = __shfl_sync(0xffffffffu, b, jc);
-            const uint64_t off_j = __shfl_sync(0xffffffffu, poff, jc);
-            const bool inside =
-                k < P && in_box(key_at_pos(leaves, lb_j + (k - off_j), LG::S, LG::BS), x0, y0, x1, y1);
-            c += __popc(__ballot_sync(0xffffffffu, inside));
+        for (uint64_t base = 0; base < P; base += 64) {  // two loads in flight per lane
+            uint32_t key[2];
+            bool act[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const uint64_t k = base + 32 * h + lane;
+                const int jc = find_cell(poff, k);
+                const uint64_t lb_j = __shfl_sync(0xffffffffu, b, jc);
+                const uint64_t off_j = __shfl_sync(0xffffffffu, poff, jc);
+                act[h] = k < P;
+                key[h] = act[h] ? key_at_pos(leaves, lb_j + (k - off_j), LG::S, LG::BS) : 0u;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                c += __popc(__ballot_sync(0xffffffffu, act[h] && in_box(key[h], x0, y0, x1, y1)));
         }
         if (lane == 0) counts[i] = c;
         if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2((uint32_t)b, (uint32_t)len);
@@ -218,19 +225,29 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
         uint64_t T;
         const uint64_t off = warp_excl_scan(run.y, lane, T);
         uint64_t out = offsets[i];
-        for (uint64_t base = 0; base < T; base += 32) {
-            const uint64_t k = base + lane;
-            const int jc = find_cell(off, k);
-            const uint64_t p = (uint64_t)__shfl_sync(0xffffffffu, run.x, jc) +
-                               (k - __shfl_sync(0xffffffffu, off, jc));
-            const bool full = __shfl_sync(0xffffffffu, (int)cell.full, jc) != 0;
-            const bool inside =
-                k < T && (full || in_box(key_at_pos(leaves, p, LG::S, LG::BS), x0, y0, x1, y1));
-            const unsigned hit = __ballot_sync(0xffffffffu, inside);
-            if (inside)
-                ids[out + __popc(hit & lt)] =
-                    reinterpret_cast<const V *>(leaves + (p / LG::S) * LG::BS + kSectorBytes)[p % LG::S];
-            out += __popc(hit);
+        for (uint64_t base = 0; base < T; base += 64) {  // two chunks' loads in flight
+            uint32_t key[2];
+            V val[2];
+            bool act[2], full[2];
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const uint64_t k = base + 32 * h + lane;
+                const int jc = find_cell(off, k);
+                const uint64_t p = (uint64_t)__shfl_sync(0xffffffffu, run.x, jc) +
+                                   (k - __shfl_sync(0xffffffffu, off, jc));
+                full[h] = __shfl_sync(0xffffffffu, (int)cell.full, jc) != 0;
+                act[h] = k < T;
+                const unsigned char *blk = leaves + (p / LG::S) * LG::BS;
+                key[h] = act[h] && !full[h] ? reinterpret_cast<const uint32_t *>(blk)[p % LG::S] : 0u;
+                val[h] = act[h] ? reinterpret_cast<const V *>(blk + kSectorBytes)[p % LG::S] : (V)0;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const bool inside = act[h] && (full[h] || in_box(key[h], x0, y0, x1, y1));
+                const unsigned hit = __ballot_sync(0xffffffffu, inside);
+                if (inside) ids[out + __popc(hit & lt)] = val[h];
+                out += __popc(hit);
+            }
         }
     }
 }

@@ -113,3 +113,25 @@ def test_range_ids_long_unsorted_segments(bt, orc, cuda):
         c, o, ids = t.range_search(dev(lo, cuda), dev(hi, cuda))
     assert np.array_equal(c.cpu().numpy(), ec)
     assert np.array_equal(ids.cpu().numpy(), ei)
+
+
+@pytest.mark.parametrize("nr,wmin,width", [(5000, 1, 40), (3000, 1, 200), (2000, 1, 1500),
+                                           (70000, 257, 300)])
+def test_range_ids_unsorted_segment_tiers(bt, orc, cuda, nr, wmin, width):
+    """Unsorted values in every segment-sort tier: warp ranking (<= 256
+    values, with duplicate values), one CTA per listed segment (<= 4096), and
+    more medium segments than the list holds (70000 x ~300 values)."""
+    g = np.random.default_rng(nr + width)
+    keys = np.unique(g.integers(0, 1 << 32, size=1 << 20, dtype=np.uint64)).astype(np.uint32)
+    vals = g.permutation(len(keys)).astype(np.uint32)
+    m = len(vals[1::7])
+    vals[0:7 * m:7] = vals[1::7]  # duplicate values
+    r = g.integers(0, len(keys) - width, size=nr)
+    w = g.integers(wmin, width + 1, size=nr)
+    lo, hi = keys[r], keys[r + w - 1]
+    ec, eo, ei = orc.range_search(keys, vals, lo, hi)
+    with bt.Tree.build(dev(keys, cuda), dev(vals, cuda)) as t:
+        c, o, ids = t.range_search(dev(lo, cuda), dev(hi, cuda))
+    assert np.array_equal(c.cpu().numpy(), ec)
+    assert np.array_equal(o.cpu().numpy(), eo)
+    assert np.array_equal(ids.cpu().numpy(), ei)
