@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "bt_internal.cuh"
+#include "bt_sort.cuh"
 
 namespace bt {
 namespace {
@@ -449,50 +450,25 @@ range_fill_kernel(const unsigned char *__restrict__ leaves, const uint64_t *__re
 }
 
 // Sorts each query's ID segment when values do not ascend with keys, in
-// three tiers by length.  Up to kWarpSortCap values: one warp copies the
-// segment to shared memory and every value's final slot is its rank (values
-// below it, plus equal values before it -- stable), written straight back.
-// Up to kSortCap: one CTA per segment, bitonic network in shared memory; the
-// warp pass lists these segments.  Longer: listed afterwards and sorted one
-// CTA each by a bitonic network over a padded copy in global memory.
-constexpr int kWarpSortCap = 256;
+// three tiers by length.  Up to kWarpSortCap values: one warp sorts the
+// segment in registers (warp_sort_small, a bitonic network) and writes it
+// back.  Up to kSortCap: one CTA per segment, bitonic network in shared
+// memory; the warp pass lists these segments.  Longer: listed afterwards and
+// sorted one CTA each by a bitonic network over a padded copy in global
+// memory.
 constexpr int kSortCap = 4096;
 constexpr unsigned int kMedListCap = 1u << 16;
 constexpr int kWSortThreads = 256;
 
-// Rank of each of the lane's M values (value index lane + 32 m) among the c
-// values of b; writes each to seg[rank].
-template <typename V, int M>
-__device__ __forceinline__ void rank_scatter(const V *b, uint32_t c, int lane, V *seg) {
-    V v[M];
-    uint32_t r[M];
-#pragma unroll
-    for (int m = 0; m < M; m++) {
-        const uint32_t e = lane + 32u * m;
-        v[m] = e < c ? b[e] : (V)0;
-        r[m] = 0;
-    }
-    for (uint32_t j = 0; j < c; j++) {
-        const V w = b[j];  // same address for the whole warp: a broadcast
-#pragma unroll
-        for (int m = 0; m < M; m++)
-            r[m] += (w < v[m]) | ((w == v[m]) & (j < lane + 32u * m));
-    }
-#pragma unroll
-    for (int m = 0; m < M; m++)
-        if (lane + 32u * m < c) seg[r[m]] = v[m];
-}
-
 // stat[0]: segments of kWarpSortCap < c <= kSortCap (listed in med_list up
-// to kMedListCap); stat[1]: set if a segment is longer than kSortCap.
+// to kMedListCap); stat[1]: set if a segment is longer than kSortCap.  With
+// skip_small, segments of up to kWarpSortCap values are already sorted.
 template <typename V>
 __global__ void __launch_bounds__(kWSortThreads)
 warp_segment_sort_kernel(const uint64_t *__restrict__ cnt, const uint64_t *__restrict__ off,
                          uint64_t nq, V *__restrict__ ids, unsigned int *__restrict__ stat,
-                         uint64_t *__restrict__ med_list) {
-    __shared__ V buf[kWSortThreads / 32][kWarpSortCap];
+                         uint64_t *__restrict__ med_list, bool skip_small) {
     const int lane = threadIdx.x & 31;
-    V *b = buf[threadIdx.x >> 5];
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nq; i += nw) {
         const uint64_t c = cnt[i];
@@ -508,15 +484,9 @@ warp_segment_sort_kernel(const uint64_t *__restrict__ cnt, const uint64_t *__res
             }
             continue;
         }
+        if (skip_small) continue;
         V *seg = ids + off[i];
-        for (uint32_t k = lane; k < (uint32_t)c; k += 32) b[k] = seg[k];
-        __syncwarp();
-        const uint32_t cc = (uint32_t)c;
-        if (cc <= 32) rank_scatter<V, 1>(b, cc, lane, seg);
-        else if (cc <= 64) rank_scatter<V, 2>(b, cc, lane, seg);
-        else if (cc <= 128) rank_scatter<V, 4>(b, cc, lane, seg);
-        else rank_scatter<V, 8>(b, cc, lane, seg);
-        __syncwarp();
+        warp_sort_small<V>(seg, seg, (uint32_t)c, lane);
     }
 }
 
@@ -665,7 +635,7 @@ bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64
 }
 
 bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
-                              uint64_t nq, void *d_ids, cudaStream_t s) {
+                              uint64_t nq, void *d_ids, cudaStream_t s, bool small_sorted) {
     if (nq == 0) return BT_OK;
     unsigned int *stat = nullptr;
     uint64_t *med = nullptr;
@@ -682,10 +652,12 @@ bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const 
     count_launch();
     if (t->val_bytes == 4)
         warp_segment_sort_kernel<uint32_t><<<gw, kWSortThreads, 0, s>>>(d_counts, d_offsets, nq,
-                                                                        (uint32_t *)d_ids, stat, med);
+                                                                        (uint32_t *)d_ids, stat, med,
+                                                                        small_sorted);
     else
         warp_segment_sort_kernel<uint64_t><<<gw, kWSortThreads, 0, s>>>(d_counts, d_offsets, nq,
-                                                                        (uint64_t *)d_ids, stat, med);
+                                                                        (uint64_t *)d_ids, stat, med,
+                                                                        small_sorted);
     unsigned int h[2] = {0, 0};
     BT_CUDA(cudaMemcpyAsync(h, stat, sizeof(h), cudaMemcpyDeviceToHost, s));
     BT_CUDA(cudaStreamSynchronize(s));

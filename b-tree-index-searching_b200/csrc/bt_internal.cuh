@@ -174,9 +174,10 @@ bt_status launch_partition_point_prealloc(const bt_tree *t, const void *d_q, uin
                                           cudaStream_t s);
 bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
                             const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
-// Sorts each segment ids[offsets[i] .. + counts[i]) ascending (value width of t).
+// Sorts each segment ids[offsets[i] .. + counts[i]) ascending (value width
+// of t).  small_sorted: segments of up to 256 values are sorted already.
 bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
-                              uint64_t nseg, void *d_ids, cudaStream_t s);
+                              uint64_t nseg, void *d_ids, cudaStream_t s, bool small_sorted = false);
 
 // (lanes per query, rounds) -> index of the search configuration table in
 // bt_search.cu, or -1.

@@ -20,6 +20,7 @@
 #include <algorithm>
 
 #include "bt_search.cuh"
+#include "bt_sort.cuh"
 
 namespace bt {
 namespace {
@@ -27,15 +28,6 @@ namespace {
 constexpr int kRThreads = 512;
 constexpr int kRWarps = kRThreads / 32;
 constexpr int kMaxCells = 16;
-
-__device__ __forceinline__ uint32_t compact16(uint32_t v) {
-    v &= 0x55555555u;
-    v = (v | (v >> 1)) & 0x33333333u;
-    v = (v | (v >> 2)) & 0x0F0F0F0Fu;
-    v = (v | (v >> 4)) & 0x00FF00FFu;
-    v = (v | (v >> 8)) & 0x0000FFFFu;
-    return v;
-}
 
 __device__ __forceinline__ uint32_t spread16d(uint32_t v) {
     v &= 0xFFFFu;
@@ -46,11 +38,18 @@ __device__ __forceinline__ uint32_t spread16d(uint32_t v) {
     return v;
 }
 
-__device__ __forceinline__ bool in_box(uint32_t z, uint32_t x0, uint32_t y0, uint32_t x1,
-                                       uint32_t y1) {
-    const uint32_t x = compact16(z), y = compact16(z >> 1);
-    return x >= x0 && x <= x1 && y >= y0 && y <= y1;
-}
+// A box in code space.  Spreading a coordinate's bits apart is strictly
+// monotone, so x in [x0, x1] holds exactly when the code's x bits (the even
+// ones) lie in [spread(x0), spread(x1)]; likewise y in the odd bits.
+struct ZBox {
+    uint32_t x0, x1, y0, y1;
+    __device__ __forceinline__ ZBox(uint32_t bx0, uint32_t by0, uint32_t bx1, uint32_t by1)
+        : x0(spread16d(bx0)), x1(spread16d(bx1)), y0(spread16d(by0) << 1), y1(spread16d(by1) << 1) {}
+    __device__ __forceinline__ bool holds(uint32_t z) const {
+        const uint32_t zx = z & 0x55555555u, zy = z & 0xAAAAAAAAu;
+        return zx >= x0 && zx <= x1 && zy >= y0 && zy <= y1;
+    }
+};
 
 // The cover of one box: cells of side 2^c, nx per row; cell j of the lane.
 struct Cell {
@@ -60,9 +59,12 @@ struct Cell {
 };
 
 __device__ __forceinline__ Cell box_cell(uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1, int j) {
-    int c = 0;
-    uint32_t nx = x1 - x0 + 1, ny = y1 - y0 + 1;
-    while ((uint64_t)nx * ny > (uint64_t)kMaxCells) {  // c = 16 gives one cell
+    // A side of s cells of size 2^c spans at least s / 2^c cells, so every
+    // c below floor(log2(s)) - 4 needs more than 16: start there.
+    const uint32_t s = max(x1 - x0, y1 - y0) + 1u;
+    int c = max(0, 31 - __clz((int)s) - 4);
+    uint32_t nx = (x1 >> c) - (x0 >> c) + 1, ny = (y1 >> c) - (y0 >> c) + 1;
+    while (nx * ny > (uint32_t)kMaxCells) {  // c = 16 gives one cell; nx, ny <= 32 here
         c++;
         nx = (x1 >> c) - (x0 >> c) + 1;
         ny = (y1 >> c) - (y0 >> c) + 1;
@@ -81,10 +83,10 @@ __device__ __forceinline__ Cell box_cell(uint32_t x0, uint32_t y0, uint32_t x1, 
 // Lanes 0-15 receive the first key position of cell `lane`, lanes 16-31 the
 // position after the last key of cell `lane - 16`: lower bounds of the
 // cells' first codes and upper bounds of their last codes, 32 descents in
-// one round (G lanes per descent, G/1 descents per group).
+// one round (G lanes per descent, G descents per group).  n < 2^32.
 template <typename V, int G>
-__device__ __forceinline__ uint64_t cell_bounds(const DevTree &t, const uint32_t *s_lvl,
-                                                uint64_t *res, const Cell &cell, int lane) {
+__device__ __forceinline__ uint32_t cell_bounds(const DevTree &t, const uint32_t *s_lvl,
+                                                uint32_t *res, const Cell &cell, int lane) {
     using LG = LeafGeom<uint32_t, V>;
     constexpr int NG = 32 / G;
     constexpr int I = G;
@@ -112,19 +114,19 @@ __device__ __forceinline__ uint64_t cell_bounds(const DevTree &t, const uint32_t
                                   gl, pos);
 #pragma unroll
     for (int s = 0; s < I; s++)
-        if (gl == 0) res[s * NG + grp] = (uint64_t)node[s] * LG::S + pos[s];
+        if (gl == 0) res[s * NG + grp] = node[s] * (uint32_t)LG::S + (uint32_t)pos[s];
     __syncwarp();
-    const uint64_t r = beyond ? t.n : res[lane];
+    const uint32_t r = beyond ? (uint32_t)t.n : res[lane];
     __syncwarp();
     return r;
 }
 
 // Exclusive prefix sum over the warp.
-__device__ __forceinline__ uint64_t warp_excl_scan(uint64_t v, int lane, uint64_t &total) {
-    uint64_t x = v;
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, int lane, uint32_t &total) {
+    uint32_t x = v;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        const uint64_t y = __shfl_up_sync(0xffffffffu, x, d);
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
         if (lane >= d) x += y;
     }
     total = __shfl_sync(0xffffffffu, x, 31);
@@ -133,22 +135,24 @@ __device__ __forceinline__ uint64_t warp_excl_scan(uint64_t v, int lane, uint64_
 
 // Cell (0..15) whose run holds item k of the concatenated runs, given each
 // lane's exclusive offset `off` (cells past the last hold offset = total).
-__device__ __forceinline__ int find_cell(uint64_t off, uint64_t k) {
+__device__ __forceinline__ int find_cell(uint32_t off, uint32_t k) {
     int j = 0;
 #pragma unroll
     for (int step = kMaxCells / 2; step >= 1; step >>= 1) {
-        const uint64_t o = __shfl_sync(0xffffffffu, off, j + step);
+        const uint32_t o = __shfl_sync(0xffffffffu, off, j + step);
         if (o <= k) j += step;
     }
     return j;
 }
 
-__device__ __forceinline__ uint32_t key_at_pos(const unsigned char *leaves, uint64_t p, int S, int BS) {
-    return reinterpret_cast<const uint32_t *>(leaves + (p / S) * BS)[p % S];
+template <typename V>
+__device__ __forceinline__ const unsigned char *block_of(const unsigned char *leaves, uint32_t p) {
+    using LG = LeafGeom<uint32_t, V>;
+    return leaves + (size_t)(p / LG::S) * LG::BS;
 }
 
 // Count pass: counts[i] = points in box i; runs[i * 16 + j] = (first key
-// position, length) of cell j's run (positions fit 32 bits: n < 2^32).
+// position, length) of cell j's run.
 template <typename V>
 __global__ void __launch_bounds__(kRThreads, 2)
 rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
@@ -157,7 +161,7 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
                   uint2 *__restrict__ runs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t *s_lvl = reinterpret_cast<uint32_t *>(smem_raw);
-    uint64_t *res = reinterpret_cast<uint64_t *>(smem_raw + (((size_t)t.smem_bytes + 15) / 16 * 16)) +
+    uint32_t *res = reinterpret_cast<uint32_t *>(smem_raw + (((size_t)t.smem_bytes + 15) / 16 * 16)) +
                     (threadIdx.x >> 5) * 32;
     stage_level<uint32_t>(s_lvl, t);
     __syncthreads();
@@ -173,81 +177,93 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
             if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2(0u, 0u);
             continue;
         }
+        const ZBox box(x0, y0, x1, y1);
         const Cell cell = box_cell(x0, y0, x1, y1, j);
-        const uint64_t b = cell_bounds<V, 4>(t, s_lvl, res, cell, lane);
-        const uint64_t ub = __shfl_sync(0xffffffffu, b, lane + kMaxCells);
-        const uint64_t len = (lane < kMaxCells && cell.valid && ub > b) ? ub - b : 0;
-        uint64_t total;
+        const uint32_t b = cell_bounds<V, 4>(t, s_lvl, res, cell, lane);
+        const uint32_t ub = __shfl_sync(0xffffffffu, b, (lane + kMaxCells) & 31);
+        const uint32_t len = (lane < kMaxCells && cell.valid && ub > b) ? ub - b : 0u;
+        uint32_t total;
         // whole runs of the cells inside the box; edge cells are scanned
-        warp_excl_scan(cell.full ? len : 0, lane, total);
+        warp_excl_scan(cell.full ? len : 0u, lane, total);
         uint64_t c = total;
-        uint64_t P;
-        const uint64_t poff = warp_excl_scan(cell.full ? 0 : len, lane, P);
-        for (uint64_t base = 0; base < P; base += 64) {  // two loads in flight per lane
+        uint32_t P;
+        const uint32_t poff = warp_excl_scan(cell.full ? 0u : len, lane, P);
+        for (uint32_t base = 0; base < P; base += 64) {  // two loads in flight per lane
             uint32_t key[2];
             bool act[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const uint64_t k = base + 32 * h + lane;
+                const uint32_t k = base + 32 * h + lane;
                 const int jc = find_cell(poff, k);
-                const uint64_t lb_j = __shfl_sync(0xffffffffu, b, jc);
-                const uint64_t off_j = __shfl_sync(0xffffffffu, poff, jc);
+                const uint32_t p = __shfl_sync(0xffffffffu, b, jc) + (k - __shfl_sync(0xffffffffu, poff, jc));
                 act[h] = k < P;
-                key[h] = act[h] ? key_at_pos(leaves, lb_j + (k - off_j), LG::S, LG::BS) : 0u;
+                key[h] = act[h] ? reinterpret_cast<const uint32_t *>(block_of<V>(leaves, p))[p % LG::S] : 0u;
             }
 #pragma unroll
-            for (int h = 0; h < 2; h++)
-                c += __popc(__ballot_sync(0xffffffffu, act[h] && in_box(key[h], x0, y0, x1, y1)));
+            for (int h = 0; h < 2; h++) c += __popc(__ballot_sync(0xffffffffu, act[h] && box.holds(key[h])));
         }
         if (lane == 0) counts[i] = c;
-        if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2((uint32_t)b, (uint32_t)len);
+        if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2(b, len);
     }
 }
 
-// Fill pass: the IDs of box i's points at ids[offsets[i] ..], cell by cell
-// (sorted afterwards).
+// Fill pass: the IDs of box i's points at ids[offsets[i] ..].  A box with at
+// most kWarpSortCap points gathers them in shared memory and writes them
+// sorted (warp_sort_small); larger ones are written cell by cell and sorted
+// afterwards.
 template <typename V>
 __global__ void __launch_bounds__(kRThreads)
 rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
                  const uint16_t *__restrict__ y0s, const uint16_t *__restrict__ x1s,
                  const uint16_t *__restrict__ y1s, uint64_t nr, const uint2 *__restrict__ runs,
-                 const uint64_t *__restrict__ offsets, V *__restrict__ ids) {
+                 const uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
+                 V *__restrict__ ids) {
+    __shared__ V s_buf[kRWarps][kWarpSortCap];
     using LG = LeafGeom<uint32_t, V>;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
+    V *buf = s_buf[threadIdx.x >> 5];
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
     for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nr;
          i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
         const uint32_t x0 = x0s[i], y0 = y0s[i], x1 = x1s[i], y1 = y1s[i];
-        if (x0 > x1 || y0 > y1) continue;
+        const uint64_t cnt = counts[i];
+        if (x0 > x1 || y0 > y1 || cnt == 0) continue;
+        const ZBox box(x0, y0, x1, y1);
         const Cell cell = box_cell(x0, y0, x1, y1, lane % kMaxCells);
         const uint2 run = lane < kMaxCells ? runs[i * kMaxCells + lane] : make_uint2(0u, 0u);
-        uint64_t T;
-        const uint64_t off = warp_excl_scan(run.y, lane, T);
-        uint64_t out = offsets[i];
-        for (uint64_t base = 0; base < T; base += 64) {  // two chunks' loads in flight
+        const bool buffered = cnt <= (uint64_t)kWarpSortCap;
+        V *dst = buffered ? buf : ids + offsets[i];
+        uint32_t T;
+        const uint32_t off = warp_excl_scan(run.y, lane, T);
+        uint32_t out = 0;
+        for (uint32_t base = 0; base < T; base += 64) {  // two chunks' loads in flight
             uint32_t key[2];
             V val[2];
             bool act[2], full[2];
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const uint64_t k = base + 32 * h + lane;
+                const uint32_t k = base + 32 * h + lane;
                 const int jc = find_cell(off, k);
-                const uint64_t p = (uint64_t)__shfl_sync(0xffffffffu, run.x, jc) +
-                                   (k - __shfl_sync(0xffffffffu, off, jc));
+                const uint32_t p = __shfl_sync(0xffffffffu, run.x, jc) + (k - __shfl_sync(0xffffffffu, off, jc));
                 full[h] = __shfl_sync(0xffffffffu, (int)cell.full, jc) != 0;
                 act[h] = k < T;
-                const unsigned char *blk = leaves + (p / LG::S) * LG::BS;
+                const unsigned char *blk = block_of<V>(leaves, p);
                 key[h] = act[h] && !full[h] ? reinterpret_cast<const uint32_t *>(blk)[p % LG::S] : 0u;
                 val[h] = act[h] ? reinterpret_cast<const V *>(blk + kSectorBytes)[p % LG::S] : (V)0;
             }
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const bool inside = act[h] && (full[h] || in_box(key[h], x0, y0, x1, y1));
+                const bool inside = act[h] && (full[h] || box.holds(key[h]));
                 const unsigned hit = __ballot_sync(0xffffffffu, inside);
-                if (inside) ids[out + __popc(hit & lt)] = val[h];
+                if (inside) dst[out + __popc(hit & lt)] = val[h];
                 out += __popc(hit);
             }
+        }
+        if (buffered) {
+            __syncwarp();
+            warp_sort_small<V>(buf, ids + offsets[i], (uint32_t)cnt, lane);
+            __syncwarp();
         }
     }
 }
@@ -256,7 +272,7 @@ template <typename V>
 bt_status rect_impl(const bt_tree *t, const uint16_t *x0, const uint16_t *y0, const uint16_t *x1,
                     const uint16_t *y1, uint64_t nr, uint64_t *counts, uint64_t *offsets,
                     void *ids, uint64_t cap, uint64_t *h_total, cudaStream_t s) {
-    const size_t smem = ((size_t)t->dev.smem_bytes + 15) / 16 * 16 + (size_t)kRWarps * 32 * sizeof(uint64_t);
+    const size_t smem = ((size_t)t->dev.smem_bytes + 15) / 16 * 16 + (size_t)kRWarps * 32 * sizeof(uint32_t);
     auto kc = rect_count_kernel<V>;
     auto kf = rect_fill_kernel<V>;
     if (smem > 48 * 1024)
@@ -295,10 +311,10 @@ bt_status rect_impl(const bt_tree *t, const uint16_t *x0, const uint16_t *y0, co
             const unsigned fgrid = (unsigned)std::max<uint64_t>(
                 1, std::min<uint64_t>((nr + kRWarps - 1) / kRWarps, (uint64_t)sm_count() * 4));
             count_launch();
-            kf<<<fgrid, kRThreads, 0, s>>>(t->dev, x0, y0, x1, y1, nr, runs, offsets, (V *)ids);
+            kf<<<fgrid, kRThreads, 0, s>>>(t->dev, x0, y0, x1, y1, nr, runs, counts, offsets, (V *)ids);
             e = cudaGetLastError();
             if (e != cudaSuccess) st = cuda_fail(e, "rectangle fill pass");
-            if (st == BT_OK) st = launch_segment_sort(t, counts, offsets, nr, ids, s);
+            if (st == BT_OK) st = launch_segment_sort(t, counts, offsets, nr, ids, s, true);
         }
     }
     ws_free(d_total, s);
