@@ -112,6 +112,118 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     }
 }
 
+// Point search over radix-grouped input (the queries ordered by their top
+// kPointGroupBits bits, as bt_group_queries leaves them).  One CTA per SM
+// takes a contiguous run of the grouped batch.  For the group of its current
+// queries it stages in shared memory the group's window of the deepest
+// separator level whose window fits (for 2^26 u32 keys and 256 groups: the
+// 32,768 leaf-block maxima of the bottom level, 128 KB), so that one binary
+// search in shared memory takes a query straight to its leaf block: the only
+// global access left is the leaf block itself.  The window of a group [lo,
+// hi] is the level's entries from the lower bound of lo to the lower bound
+// of hi; every query of the group has its lower bound inside it.  Warps whose
+// tile holds a query of another group (tiles at group boundaries, or input
+// that is not grouped at all) take the full descent from the root instead,
+// so results never depend on the order of the input.
+constexpr int kWinThreads = 1024;
+constexpr int kWinWarps = kWinThreads / 32;
+constexpr size_t kWinBytes = 192 * 1024;
+// Below this batch size a window staged per CTA costs more than it saves.
+constexpr uint64_t kWinMinQueries = 1ull << 21;
+
+template <typename K, typename V, int G, int R>
+__global__ void __launch_bounds__(kWinThreads, 1)
+point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
+                    const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out, int shift) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *s_win = reinterpret_cast<K *>(smem_raw);
+    __shared__ uint32_t s_blk[2];
+    constexpr uint32_t kCap = (uint32_t)(kWinBytes / sizeof(K));
+    constexpr int F = kLineBytes / (int)sizeof(K);
+    constexpr int LOGF = F == 32 ? 5 : 4;
+    constexpr uint32_t ROW = sizeof(K) == 4 ? 32u : 16u;  // swizzle row (elements)
+    constexpr int NG = 32 / G;
+    constexpr int I = G / R;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int grp = lane / G;
+    const int gl = lane % G;
+    const K tmax = (K)t.max_key;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    const K *seps = static_cast<const K *>(t.seps);
+    const uint64_t ntiles = (nq + 31) / 32;
+    const uint64_t per_cta = (ntiles + gridDim.x - 1) / gridDim.x;
+    const uint64_t c_begin = blockIdx.x * per_cta;
+    const uint64_t c_end = min(ntiles, c_begin + per_cta);
+    uint64_t staged = ~0ull;  // group whose window is staged (same in every thread)
+    int wlvl = 0;
+    uint32_t w0 = 0, wm = 1;
+    for (uint64_t t0 = c_begin; t0 < c_end; t0 += kWinWarps) {
+        const uint64_t b = (uint64_t)q[t0 * 32] >> shift;  // group of this step's first query
+        if (b != staged) {
+            __syncthreads();  // the old window is no longer read
+            if (threadIdx.x < 2) {
+                const uint64_t lo = b << shift;
+                const uint64_t hi = lo | ((1ull << shift) - 1ull);
+                const uint64_t k = threadIdx.x == 0 ? lo : hi;
+                s_blk[threadIdx.x] = block_lower_bound<K>(t, k < (uint64_t)tmax ? (K)k : tmax);
+            }
+            __syncthreads();
+            // deepest level whose window fits (level 0 holds at most F entries)
+            const uint32_t blo = s_blk[0], bhi = s_blk[1];
+            wlvl = t.nlevels - 1;
+            int sh = 0;
+            while (wlvl > 0 && (bhi >> sh) - (blo >> sh) + 1u > kCap) {
+                wlvl--;
+                sh += LOGF;
+            }
+            w0 = blo >> sh;
+            wm = (bhi >> sh) - w0 + 1u;
+            const K *src = seps + t.lvl_off[wlvl] + w0;
+            const uint32_t staged_n = (wm + ROW - 1) / ROW * ROW;
+            for (uint32_t i = threadIdx.x; i < staged_n; i += blockDim.x)
+                s_win[swz<K>(i)] = i < wm ? src[i] : key_max<K>();
+            __syncthreads();
+            staged = b;
+        }
+        const uint64_t tile = t0 + warp;
+        if (tile >= c_end) continue;
+        const uint64_t base = tile * 32;
+        const uint64_t my = base + lane;
+        const K myq = my < nq ? q[my] : (K)0;
+        const K myqe = myq < tmax ? myq : tmax;
+        // phase 1: the window, or (whole warp) the descent from the root
+        const bool inwin = my >= nq || ((uint64_t)myq >> shift) == staged;
+        const bool win = __all_sync(0xffffffffu, inwin);
+        uint32_t mynode = 0;
+        if (win) {
+            const uint32_t p = smem_bound<K>(s_win, wm, myqe, false);
+            mynode = w0 + (p < wm ? p : wm - 1u);
+        }
+        const int from = win ? wlvl + 1 : 0;
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            K qv[I], qe[I];
+            bool up[I];
+            uint32_t node[I];
+#pragma unroll
+            for (int s = 0; s < I; s++) {
+                const int k = r * (NG * I) + s * NG + grp;
+                qv[s] = __shfl_sync(0xffffffffu, myq, k);
+                node[s] = __shfl_sync(0xffffffffu, mynode, k);
+                qe[s] = qv[s] < tmax ? qv[s] : tmax;
+                up[s] = false;
+            }
+            walk_from<K, G, I>(t, from, qe, up, node, grp, gl);
+            leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
+                const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
+                if (qi >= nq) return nullptr;
+                return out + perm[qi];
+            });
+        }
+    }
+}
+
 // Lower bound of lo and upper bound of hi per query: 64 descents per warp
 // tile of 32 queries (d < 32: lower bound of query d, else upper bound of
 // query d - 32), passed in 2R rounds.  counts[i] = ub - lb (0 if lo > hi);
@@ -256,9 +368,33 @@ bt_status point_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm
     return BT_OK;
 }
 
+template <typename K, typename V, int G, int R>
+bt_status window_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
+                        void *d_out, cudaStream_t s) {
+    auto fn = point_window_kernel<K, V, G, R>;
+    bt_status st = set_smem(fn, kWinBytes);
+    if (st != BT_OK) return st;
+    const uint64_t ntiles = (nq + 31) / 32;
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, sm_count()));
+    const int shift = 8 * t->key_bytes - kPointGroupBits;
+    count_launch();
+    fn<<<grid, kWinThreads, kWinBytes, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out, shift);
+    BT_CUDA(cudaGetLastError());
+    return BT_OK;
+}
+
 template <typename K, typename V, bool PERM>
 bt_status point_cfg(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
                     void *d_out, cudaStream_t s) {
+    if (PERM && nq >= kWinMinQueries) {
+        switch (t->search_cfg) {
+            case 0: return window_launch<K, V, 8, 1>(t, d_q, d_perm, nq, d_out, s);
+            case 1: return window_launch<K, V, 8, 2>(t, d_q, d_perm, nq, d_out, s);
+            case 2: return window_launch<K, V, 4, 1>(t, d_q, d_perm, nq, d_out, s);
+            case 3: return window_launch<K, V, 4, 2>(t, d_q, d_perm, nq, d_out, s);
+            default: return window_launch<K, V, 2, 1>(t, d_q, d_perm, nq, d_out, s);
+        }
+    }
     switch (t->search_cfg) {
         case 0: return point_launch<K, V, 8, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
         case 1: return point_launch<K, V, 8, 2, PERM>(t, d_q, d_perm, nq, d_out, s);

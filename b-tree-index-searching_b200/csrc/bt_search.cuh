@@ -120,12 +120,36 @@ __device__ __forceinline__ void level_step(const K *__restrict__ lp, const K (&q
 // to stay on real separators.  On entry node[s] is the node index on level
 // smem_level + 1 (phase 1's result); on return it is the leaf block index.
 template <typename K, int G, int I>
+__device__ __forceinline__ void walk_from(const DevTree &t, int from, const K (&qe)[I],
+                                          const bool (&upper)[I], uint32_t (&node)[I], int grp,
+                                          int gl) {
+    const K *gseps = static_cast<const K *>(t.seps);
+    for (int lvl = from; lvl < t.nlevels; lvl++)
+        level_step<K, G, I>(gseps + t.lvl_off[lvl], qe, upper, node, grp, gl);
+}
+
+template <typename K, int G, int I>
 __device__ __forceinline__ void walk_global(const DevTree &t, const K (&qe)[I],
                                             const bool (&upper)[I], uint32_t (&node)[I], int grp,
                                             int gl) {
-    const K *gseps = static_cast<const K *>(t.seps);
-    for (int lvl = t.smem_level + 1; lvl < t.nlevels; lvl++)
-        level_step<K, G, I>(gseps + t.lvl_off[lvl], qe, upper, node, grp, gl);
+    walk_from<K, G, I>(t, t.smem_level + 1, qe, upper, node, grp, gl);
+}
+
+// Leaf block holding the lower bound of q (q <= max key) by one thread:
+// every separator line from the root, scanned whole.
+template <typename K>
+__device__ __forceinline__ uint32_t block_lower_bound(const DevTree &t, K q) {
+    constexpr int F = kLineBytes / (int)sizeof(K);
+    const K *seps = static_cast<const K *>(t.seps);
+    uint32_t node = 0;
+    for (int lvl = 0; lvl < t.nlevels; lvl++) {
+        const K *line = seps + t.lvl_off[lvl] + (size_t)node * F;
+        uint32_t c = 0;
+#pragma unroll
+        for (int i = 0; i < F; i++) c += line[i] < q ? 1u : 0u;
+        node = node * F + c;
+    }
+    return node;
 }
 
 // Shared-memory slot of sorted element p.  A binary search over 2^k
