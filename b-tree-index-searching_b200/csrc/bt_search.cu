@@ -86,6 +86,7 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
         // phase 1: one lane per query, binary search of the staged level
         const uint64_t my = base + lane;
         const K myq = my < nq ? q[my] : (K)0;
+        const uint32_t myperm = PERM && my < nq ? perm[my] : 0u;  // loaded early
         const uint32_t mynode = smem_bound<K>(s_lvl, t.smem_entries, myq < tmax ? myq : tmax, false);
 
         // phase 2: G lanes per query through the global levels and the leaf
@@ -93,12 +94,13 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
         for (int r = 0; r < R; r++) {
             K qv[I], qe[I];
             bool up[I];
-            uint32_t node[I];
+            uint32_t node[I], pv[I];
 #pragma unroll
             for (int s = 0; s < I; s++) {
                 const int k = r * (NG * I) + s * NG + grp;  // query of the tile
                 qv[s] = __shfl_sync(0xffffffffu, myq, k);
                 node[s] = __shfl_sync(0xffffffffu, mynode, k);
+                pv[s] = PERM ? __shfl_sync(0xffffffffu, myperm, k) : 0u;
                 qe[s] = qv[s] < tmax ? qv[s] : tmax;
                 up[s] = false;
             }
@@ -106,7 +108,7 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
             leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
                 const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
                 if (qi >= nq) return nullptr;
-                return out + (PERM ? (uint64_t)perm[qi] : qi);
+                return out + (PERM ? (uint64_t)pv[s] : qi);
             });
         }
     }
@@ -191,6 +193,7 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
         const uint64_t base = tile * 32;
         const uint64_t my = base + lane;
         const K myq = my < nq ? q[my] : (K)0;
+        const uint32_t myperm = my < nq ? perm[my] : 0u;  // loaded early, off the critical path
         const K myqe = myq < tmax ? myq : tmax;
         // phase 1: the window, or (whole warp) the descent from the root
         const bool inwin = my >= nq || ((uint64_t)myq >> shift) == staged;
@@ -205,12 +208,13 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
         for (int r = 0; r < R; r++) {
             K qv[I], qe[I];
             bool up[I];
-            uint32_t node[I];
+            uint32_t node[I], pv[I];
 #pragma unroll
             for (int s = 0; s < I; s++) {
                 const int k = r * (NG * I) + s * NG + grp;
                 qv[s] = __shfl_sync(0xffffffffu, myq, k);
                 node[s] = __shfl_sync(0xffffffffu, mynode, k);
+                pv[s] = __shfl_sync(0xffffffffu, myperm, k);
                 qe[s] = qv[s] < tmax ? qv[s] : tmax;
                 up[s] = false;
             }
@@ -218,7 +222,7 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
             leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
                 const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
                 if (qi >= nq) return nullptr;
-                return out + perm[qi];
+                return out + pv[s];
             });
         }
     }

@@ -48,13 +48,21 @@ __device__ __forceinline__ void load_bytes(const void *p, uint32_t (&v)[NB / 4])
     }
 }
 
+// L2 policy for data touched once per query: its lines are the first the
+// L2 evicts, so the separator levels and the result lines stay resident.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 // 16-byte load of data touched once per query (leaf blocks): read-only path,
-// no L1 allocation, so L1 keeps the separator lines.
+// no L1 allocation (L1 keeps the separator lines), evict-first in L2.
 __device__ __forceinline__ uint4 load_stream16(const void *p) {
     uint4 x;
-    asm volatile("ld.global.nc.L1::no_allocate.v4.b32 {%0,%1,%2,%3}, [%4];"
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.b32 {%0,%1,%2,%3}, [%4], %5;"
                  : "=r"(x.x), "=r"(x.y), "=r"(x.z), "=r"(x.w)
-                 : "l"(p));
+                 : "l"(p), "l"(l2_evict_first()));
     return x;
 }
 

@@ -664,7 +664,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": None if tq is None else tq * nq,
-                         "kernel": "point_kernel (grouped batch)",
+                         "kernel": "point_window_kernel (grouped batch)",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "kernel_ms": statistics.mean(search_ms)},
             "cpu_baseline": cpu,
