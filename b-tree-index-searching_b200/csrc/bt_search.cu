@@ -228,101 +228,6 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     }
 }
 
-// The same for u32 keys with one thread per query all the way: I queries per
-// lane (a warp tile is 32 * I queries), the window search in shared memory,
-// the levels below the window (if any) by walk_scalar, then the whole leaf
-// block loaded into registers.  With no lanes spent on cooperation, a warp
-// keeps 32 * I leaf blocks in flight.
-template <typename V, int I>
-__global__ void __launch_bounds__(kWinThreads, 1)
-point_window1_kernel(const __grid_constant__ DevTree t, const uint32_t *__restrict__ q,
-                     const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out, int shift) {
-    using K = uint32_t;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *s_win = reinterpret_cast<K *>(smem_raw);
-    __shared__ uint32_t s_blk[2];
-    constexpr uint32_t kCap = (uint32_t)(kWinBytes / sizeof(K));
-    constexpr int LOGF = 5;
-    constexpr uint32_t ROW = 32u;
-    constexpr uint64_t TQ = 32 * I;  // queries per warp tile
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    const K tmax = (K)t.max_key;
-    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    const K *seps = static_cast<const K *>(t.seps);
-    const uint64_t ntiles = (nq + TQ - 1) / TQ;
-    const uint64_t per_cta = (ntiles + gridDim.x - 1) / gridDim.x;
-    const uint64_t c_begin = blockIdx.x * per_cta;
-    const uint64_t c_end = min(ntiles, c_begin + per_cta);
-    uint64_t staged = ~0ull;
-    int wlvl = 0;
-    uint32_t w0 = 0, wm = 1;
-    for (uint64_t t0 = c_begin; t0 < c_end; t0 += kWinWarps) {
-        const uint64_t b = (uint64_t)q[t0 * TQ] >> shift;
-        if (b != staged) {
-            __syncthreads();
-            if (threadIdx.x < 2) {
-                const uint64_t lo = b << shift;
-                const uint64_t hi = lo | ((1ull << shift) - 1ull);
-                const uint64_t k = threadIdx.x == 0 ? lo : hi;
-                s_blk[threadIdx.x] = block_lower_bound<K>(t, k < (uint64_t)tmax ? (K)k : tmax);
-            }
-            __syncthreads();
-            const uint32_t blo = s_blk[0], bhi = s_blk[1];
-            wlvl = t.nlevels - 1;
-            int sh = 0;
-            while (wlvl > 0 && (bhi >> sh) - (blo >> sh) + 1u > kCap) {
-                wlvl--;
-                sh += LOGF;
-            }
-            w0 = blo >> sh;
-            wm = (bhi >> sh) - w0 + 1u;
-            const K *src = seps + t.lvl_off[wlvl] + w0;
-            const uint32_t staged_n = (wm + ROW - 1) / ROW * ROW;
-            for (uint32_t i = threadIdx.x; i < staged_n; i += blockDim.x)
-                s_win[swz<K>(i)] = i < wm ? src[i] : key_max<K>();
-            __syncthreads();
-            staged = b;
-        }
-        const uint64_t tile = t0 + warp;
-        if (tile >= c_end) continue;
-        const uint64_t base = tile * TQ;
-        K qv[I], qe[I];
-        uint32_t pv[I], node[I];
-        bool inwin = true;
-#pragma unroll
-        for (int s = 0; s < I; s++) {
-            const uint64_t i = base + s * 32 + lane;
-            qv[s] = i < nq ? q[i] : (K)0;
-            pv[s] = i < nq ? perm[i] : 0u;
-            qe[s] = qv[s] < tmax ? qv[s] : tmax;
-            inwin &= i >= nq || ((uint64_t)qv[s] >> shift) == staged;
-        }
-        if (__all_sync(0xffffffffu, inwin)) {
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                const uint32_t p = smem_bound<K>(s_win, wm, qe[s], false);
-                node[s] = w0 + (p < wm ? p : wm - 1u);
-            }
-            if (wlvl + 1 < t.nlevels) {
-#pragma unroll
-                for (int s = 0; s < I; s++) node[s] = walk_scalar<K>(t, wlvl + 1, node[s], qe[s]);
-            }
-        } else {  // a tile that mixes groups: the descent from the root
-#pragma unroll
-            for (int s = 0; s < I; s++) node[s] = walk_scalar<K>(t, 0, 0u, qe[s]);
-        }
-        LeafRegs<K, V> lr[I];
-#pragma unroll
-        for (int s = 0; s < I; s++) lr[s].load(leaves, node[s]);
-#pragma unroll
-        for (int s = 0; s < I; s++) {
-            const uint64_t i = base + s * 32 + lane;
-            if (i < nq) out[pv[s]] = lr[s].lookup(qv[s], qe[s], tmax);
-        }
-    }
-}
-
 // Lower bound of lo and upper bound of hi per query: 64 descents per warp
 // tile of 32 queries (d < 32: lower bound of query d, else upper bound of
 // query d - 32), passed in 2R rounds.  counts[i] = ub - lb (0 if lo > hi);
@@ -482,27 +387,9 @@ bt_status window_launch(const bt_tree *t, const void *d_q, const uint32_t *d_per
     return BT_OK;
 }
 
-template <typename V, int I>
-bt_status window1_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
-                         void *d_out, cudaStream_t s) {
-    auto fn = point_window1_kernel<V, I>;
-    bt_status st = set_smem(fn, kWinBytes);
-    if (st != BT_OK) return st;
-    const uint64_t ntiles = (nq + 32 * I - 1) / (32 * I);
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, sm_count()));
-    const int shift = 32 - kPointGroupBits;
-    count_launch();
-    fn<<<grid, kWinThreads, kWinBytes, s>>>(t->dev, (const uint32_t *)d_q, d_perm, nq, (V *)d_out, shift);
-    BT_CUDA(cudaGetLastError());
-    return BT_OK;
-}
-
 template <typename K, typename V, bool PERM>
 bt_status point_cfg(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
                     void *d_out, cudaStream_t s) {
-    if constexpr (PERM && sizeof(K) == 4) {
-        if (nq >= kWinMinQueries) return window1_launch<V, 2>(t, d_q, d_perm, nq, d_out, s);
-    }
     if (PERM && nq >= kWinMinQueries) {
         switch (t->search_cfg) {
             case 0: return window_launch<K, V, 8, 1>(t, d_q, d_perm, nq, d_out, s);

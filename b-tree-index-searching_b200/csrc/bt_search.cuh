@@ -143,26 +143,6 @@ __device__ __forceinline__ void walk_global(const DevTree &t, const K (&qe)[I],
     walk_from<K, G, I>(t, t.smem_level + 1, qe, upper, node, grp, gl);
 }
 
-// Levels from..nlevels-1 by one thread: in each 128-byte node line a binary
-// search for the separators below q (the first probe brings the line into
-// L1, the rest hit it).  node is the node index on level `from`; returns the
-// leaf block.  q must not exceed the max key.
-template <typename K>
-__device__ __forceinline__ uint32_t walk_scalar(const DevTree &t, int from, uint32_t node, K q) {
-    constexpr int F = kLineBytes / (int)sizeof(K);
-    const K *seps = static_cast<const K *>(t.seps);
-    for (int lvl = from; lvl < t.nlevels; lvl++) {
-        const K *line = seps + t.lvl_off[lvl] + (size_t)node * F;
-        uint32_t c = 0;
-#pragma unroll
-        for (int step = F / 2; step >= 1; step >>= 1)
-            if (line[c + step - 1] < q) c += step;
-        c += line[c] < q ? 1u : 0u;
-        node = node * F + c;
-    }
-    return node;
-}
-
 // Leaf block holding the lower bound of q (q <= max key) by one thread:
 // every separator line from the root, scanned whole.
 template <typename K>
@@ -311,51 +291,6 @@ __device__ __forceinline__ void leaf_point(const unsigned char *__restrict__ lea
         }
     }
 }
-
-// One thread per query: the whole leaf block in registers (key chunks, then
-// value chunks).
-template <typename K, typename V>
-struct LeafRegs {
-    using LG = LeafGeom<K, V>;
-    static constexpr int NKC = kSectorBytes / 16;
-    static constexpr int NC = NKC + (LG::VB + 15) / 16;
-    uint4 c[NC];
-
-    __device__ __forceinline__ void load(const unsigned char *leaves, uint32_t blk) {
-        const unsigned char *p = leaves + (size_t)blk * LG::BS;
-#pragma unroll
-        for (int i = 0; i < NC; i++)
-            c[i] = load_stream16(p + (i < NKC ? i * 16 : kSectorBytes + (i - NKC) * 16));
-    }
-    __device__ __forceinline__ uint32_t word(int i) const {  // i: compile-time after unrolling
-        const uint4 &x = c[i / 4];
-        return (i & 3) == 0 ? x.x : (i & 3) == 1 ? x.y : (i & 3) == 2 ? x.z : x.w;
-    }
-    __device__ __forceinline__ K key(int k) const {
-        if constexpr (sizeof(K) == 4) return word(k);
-        else return ((uint64_t)word(2 * k + 1) << 32) | word(2 * k);
-    }
-    __device__ __forceinline__ V value(int k) const {
-        constexpr int W0 = NKC * 4;  // first value word
-        if constexpr (sizeof(V) == 4) return word(W0 + k);
-        else return ((uint64_t)word(W0 + 2 * k + 1) << 32) | word(W0 + 2 * k);
-    }
-    // Value at the lower bound of qe if the key there equals qv, else all-ones.
-    __device__ __forceinline__ V lookup(K qv, K qe, K tmax) const {
-        int cnt = 0;
-        bool eq = false;
-#pragma unroll
-        for (int k = 0; k < LG::S; k++) {
-            const K x = key(k);
-            cnt += x < qe ? 1 : 0;
-            eq |= x == qv;
-        }
-        V v = 0;
-#pragma unroll
-        for (int k = 0; k < LG::S; k++) v = (k == cnt) ? value(k) : v;
-        return (eq && qv <= tmax && cnt < LG::S) ? v : key_max<V>();
-    }
-};
 
 // Lower (upper, per slot) bound slot inside each query's leaf block, keys
 // only; every lane of the group receives pos[s].
