@@ -117,6 +117,7 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
                     K *__restrict__ ob, uint32_t *__restrict__ operm) {
     __shared__ uint32_t cnt[kPWarps][256];
     __shared__ uint32_t tile_start[256];
+    __shared__ uint32_t tile_base[256];  // global start of each digit's run of this tile
     __shared__ uint32_t warp_tot[8];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sa = reinterpret_cast<K *>(smem_raw);
@@ -126,6 +127,7 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kPWarps * 256; i += kPT) (&cnt[0][0])[i] = 0;
+    if (threadIdx.x < 256) tile_base[threadIdx.x] = base[(uint64_t)threadIdx.x * ntiles + blockIdx.x];
     __syncthreads();
 
     const uint64_t t0 = (uint64_t)blockIdx.x * kPTile;
@@ -146,11 +148,15 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
         }
     }
     // Stable rank of every item among the same-digit items of this warp's
-    // sub-tile (item order = j-major, then lane).
+    // sub-tile (item order = j-major, then lane).  The peer masks do not
+    // depend on the counters: take them all first.
     const unsigned lt = (1u << lane) - 1u;
+    unsigned mm[kIPL];
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) mm[j] = __match_any_sync(0xffffffffu, dg[j]);
 #pragma unroll
     for (int j = 0; j < kIPL; j++) {
-        const unsigned m = __match_any_sync(0xffffffffu, dg[j]);
+        const unsigned m = mm[j];
         uint32_t c = 0;
         if (dg[j] != 0xFFFFFFFFu) c = cnt[w][dg[j]];
         __syncwarp();
@@ -191,7 +197,7 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
     const uint32_t tn = (uint32_t)min((uint64_t)kPTile, n - t0);
     for (uint32_t lp = threadIdx.x; lp < tn; lp += kPT) {
         const uint32_t d = sd[lp];
-        const uint64_t g = (uint64_t)base[(uint64_t)d * ntiles + blockIdx.x] + (lp - tile_start[d]);
+        const uint64_t g = (uint64_t)tile_base[d] + (lp - tile_start[d]);
         oa[g] = sa[lp];
         if (HAS_B) ob[g] = sb[lp];
         operm[g] = sp[lp];
