@@ -108,6 +108,7 @@ _PROTOS = {
     "bt_range_count_host": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
     "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
     "bt_kernel_launches": (ctypes.c_uint64, []),
+    "bt_measure_gather": (_I, [_U64, _U64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "bt_set_search_config": (_I, [_P, _I, _I]),
     "bt_point_search_grouped_noalloc": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_train": (_I, [_P, ctypes.POINTER(bt_learned_config), _P,
@@ -550,3 +551,11 @@ def version():
 def kernel_launches():
     """Kernel launches issued by the library so far in this process."""
     return lib().bt_kernel_launches()
+
+
+def measure_gather(region_bytes, n_reads=1 << 24, block_bytes=64):
+    """Random block reads per second the current GPU sustains (bt_measure_gather)."""
+    r = ctypes.c_double(0)
+    _check(lib().bt_measure_gather(region_bytes, n_reads, block_bytes, ctypes.byref(r)),
+           "bt_measure_gather")
+    return r.value

@@ -28,6 +28,7 @@ SOURCES = [
     "bt_server.cu",
     "bt_forest.cu",
     "bt_rect.cu",
+    "bt_probe.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

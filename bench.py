@@ -266,7 +266,7 @@ def run_reference(args):
 # ------------------------------------------ learned index + serving --------
 
 def learned_section(args, device, bt, flush):
-    """2^28 unique u64 keys (cumulative sum of
+    """Learned index and serving workload: 2^28 unique u64 keys (cumulative sum of
     floor(lognormal(4, 2)) + 1 gaps), value = rank; FP32 two-stage model with
     2^16 leaf segments trained on the GPU.  Reports the plain and the learned
     batched point-search throughput on a 2^24-query batch (90% hits uniform
@@ -382,7 +382,7 @@ def _timed_ms(fn, stream, flush, steps):
 
 
 def forest_section(args, device, bt, flush):
-    """4096 trees of round(2^U), U ~ [10, 20], u32
+    """Batched uneven forest workload: 4096 trees of round(2^U), U ~ [10, 20], u32
     keys; per tree round(2^U), U ~ [6, 16], point queries (80% hits) plus 1%
     range queries of width [1, 2^12] ranks; every batch is one launch of a
     captured CUDA graph.  The plan's lanes/rounds and tile are chosen by
@@ -447,7 +447,7 @@ def forest_section(args, device, bt, flush):
 
 
 def rect_section(args, device, bt, flush):
-    """2^24 points (x, y uniform u16) keyed by their
+    """Rectangle workload: 2^24 points (x, y uniform u16) keyed by their
     32-bit Morton code (value = point ID, sorted by (code, ID)); 2^20
     rectangles with a uniform corner and sides uniform in [1, 256].  Timed:
     one bt_rect_search call (count pass, scan, fill pass, per-box ID sort)
@@ -628,10 +628,16 @@ def run_ours(args):
 
     # ---- roofline of the dominant kernel (the grouped search kernel) --------
     kb = vb = 4
-    alg_bytes = nq * (kb + vb + 32) + hits * 32  # per launch, see DESIGN.md
+    # per launch: key in, value out, the leaf block's key sector, and its
+    # value sector on a hit
+    alg_bytes = nq * (kb + vb + 32) + hits * 32
     search_s = statistics.mean(search_ms) / 1000.0
     achieved = alg_bytes / search_s / 1e9
     peak, peak_kind = measured_peak()
+    # the ceiling for one random leaf-block read per query: random 64-byte
+    # reads over a region the size of the tree's leaves, measured here
+    leaf_bytes = -(-len(keys) // (32 // kb)) * 64
+    gather_rps = bt.measure_gather(leaf_bytes, 1 << 24, 64)
     tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
 
     learned = forest = rect = None
@@ -666,7 +672,12 @@ def run_ours(args):
                          "traffic": None if tq is None else tq * nq,
                          "kernel": "point_window_kernel (grouped batch)",
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel_ms": statistics.mean(search_ms)},
+                         "kernel_ms": statistics.mean(search_ms),
+                         "random_gather_ceiling": {
+                             "reads_per_s": gather_rps, "block_bytes": 64,
+                             "region_bytes": leaf_bytes,
+                             "search_queries_per_s": nq / search_s,
+                             "frac": nq / search_s / gather_rps}},
             "cpu_baseline": cpu,
             "clocks": clk,
             "gpu_launches": int(launches),

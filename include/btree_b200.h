@@ -376,6 +376,16 @@ BT_API bt_status bt_server_replay(bt_server *srv, uint64_t nreq, const uint64_t 
  * devices, all threads).  Lets a caller count the device work behind a call. */
 BT_API uint64_t bt_kernel_launches(void);
 
+/* Measurement aid (no counterpart in the reference): reads n_reads blocks of
+ * block_bytes (32, 64 or 128) at uniformly random aligned addresses of a
+ * region_bytes buffer on the current device, 16 bytes per lane, L1 bypassed
+ * and L2 flushed first, and returns the best of three timed runs in random
+ * reads per second.  A point search that misses the cache makes one such read
+ * per query, so this is the ceiling its throughput is set against.  Allocates
+ * and frees its own buffers; synchronous. */
+BT_API bt_status bt_measure_gather(uint64_t region_bytes, uint64_t n_reads, uint32_t block_bytes,
+                                   double *reads_per_s);
+
 #ifdef __cplusplus
 }
 #endif
