@@ -55,6 +55,10 @@ def parse_args(argv=None):
     p.add_argument("--serve-rate", type=float, default=20000.0, help="requests per second")
     p.add_argument("--no-forest", action="store_true", help="skip the 4096-tree forest section")
     p.add_argument("--no-rect", action="store_true", help="skip the rectangle-search section")
+    p.add_argument("--rect-boxes-log2", type=int, default=20, help="boxes in the rectangle section")
+    p.add_argument("--only", choices=["learned", "forest", "rect"],
+                   help="run one extension section alone on cuda:0 and print its JSON object "
+                        "(for profiling; not the bench line)")
     return p.parse_args(argv)
 
 
@@ -457,7 +461,7 @@ def rect_section(args, device, bt, flush):
     import ctypes
     import torch
     wl = importlib.import_module(PKG + ".workloads")
-    z, ids, x0, y0, x1, y1 = wl.zorder_points()
+    z, ids, x0, y0, x1, y1 = wl.zorder_points(n_rects=1 << args.rect_boxes_log2)
     stream = torch.cuda.current_stream(device)
     tree = bt.Tree.build(torch.from_numpy(z).to(device), torch.from_numpy(ids).to(device))
     d = [torch.from_numpy(a).to(device) for a in (x0, y0, x1, y1)]
@@ -482,7 +486,7 @@ def rect_section(args, device, bt, flush):
     zid = np.empty(len(z), dtype=np.uint32)
     zid[ids] = z
     ok = True
-    for i in range(2048):
+    for i in range(min(2048, len(x0))):
         h = got[int(off[i]):int(off[i] + c[i])]
         hz = zid[h]
         hx, hy = (wl.compact_u16(hz), wl.compact_u16(hz >> np.uint32(1)))
@@ -702,10 +706,23 @@ def run_ours(args):
     return 0
 
 
+def run_only(args):
+    import torch
+    bt = importlib.import_module(PKG)
+    device = torch.device("cuda:0")
+    torch.cuda.set_device(device)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    fn = {"learned": learned_section, "forest": forest_section, "rect": rect_section}[args.only]
+    print(json.dumps(fn(args, device, bt, flush)), flush=True)
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.only:
+        return run_only(args)
     return run_ours(args)
 
 
