@@ -118,6 +118,7 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
     __shared__ uint32_t cnt[kPWarps][256];
     __shared__ uint32_t tile_start[256];
     __shared__ uint32_t tile_base[256];  // global start of each digit's run of this tile
+    __shared__ uint32_t digit_tot[256];  // items of each digit in this tile
     __shared__ uint32_t warp_tot[8];
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *sa = reinterpret_cast<K *>(smem_raw);
@@ -154,26 +155,42 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
     unsigned mm[kIPL];
 #pragma unroll
     for (int j = 0; j < kIPL; j++) mm[j] = __match_any_sync(0xffffffffu, dg[j]);
+    // Rows in order: each row's leader of a digit adds the row's count to the
+    // warp's counter and hands the old value to its peers (the next row's
+    // atomic comes after this row's shuffle, so the order is the item order).
 #pragma unroll
     for (int j = 0; j < kIPL; j++) {
         const unsigned m = mm[j];
+        const int leader = __ffs(m) - 1;
         uint32_t c = 0;
-        if (dg[j] != 0xFFFFFFFFu) c = cnt[w][dg[j]];
-        __syncwarp();
-        if (dg[j] != 0xFFFFFFFFu && lane == __ffs(m) - 1) cnt[w][dg[j]] = c + __popc(m);
-        __syncwarp();
+        if (dg[j] != 0xFFFFFFFFu && lane == leader) c = atomicAdd(&cnt[w][dg[j]], (uint32_t)__popc(m));
+        c = __shfl_sync(0xffffffffu, c, leader);
         rk[j] = c + __popc(m & lt);
     }
     __syncthreads();
-    uint32_t tot = 0;
-    if (threadIdx.x < 256) {
-        const int d = threadIdx.x;
-        for (int ww = 0; ww < kPWarps; ww++) {
-            const uint32_t c = cnt[ww][d];
-            cnt[ww][d] = tot;
-            tot += c;
+    // Per digit: exclusive prefix over the 16 warps, and the tile total.
+    // Warp ww handles digits 16 ww .. 16 ww + 15, half a lane-row each of
+    // the warps 0-7 and 8-15.
+    {
+        const int d = 16 * w + (lane & 15);
+        const int h = lane >> 4;
+        uint32_t v[kPWarps / 2], run = 0;
+#pragma unroll
+        for (int k = 0; k < kPWarps / 2; k++) v[k] = cnt[(kPWarps / 2) * h + k][d];
+        uint32_t half_tot = 0;
+#pragma unroll
+        for (int k = 0; k < kPWarps / 2; k++) half_tot += v[k];
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, half_tot, 16);
+        run = h ? other : 0u;
+#pragma unroll
+        for (int k = 0; k < kPWarps / 2; k++) {
+            cnt[(kPWarps / 2) * h + k][d] = run;
+            run += v[k];
         }
+        if (h == 0) digit_tot[d] = half_tot + other;
     }
+    __syncthreads();
+    uint32_t tot = threadIdx.x < 256 ? digit_tot[threadIdx.x] : 0u;
     uint32_t ex = 0;
     if (threadIdx.x < 256) ex = block_exscan256(tot, warp_tot);
     __syncthreads();
