@@ -28,24 +28,28 @@ bt_status check_tree(const bt_tree *t) {
     return BT_OK;
 }
 
-// Two non-blocking streams per device for the host-buffer pipelines.
+// Non-blocking streams per device for the host-buffer pipelines, one per
+// buffer slot.  Chunk i runs on slot i % kPipeSlots: its H2D copy waits only
+// for the D2H copy of chunk i - kPipeSlots, so with three slots the
+// host-to-device engine keeps copying while the device-to-host engine drains
+// the two chunks before (PCIe carries both directions at once).
+constexpr int kPipeSlots = 3;
 struct PipeStreams {
-    cudaStream_t s[2] = {nullptr, nullptr};
+    cudaStream_t s[kPipeSlots] = {};
     bool ready = false;
 };
 std::mutex g_pipe_mu;
 PipeStreams g_pipe[64];
 
-bt_status pipe_streams(int dev, cudaStream_t (&out)[2]) {
+bt_status pipe_streams(int dev, cudaStream_t (&out)[kPipeSlots]) {
     std::lock_guard<std::mutex> lk(g_pipe_mu);
     PipeStreams &p = g_pipe[dev];
     if (!p.ready) {
-        for (int i = 0; i < 2; i++)
+        for (int i = 0; i < kPipeSlots; i++)
             BT_CUDA(cudaStreamCreateWithFlags(&p.s[i], cudaStreamNonBlocking));
         p.ready = true;
     }
-    out[0] = p.s[0];
-    out[1] = p.s[1];
+    for (int i = 0; i < kPipeSlots; i++) out[i] = p.s[i];
     return BT_OK;
 }
 
@@ -93,22 +97,22 @@ template <typename Run>
 bt_status host_pipeline(const bt_tree *t, cudaStream_t caller, uint64_t nq, uint64_t chunk,
                         int n_in, const void *const *h_in, const size_t *in_w, void *h_out,
                         size_t out_w, Run run) {
-    cudaStream_t ps[2];
+    cudaStream_t ps[kPipeSlots];
     bt_status st = pipe_streams(t->device, ps);
     if (st != BT_OK) return st;
     cudaEvent_t ev;
     BT_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     cudaEventRecord(ev, caller);
-    for (int i = 0; i < 2; i++) cudaStreamWaitEvent(ps[i], ev, 0);
-    void *din[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
-    void *dout[2] = {nullptr, nullptr};
+    for (int i = 0; i < kPipeSlots; i++) cudaStreamWaitEvent(ps[i], ev, 0);
+    void *din[kPipeSlots][2] = {};
+    void *dout[kPipeSlots] = {};
     const uint64_t cap = std::min(chunk, nq);
-    for (int i = 0; i < 2 && st == BT_OK; i++) {
+    for (int i = 0; i < kPipeSlots && st == BT_OK; i++) {
         for (int k = 0; k < n_in && st == BT_OK; k++) st = ws_alloc(&din[i][k], cap * in_w[k], ps[i]);
         if (st == BT_OK) st = ws_alloc(&dout[i], cap * out_w, ps[i]);
     }
     for (uint64_t c0 = 0, ci = 0; c0 < nq && st == BT_OK; c0 += chunk, ci++) {
-        const int slot = (int)(ci & 1);
+        const int slot = (int)(ci % kPipeSlots);
         cudaStream_t s = ps[slot];
         const uint64_t m = std::min(chunk, nq - c0);
         for (int k = 0; k < n_in && st == BT_OK; k++) {
@@ -123,24 +127,27 @@ bt_status host_pipeline(const bt_tree *t, cudaStream_t caller, uint64_t nq, uint
             if (e != cudaSuccess) st = cuda_fail(e, "cudaMemcpyAsync D2H");
         }
     }
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kPipeSlots; i++) {
         for (int k = 0; k < n_in; k++) ws_free(din[i][k], ps[i]);
         ws_free(dout[i], ps[i]);
     }
-    cudaError_t e0 = cudaStreamSynchronize(ps[0]);
-    cudaError_t e1 = cudaStreamSynchronize(ps[1]);
+    cudaError_t es = cudaSuccess;
+    for (int i = 0; i < kPipeSlots; i++) {
+        const cudaError_t e = cudaStreamSynchronize(ps[i]);
+        if (es == cudaSuccess) es = e;
+    }
     cudaEventDestroy(ev);
     if (st != BT_OK) return st;
-    if (e0 != cudaSuccess) return cuda_fail(e0, "cudaStreamSynchronize");
-    if (e1 != cudaSuccess) return cuda_fail(e1, "cudaStreamSynchronize");
+    if (es != cudaSuccess) return cuda_fail(es, "cudaStreamSynchronize");
     return BT_OK;
 }
 
 uint64_t pipeline_chunk(uint64_t nq) {
-    // Four chunks or more for large batches (copy/compute overlap), but not
-    // below 1M queries (per-chunk launch and grouping overheads).
-    const uint64_t c = (nq + 3) / 4;
-    return std::max<uint64_t>(c, std::min<uint64_t>(nq, 1ull << 20));
+    // Eight chunks or more for large batches (copy/compute overlap), but not
+    // below 2M queries (per-chunk launch and grouping overheads; the grouped
+    // search's window kernel starts at 2^21 queries).
+    const uint64_t c = (nq + 7) / 8;
+    return std::max<uint64_t>(c, std::min<uint64_t>(nq, 1ull << 21));
 }
 
 }  // namespace
