@@ -160,16 +160,6 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     uint64_t staged = ~0ull;  // group whose window is staged (same in every thread)
     int wlvl = 0;
     uint32_t w0 = 0, wm = 1;
-    // Software pipeline across a warp's tiles (one round per tile, u32 keys,
-    // at most 4 lanes per query -- wider states spill): the leaf blocks of
-    // one tile are in flight while the next tile's queries are read and
-    // searched in the window; the previous tile is finished after that.
-    constexpr bool PIPE = R == 1 && G <= 4 && sizeof(K) == 4;
-    bool pend = false;
-    uint64_t pbase = 0;
-    K pqv[I];
-    uint32_t ppv[I];
-    LeafChunks<K, V, G, I> pch;
     for (uint64_t t0 = c_begin; t0 < c_end; t0 += kWinWarps) {
         const uint64_t b = (uint64_t)q[t0 * 32] >> shift;  // group of this step's first query
         if (b != staged) {
@@ -214,39 +204,6 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
             mynode = w0 + (p < wm ? p : wm - 1u);
         }
         const int from = win ? wlvl + 1 : 0;
-        if constexpr (PIPE) {
-            K qv[I], qe[I];
-            bool up[I];
-            uint32_t node[I], pv[I];
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                const int k = s * NG + grp;
-                qv[s] = __shfl_sync(0xffffffffu, myq, k);
-                node[s] = __shfl_sync(0xffffffffu, mynode, k);
-                pv[s] = __shfl_sync(0xffffffffu, myperm, k);
-                qe[s] = qv[s] < tmax ? qv[s] : tmax;
-                up[s] = false;
-            }
-            walk_from<K, G, I>(t, from, qe, up, node, grp, gl);
-            if (pend) {
-                K pqe[I];
-#pragma unroll
-                for (int s = 0; s < I; s++) pqe[s] = pqv[s] < tmax ? pqv[s] : tmax;
-                leaf_finish<K, V, G, I>(pch, pqv, pqe, tmax, grp, gl, [&](int s) -> V * {
-                    const uint64_t qi = pbase + (uint64_t)(s * NG + grp);
-                    return qi < nq ? out + ppv[s] : nullptr;
-                });
-            }
-            leaf_issue<K, V, G, I>(leaves, node, gl, pch);
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                pqv[s] = qv[s];
-                ppv[s] = pv[s];
-            }
-            pbase = base;
-            pend = true;
-            continue;
-        }
 #pragma unroll
         for (int r = 0; r < R; r++) {
             K qv[I], qe[I];
@@ -268,15 +225,6 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
                 return out + pv[s];
             });
         }
-    }
-    if (PIPE && pend) {
-        K pqe[I];
-#pragma unroll
-        for (int s = 0; s < I; s++) pqe[s] = pqv[s] < tmax ? pqv[s] : tmax;
-        leaf_finish<K, V, G, I>(pch, pqv, pqe, tmax, grp, gl, [&](int s) -> V * {
-            const uint64_t qi = pbase + (uint64_t)(s * NG + grp);
-            return qi < nq ? out + ppv[s] : nullptr;
-        });
     }
 }
 

@@ -215,17 +215,19 @@ struct LeafStage {
     static constexpr int KCPL = (NKC + G - 1) / G;       // key chunks per lane
 };
 
-template <typename K, typename V, int G, int I>
-using LeafChunks = uint32_t[I][LeafStage<K, V, G>::CPL][4];
-
-// First half of leaf_point: issue the loads of each slot's leaf block (the
-// registers fill in the background; nothing waits for them here).
-template <typename K, typename V, int G, int I>
-__device__ __forceinline__ void leaf_issue(const unsigned char *__restrict__ leaves,
-                                           const uint32_t (&node)[I], int gl,
-                                           LeafChunks<K, V, G, I> &ch) {
+// Leaf stage of I point queries.  Each query's leaf block (key chunks, then
+// value chunks) is loaded by its lane group with 16-byte streaming loads, the
+// lower-bound slot and the match are found, and the lane holding the value
+// writes it -- or all-ones on a miss -- to dst(s); dst returns null to skip
+// a slot.  leaves points at leaf block 0 of the tree; node[s] is the block.
+template <typename K, typename V, int G, int I, typename Dst>
+__device__ __forceinline__ void leaf_point(const unsigned char *__restrict__ leaves,
+                                           const uint32_t (&node)[I], const K (&qv)[I],
+                                           const K (&qe)[I], K tmax, int grp, int gl, Dst dst) {
     using LG = LeafGeom<K, V>;
     using LS = LeafStage<K, V, G>;
+    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
+    uint32_t ch[I][LS::CPL][4];
 #pragma unroll
     for (int s = 0; s < I; s++) {
         const unsigned char *blk = leaves + (size_t)node[s] * LG::BS;
@@ -242,17 +244,6 @@ __device__ __forceinline__ void leaf_issue(const unsigned char *__restrict__ lea
             }
         }
     }
-}
-
-// Second half: find each slot's lower-bound position and match in the
-// loaded block; the lane holding the value writes it -- or all-ones on a
-// miss -- to dst(s) (dst returns null to skip a slot).
-template <typename K, typename V, int G, int I, typename Dst>
-__device__ __forceinline__ void leaf_finish(const LeafChunks<K, V, G, I> &ch, const K (&qv)[I],
-                                            const K (&qe)[I], K tmax, int grp, int gl, Dst dst) {
-    using LG = LeafGeom<K, V>;
-    using LS = LeafStage<K, V, G>;
-    const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
 #pragma unroll
     for (int s = 0; s < I; s++) {
         int cnt = 0;
@@ -299,20 +290,6 @@ __device__ __forceinline__ void leaf_finish(const LeafChunks<K, V, G, I> &ch, co
             }
         }
     }
-}
-
-// Leaf stage of I point queries.  Each query's leaf block (key chunks, then
-// value chunks) is loaded by its lane group with 16-byte streaming loads, the
-// lower-bound slot and the match are found, and the lane holding the value
-// writes it -- or all-ones on a miss -- to dst(s); dst returns null to skip
-// a slot.  leaves points at leaf block 0 of the tree; node[s] is the block.
-template <typename K, typename V, int G, int I, typename Dst>
-__device__ __forceinline__ void leaf_point(const unsigned char *__restrict__ leaves,
-                                           const uint32_t (&node)[I], const K (&qv)[I],
-                                           const K (&qe)[I], K tmax, int grp, int gl, Dst dst) {
-    LeafChunks<K, V, G, I> ch;
-    leaf_issue<K, V, G, I>(leaves, node, gl, ch);
-    leaf_finish<K, V, G, I>(ch, qv, qe, tmax, grp, gl, dst);
 }
 
 // Lower (upper, per slot) bound slot inside each query's leaf block, keys
