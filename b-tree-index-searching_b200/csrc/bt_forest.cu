@@ -39,6 +39,8 @@ struct FItem {
     uint32_t kind;  // 0 point, 1 range
     uint64_t begin;
     uint64_t count;
+    int32_t slvl;  // separator level staged in shared memory for this item, -1 for none
+    uint32_t sm;   // its entries (a whole number of 128-byte nodes)
 };
 
 // --------------------------------------------------------------- build ----
@@ -264,6 +266,8 @@ bt_status forest_build_impl(bt_forest *f, const void *d_keys, const void *d_vals
 // --------------------------------------------------------------- search ---
 
 constexpr int kFThreads = 256;
+constexpr int kFWarps = kFThreads / 32;
+constexpr size_t kFStageBytes = 16 * 1024;  // separator level staged per work item
 
 struct ForestDev {
     const FTree *desc;
@@ -271,26 +275,36 @@ struct ForestDev {
     const void *seps;
 };
 
+// One CTA per work item (one tree, up to `tile` queries of one kind), taken
+// from a device queue so trees of very different sizes balance.  For an
+// item with enough queries the CTA stages the deepest separator level of its
+// tree that fits in 16 KB (chosen on the host: the item's slvl/sm); a binary
+// search there resolves every level above it, the remaining levels and the
+// leaf are walked by lane groups as in the single-tree kernels.
 template <typename K, typename V, int G, int R>
-__global__ void __launch_bounds__(kFThreads)
+__global__ void __launch_bounds__(kFThreads, 3)
 forest_kernel(const __grid_constant__ ForestDev f, const FItem *__restrict__ items, uint64_t n_items,
               unsigned long long *__restrict__ counter, const K *__restrict__ q,
               V *__restrict__ out, const K *__restrict__ lo, const K *__restrict__ hi,
               uint64_t *__restrict__ counts) {
-    __shared__ uint64_t s_res[kFThreads / 32][64];
+    __shared__ __align__(16) K s_lvl[kFStageBytes / sizeof(K)];
+    __shared__ uint64_t s_res[kFWarps][64];
+    __shared__ unsigned long long s_item;
     using LG = LeafGeom<K, V>;
     constexpr int NG = 32 / G;
     constexpr int I = G / R;
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const int grp = lane / G;
     const int gl = lane % G;
-    uint64_t *res = s_res[threadIdx.x >> 5];
+    uint64_t *res = s_res[warp];
     const K *seps = static_cast<const K *>(f.seps);
 
     for (;;) {
-        unsigned long long it = 0;
-        if (lane == 0) it = atomicAdd(counter, 1ull);
-        it = __shfl_sync(0xffffffffu, it, 0);
+        __syncthreads();  // the previous item's staged level is no longer read
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1ull);
+        __syncthreads();
+        const unsigned long long it = s_item;
         if (it >= n_items) break;
         const FItem w = items[it];
         const FTree &d = f.desc[w.tree];
@@ -299,10 +313,25 @@ forest_kernel(const __grid_constant__ ForestDev f, const FItem *__restrict__ ite
         const K tmax = (K)d.max_key;
         const K *tseps = seps + d.sep0;
         const unsigned char *tleaves = f.leaves + d.block0 * LG::BS;
-        for (uint64_t sub = 0; sub < w.count; sub += 32) {
+        const int sl = n > 0 ? w.slvl : -1;
+        if (sl >= 0) {
+            const K *src = tseps + d.lvl_off[sl];
+            for (uint32_t i = threadIdx.x; i < w.sm; i += kFThreads) s_lvl[swz<K>(i)] = src[i];
+            __syncthreads();
+        }
+        const int from = sl + 1;  // first level walked in global memory
+        for (uint64_t sub = (uint64_t)warp * 32; sub < w.count; sub += kFWarps * 32) {
             const uint64_t base = w.begin + sub;
             const uint64_t end = w.begin + w.count;
+            const uint64_t my = base + lane;
             if (w.kind == 0) {
+                const K myq = my < end ? q[my] : (K)0;
+                if (n == 0) {
+                    if (my < end) out[my] = key_max<V>();
+                    continue;
+                }
+                const K myqe = myq < tmax ? myq : tmax;
+                const uint32_t mynode = sl >= 0 ? smem_bound<K>(s_lvl, w.sm, myqe, false) : 0u;
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     K qv[I], qe[I];
@@ -310,21 +339,13 @@ forest_kernel(const __grid_constant__ ForestDev f, const FItem *__restrict__ ite
                     uint32_t node[I];
 #pragma unroll
                     for (int s = 0; s < I; s++) {
-                        const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                        qv[s] = qi < end ? q[qi] : (K)0;
+                        const int k = r * (NG * I) + s * NG + grp;
+                        qv[s] = __shfl_sync(0xffffffffu, myq, k);
+                        node[s] = __shfl_sync(0xffffffffu, mynode, k);
                         qe[s] = qv[s] < tmax ? qv[s] : tmax;
                         up[s] = false;
-                        node[s] = 0;
                     }
-                    if (n == 0) {
-#pragma unroll
-                        for (int s = 0; s < I; s++) {
-                            const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                            if (gl == 0 && qi < end) out[qi] = key_max<V>();
-                        }
-                        continue;
-                    }
-                    for (int lvl = 0; lvl < nl; lvl++)
+                    for (int lvl = from; lvl < nl; lvl++)
                         level_step<K, G, I>(tseps + d.lvl_off[lvl], qe, up, node, grp, gl);
                     leaf_point<K, V, G, I>(tleaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
                         const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
@@ -333,11 +354,15 @@ forest_kernel(const __grid_constant__ ForestDev f, const FItem *__restrict__ ite
                 }
             } else {
                 // 64 descents: lower bounds of lo (d < 32), upper bounds of hi
-                const uint64_t my = base + lane;
                 const bool v = my < end;
                 const K a = v ? lo[my] : (K)0;
                 const K b = v ? hi[my] : (K)0;
                 if (n > 0) {
+                    const K qa = a <= tmax ? a : tmax;
+                    const K qb = b < tmax ? b : tmax;
+                    const bool ub_upper = b < tmax;
+                    const uint32_t na = sl >= 0 ? smem_bound<K>(s_lvl, w.sm, qa, false) : 0u;
+                    const uint32_t nb = sl >= 0 ? smem_bound<K>(s_lvl, w.sm, qb, ub_upper) : 0u;
 #pragma unroll
                     for (int r = 0; r < 2 * R; r++) {
                         const bool which = r >= R;
@@ -347,17 +372,11 @@ forest_kernel(const __grid_constant__ ForestDev f, const FItem *__restrict__ ite
 #pragma unroll
                         for (int s = 0; s < I; s++) {
                             const int k = (r % R) * (NG * I) + s * NG + grp;
-                            const K x = __shfl_sync(0xffffffffu, which ? b : a, k);
-                            if (which) {
-                                qe[s] = x < tmax ? x : tmax;
-                                up[s] = x < tmax;
-                            } else {
-                                qe[s] = x <= tmax ? x : tmax;
-                                up[s] = false;
-                            }
-                            node[s] = 0;
+                            qe[s] = __shfl_sync(0xffffffffu, which ? qb : qa, k);
+                            node[s] = __shfl_sync(0xffffffffu, which ? nb : na, k);
+                            up[s] = which ? __shfl_sync(0xffffffffu, (int)ub_upper, k) != 0 : false;
                         }
-                        for (int lvl = 0; lvl < nl; lvl++)
+                        for (int lvl = from; lvl < nl; lvl++)
                             level_step<K, G, I>(tseps + d.lvl_off[lvl], qe, up, node, grp, gl);
                         int pos[I];
                         leaf_bound<K, V, G, I>(tleaves, node, qe, up, grp, gl, pos);
@@ -399,8 +418,7 @@ bt_status forest_capture(bt_forest_plan *p, const PlanArgs &a) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kFThreads, 0) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
-    const uint64_t warps_wanted = std::max<uint64_t>(1, p->n_items);
-    const uint64_t ctas = std::min<uint64_t>((warps_wanted + 7) / 8, (uint64_t)sm_count() * per_sm);
+    const uint64_t ctas = std::min<uint64_t>(std::max<uint64_t>(1, p->n_items), (uint64_t)sm_count() * per_sm);
     ForestDev fd{p->forest->d_desc, (const unsigned char *)p->forest->d_leaves, p->forest->d_seps};
     BT_CUDA(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(p->d_counter, 0, sizeof(unsigned long long), p->cap);
@@ -502,17 +520,38 @@ bt_status bt_forest_plan_create(const bt_forest *f, const void *d_q, const uint6
     for (uint32_t t = 0; t < T; t++) {
         if (h_qoff[t + 1] < h_qoff[t]) return fail(BT_ERR_INVALID_ARGUMENT, "query offsets decrease");
         for (uint64_t b = h_qoff[t]; b < h_qoff[t + 1]; b += tile)
-            items.push_back({t, 0u, b, std::min<uint64_t>(tile, h_qoff[t + 1] - b)});
+            items.push_back({t, 0u, b, std::min<uint64_t>(tile, h_qoff[t + 1] - b), -1, 0u});
     }
     if (h_qoff[T] > 0 && (!d_q || !d_out)) return fail(BT_ERR_INVALID_ARGUMENT, "queries or out is NULL");
     if (h_roff) {
         for (uint32_t t = 0; t < T; t++) {
             if (h_roff[t + 1] < h_roff[t]) return fail(BT_ERR_INVALID_ARGUMENT, "range offsets decrease");
             for (uint64_t b = h_roff[t]; b < h_roff[t + 1]; b += tile)
-                items.push_back({t, 1u, b, std::min<uint64_t>(tile, h_roff[t + 1] - b)});
+                items.push_back({t, 1u, b, std::min<uint64_t>(tile, h_roff[t + 1] - b), -1, 0u});
         }
         if (h_roff[T] > 0 && (!d_lo || !d_hi || !d_counts))
             return fail(BT_ERR_INVALID_ARGUMENT, "lo, hi or counts is NULL");
+    }
+    // The level each item stages: the deepest one that fits kFStageBytes and
+    // is not much larger than the descents it saves (16 entries per descent).
+    {
+        const int kb = f->key_bytes;
+        const uint64_t S = kSectorBytes / kb, F = kLineBytes / kb;
+        for (FItem &it : items) {
+            const FTree &d = f->h_desc[it.tree];
+            if (d.n == 0) continue;
+            const uint64_t descents = it.count * (it.kind == 0 ? 1 : 2);
+            for (int l = d.nlevels - 1; l >= 0; l--) {
+                const uint64_t nb = (d.n + S - 1) / S;
+                const uint64_t ent = l + 1 < d.nlevels ? d.lvl_off[l + 1] - d.lvl_off[l]
+                                                       : (nb + F - 1) / F * F;
+                if (ent * kb <= kFStageBytes && ent <= 16 * descents) {
+                    it.slvl = l;
+                    it.sm = (uint32_t)ent;
+                    break;
+                }
+            }
+        }
     }
     // largest work items first: the queue ends with small ones, which balances the tail
     std::stable_sort(items.begin(), items.end(),
