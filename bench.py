@@ -402,7 +402,7 @@ def forest_section(args, device, bt, flush):
     counts = torch.empty(len(lo), dtype=torch.uint64, device=device)
     tried = {}
     for cfg in ((4, 1), (8, 1), (8, 2)):
-        for tile in (512, 2048):
+        for tile in (512, 2048, 8192):
             with f.plan(dq, qoff, out, dlo, dhi, roff, counts, *cfg, tile=tile) as p:
                 p.run(stream)
                 tried[f"{cfg[0]}x{cfg[1]}/t{tile}"] = _timed_ms(lambda: p.run(stream), stream, flush, 3)
