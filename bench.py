@@ -56,6 +56,7 @@ def parse_args(argv=None):
     p.add_argument("--no-forest", action="store_true", help="skip the 4096-tree forest section")
     p.add_argument("--no-rect", action="store_true", help="skip the rectangle-search section")
     p.add_argument("--rect-boxes-log2", type=int, default=20, help="boxes in the rectangle section")
+    p.add_argument("--forest-trees", type=int, default=4096, help="trees in the forest section")
     p.add_argument("--only", choices=["learned", "forest", "rect"],
                    help="run one extension section alone on cuda:0 and print its JSON object "
                         "(for profiling; not the bench line)")
@@ -393,7 +394,7 @@ def forest_section(args, device, bt, flush):
     timing the candidates."""
     import torch
     wl = importlib.import_module(PKG + ".workloads")
-    keys, vals, koff, q, qoff, lo, hi, roff = wl.forest()
+    keys, vals, koff, q, qoff, lo, hi, roff = wl.forest(num_trees=args.forest_trees)
     stream = torch.cuda.current_stream(device)
     f = bt.Forest(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device), koff)
     dq = torch.from_numpy(q).to(device)
