@@ -451,6 +451,53 @@ def forest_section(args, device, bt, flush):
     }
 
 
+def range_section(args, device, bt, flush, tree, keys):
+    """Range search on the benchmark tree (2^26 u32 keys, value = rank): 2^22
+    ranges [key[r], key[min(r + w - 1, n - 1)]], r uniform, w uniform in
+    [1, 64] ranks.  Counts in the three modes of the reference (basic, 2-D
+    grouped, Z-order grouped; grouping included in the time), and counts plus
+    hit IDs (values ascend with keys here, so no sort)."""
+    import torch
+    wl = importlib.import_module(PKG + ".workloads")
+    nr = 1 << 22
+    lo, hi = wl.range_queries(keys, nr, 64)
+    stream = torch.cuda.current_stream(device)
+    dlo, dhi = torch.from_numpy(lo).to(device), torch.from_numpy(hi).to(device)
+    cnt = torch.empty(nr, dtype=torch.uint64, device=device)
+    res = {}
+    counts_ref = None
+    for mode in ("basic", "2d", "zorder"):
+        tree.range_count(dlo, dhi, mode=mode, out=cnt, stream=stream)
+        ms = _timed_ms(lambda: tree.range_count(dlo, dhi, mode=mode, out=cnt, stream=stream),
+                       stream, flush, max(3, args.steps))
+        c = cnt.cpu().numpy()
+        if counts_ref is None:
+            counts_ref = c
+        res[mode] = {"ranges_per_s": nr / (ms / 1e3), "ms": ms,
+                     "same_counts_as_basic": bool(np.array_equal(c, counts_ref))}
+    # with unique keys and value = rank, the count of [key[r], key[e]] is e - r + 1
+    r_idx = np.searchsorted(keys, lo)
+    e_idx = np.searchsorted(keys, hi)
+    counts_ok = bool(np.array_equal(counts_ref.astype(np.int64), e_idx - r_idx + 1))
+    hits = int(counts_ref.sum())
+    tree.range_search(dlo, dhi, mode="basic", ids_capacity=hits)
+    ms_ids = _timed_ms(lambda: tree.range_search(dlo, dhi, mode="basic", ids_capacity=hits,
+                                                 stream=stream),
+                       stream, flush, max(3, args.steps // 3))
+    peak, _ = measured_peak()
+    alg = nr * (2 * 4 + 8 + 2 * 32)  # both bounds' keys in, count out, two key sectors
+    base_ms = res["basic"]["ms"]
+    return {
+        "workload": "2^26 u32 keys (value = rank), 2^22 ranges of width uniform [1, 64] ranks",
+        "counts": res, "counts_equal_rank_difference": counts_ok,
+        "ids": {"ranges_per_s": nr / (ms_ids / 1e3), "ms": ms_ids, "hits": hits,
+                "api": "Tree.range_search (counts, scan, offsets, ID fill)"},
+        "roofline": {"bound": "hbm", "kernel": "bounds_kernel (basic counts)",
+                     "achieved": alg / (base_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (base_ms / 1e3) / 1e9 / peak},
+    }
+
+
 def rect_section(args, device, bt, flush):
     """Rectangle workload: 2^24 points (x, y uniform u16) keyed by their
     32-bit Morton code (value = point ID, sorted by (code, ID)); 2^20
@@ -645,6 +692,7 @@ def run_ours(args):
     gather_rps = bt.measure_gather(leaf_bytes, 1 << 24, 64)
     tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
 
+    ranges = range_section(args, device, bt, flush, tree, keys) if world == 1 else None
     learned = forest = rect = None
     if world == 1 and not args.no_learned:
         learned = learned_section(args, device, bt, flush)
@@ -699,6 +747,7 @@ def run_ours(args):
             "learned_index": learned,
             "forest": forest,
             "rectangles": rect,
+            "ranges": ranges,
         }
         print(json.dumps(line), flush=True)
     tree.close()
