@@ -233,7 +233,7 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
 // query d - 32), passed in 2R rounds.  counts[i] = ub - lb (0 if lo > hi);
 // lb_out[i] = lb.
 template <typename K, typename V, int G, int R, bool PERM>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 2)
 bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
               const K *__restrict__ hi, const uint32_t *__restrict__ perm, uint64_t nq,
               uint64_t *__restrict__ counts, uint64_t *__restrict__ lb_out) {
