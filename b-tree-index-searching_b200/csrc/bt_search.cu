@@ -115,7 +115,8 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
 }
 
 // Point search over radix-grouped input (the queries ordered by their top
-// kPointGroupBits bits, as bt_group_queries leaves them).  One CTA per SM
+// kPointGroupBits bits below the tree's key length, as bt_group_queries
+// leaves them).  One CTA per SM
 // takes a contiguous run of the grouped batch.  For the group of its current
 // queries it stages in shared memory the group's window of the deepest
 // separator level whose window fits (for 2^26 u32 keys and 256 groups: the
@@ -127,6 +128,15 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
 // tile holds a query of another group (tiles at group boundaries, or input
 // that is not grouped at all) take the full descent from the root instead,
 // so results never depend on the order of the input.
+// The group of a key as the grouping pass forms it: its bits above `shift`
+// (the tree's key length less kPointGroupBits), the last group taking
+// everything above.
+constexpr uint64_t kLastGroup = (1u << kPointGroupBits) - 1u;
+__device__ __forceinline__ uint64_t group_of(uint64_t k, int shift) {
+    const uint64_t g = k >> shift;
+    return g < kLastGroup ? g : kLastGroup;
+}
+
 constexpr int kWinThreads = 1024;
 constexpr int kWinWarps = kWinThreads / 32;
 constexpr size_t kWinBytes = 192 * 1024;
@@ -161,12 +171,12 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     int wlvl = 0;
     uint32_t w0 = 0, wm = 1;
     for (uint64_t t0 = c_begin; t0 < c_end; t0 += kWinWarps) {
-        const uint64_t b = (uint64_t)q[t0 * 32] >> shift;  // group of this step's first query
+        const uint64_t b = group_of((uint64_t)q[t0 * 32], shift);  // group of this step's first query
         if (b != staged) {
             __syncthreads();  // the old window is no longer read
             if (threadIdx.x < 2) {
                 const uint64_t lo = b << shift;
-                const uint64_t hi = lo | ((1ull << shift) - 1ull);
+                const uint64_t hi = b == kLastGroup ? ~0ull : lo | ((1ull << shift) - 1ull);
                 const uint64_t k = threadIdx.x == 0 ? lo : hi;
                 s_blk[threadIdx.x] = block_lower_bound<K>(t, k < (uint64_t)tmax ? (K)k : tmax);
             }
@@ -196,7 +206,7 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
         const uint32_t myperm = my < nq ? perm[my] : 0u;  // loaded early, off the critical path
         const K myqe = myq < tmax ? myq : tmax;
         // phase 1: the window, or (whole warp) the descent from the root
-        const bool inwin = my >= nq || ((uint64_t)myq >> shift) == staged;
+        const bool inwin = my >= nq || group_of((uint64_t)myq, shift) == staged;
         const bool win = __all_sync(0xffffffffu, inwin);
         uint32_t mynode = 0;
         if (win) {
@@ -380,7 +390,7 @@ bt_status window_launch(const bt_tree *t, const void *d_q, const uint32_t *d_per
     if (st != BT_OK) return st;
     const uint64_t ntiles = (nq + 31) / 32;
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, sm_count()));
-    const int shift = 8 * t->key_bytes - kPointGroupBits;
+    const int shift = std::max(0, bitlen64(t->max_key) - kPointGroupBits);  // as the grouping pass
     count_launch();
     fn<<<grid, kWinThreads, kWinBytes, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out, shift);
     BT_CUDA(cudaGetLastError());

@@ -89,3 +89,17 @@ def test_grouped_batch_accepts_ungrouped_input(bt, orc, cuda):
         perm = torch.arange(len(q), dtype=torch.int64, device=cuda).to(torch.uint32)
         got = t.search_grouped_batch(dev(q, cuda), perm).cpu().numpy()
     assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("kt", [np.uint32, np.uint64])
+def test_grouped_window_tiny_key_range(bt, orc, cuda, kt):
+    """Keys 0..199: groups are single key values (the group shift is 0), the
+    last group holds every larger query."""
+    g = np.random.default_rng(200)
+    keys = np.arange(0, 200, dtype=kt)
+    vals = g.permutation(200).astype(kt)
+    q = g.integers(0, 300, size=NQ, dtype=np.uint64).astype(kt)
+    q[:4] = [0, 199, 200, np.iinfo(kt).max]
+    exp = orc.point_search(keys, vals, q)
+    with bt.Tree.build(dev(keys, cuda), dev(vals, cuda)) as t:
+        assert np.array_equal(t.point_search(dev(q, cuda), mode="grouped").cpu().numpy(), exp)
