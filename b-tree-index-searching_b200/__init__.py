@@ -109,6 +109,8 @@ _PROTOS = {
     "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
     "bt_kernel_launches": (ctypes.c_uint64, []),
     "bt_measure_gather": (_I, [_U64, _U64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
+    "bt_sort_pairs": (_I, [_P, _P, _U64, _I, _I, _P, _P, _P]),
+    "bt_build_unsorted": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
     "bt_set_search_config": (_I, [_P, _I, _I]),
     "bt_point_search_grouped_noalloc": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_train": (_I, [_P, ctypes.POINTER(bt_learned_config), _P,
@@ -208,6 +210,22 @@ class Tree:
             st = L.bt_build_host(keys.ctypes.data_as(_P), values.ctypes.data_as(_P), n, kb, vb,
                                  _stream_ptr(stream), ctypes.byref(out))
         _check(st, "bt_build")
+        info = bt_info()
+        _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
+        return cls(out.value, info)
+
+    @classmethod
+    def build_unsorted(cls, keys, values, stream=None):
+        """Build from unsorted CUDA tensors: sorted on the device first
+        (bt_build_unsorted); equal keys keep their input order."""
+        L = lib()
+        out = ctypes.c_void_p()
+        if len(values) != len(keys):
+            raise ValueError("keys and values differ in length")
+        keys, values = keys.contiguous(), values.contiguous()
+        _check(L.bt_build_unsorted(_P(keys.data_ptr()), _P(values.data_ptr()), len(keys),
+                                   keys.element_size(), values.element_size(), _stream_ptr(stream),
+                                   ctypes.byref(out)), "bt_build_unsorted")
         info = bt_info()
         _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
         return cls(out.value, info)
@@ -551,6 +569,18 @@ def version():
 def kernel_launches():
     """Kernel launches issued by the library so far in this process."""
     return lib().bt_kernel_launches()
+
+
+def sort_pairs(keys, values, stream=None):
+    """Stable device sort of (key, value) CUDA tensors by key (bt_sort_pairs);
+    returns new tensors."""
+    import torch
+    keys, values = keys.contiguous(), values.contiguous()
+    ok, ov = torch.empty_like(keys), torch.empty_like(values)
+    _check(lib().bt_sort_pairs(_P(keys.data_ptr()), _P(values.data_ptr()), len(keys),
+                               keys.element_size(), values.element_size(), _P(ok.data_ptr()),
+                               _P(ov.data_ptr()), _stream_ptr(stream)), "bt_sort_pairs")
+    return ok, ov
 
 
 def measure_gather(region_bytes, n_reads=1 << 24, block_bytes=64):

@@ -222,6 +222,48 @@ bt_status bt_build(const void *d_sorted_keys, const void *d_values, uint64_t n, 
     return BT_OK;
 }
 
+bt_status bt_sort_pairs(const void *d_keys, const void *d_values, uint64_t n, int key_bytes,
+                        int value_bytes, void *d_keys_out, void *d_values_out, void *stream) {
+    using namespace bt;
+    if ((key_bytes != 4 && key_bytes != 8) || (value_bytes != 4 && value_bytes != 8))
+        return fail(BT_ERR_INVALID_ARGUMENT, "key_bytes and value_bytes must be 4 or 8");
+    if (n == 0) return BT_OK;
+    if (!d_keys || !d_values || !d_keys_out || !d_values_out)
+        return fail(BT_ERR_INVALID_ARGUMENT, "a key or value pointer is NULL");
+    if (d_keys_out == d_keys || d_values_out == d_values)
+        return fail(BT_ERR_INVALID_ARGUMENT, "outputs must not alias the inputs");
+    int dev = 0;
+    BT_CUDA(cudaGetDevice(&dev));
+    bt_status st = require_device(dev);
+    if (st != BT_OK) return st;
+    return launch_sort_pairs(key_bytes, value_bytes, d_keys, d_values, n, d_keys_out, d_values_out,
+                             (cudaStream_t)stream);
+}
+
+bt_status bt_build_unsorted(const void *d_keys, const void *d_values, uint64_t n, int key_bytes,
+                            int value_bytes, void *stream, bt_tree **out) {
+    using namespace bt;
+    if (!out) return fail(BT_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    if ((key_bytes != 4 && key_bytes != 8) || (value_bytes != 4 && value_bytes != 8))
+        return fail(BT_ERR_INVALID_ARGUMENT, "key_bytes and value_bytes must be 4 or 8");
+    if (n == 0) return bt_build(nullptr, nullptr, 0, key_bytes, value_bytes, stream, out);
+    if (!d_keys || !d_values) return fail(BT_ERR_INVALID_ARGUMENT, "keys or values pointer is NULL");
+    int dev = 0;
+    BT_CUDA(cudaGetDevice(&dev));
+    bt_status st = require_device(dev);
+    if (st != BT_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    void *sk = nullptr, *sv = nullptr;
+    st = ws_alloc(&sk, n * key_bytes, s);
+    if (st == BT_OK) st = ws_alloc(&sv, n * value_bytes, s);
+    if (st == BT_OK) st = launch_sort_pairs(key_bytes, value_bytes, d_keys, d_values, n, sk, sv, s);
+    if (st == BT_OK) st = bt_build(sk, sv, n, key_bytes, value_bytes, stream, out);
+    ws_free(sk, s);
+    ws_free(sv, s);
+    return st;
+}
+
 bt_status bt_build_host(const void *h_sorted_keys, const void *h_values, uint64_t n,
                         int key_bytes, int value_bytes, void *stream, bt_tree **out) {
     using namespace bt;

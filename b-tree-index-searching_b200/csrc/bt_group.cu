@@ -53,6 +53,7 @@ __device__ __forceinline__ uint32_t spread16(uint32_t x) {
 
 template <typename K>
 __device__ __forceinline__ uint32_t group_key(K a, K b, const GroupKeyParams &p) {
+    if (p.kind == kPartRadix) return (uint32_t)((uint64_t)a >> p.shift);  // caller takes the low byte
     const uint64_t lim = (1ull << p.cbits) - 1;
     uint64_t x = (uint64_t)a >> p.shift;
     x = x < lim ? x : lim;
@@ -422,6 +423,75 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
     return st;
 }
 
+template <typename V>
+__global__ void gather_kernel(const V *__restrict__ in, const uint32_t *__restrict__ idx, uint64_t n,
+                              V *__restrict__ out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = in[idx[i]];
+}
+
+// LSD radix sort of keys carrying the input index: pass p partitions by
+// byte p of the key (stable), so after the last pass the keys are sorted and
+// equal keys keep their input order; then values are gathered by index.
+template <typename K, typename V>
+bt_status sort_pairs_impl(const K *d_keys, const V *d_vals, uint64_t n, K *out_keys, V *out_vals,
+                          cudaStream_t s) {
+    const int passes = (int)sizeof(K);
+    const uint64_t ntiles = (n + kPTile - 1) / kPTile;
+    const uint64_t ncounts = ntiles * 256;
+    const uint64_t scan_we = scan_ws_elems(ncounts);
+    const size_t ws_bytes = (ncounts + scan_we) * sizeof(uint32_t) + 256 +
+                            2 * n * (sizeof(K) + sizeof(uint32_t)) + 512;
+    unsigned char *ws = nullptr;
+    bt_status st = ws_alloc((void **)&ws, ws_bytes, s);
+    if (st != BT_OK) return st;
+    uint32_t *counts = reinterpret_cast<uint32_t *>(ws);
+    uint32_t *scan_ws = counts + ncounts;
+    unsigned char *pp = ws + ((ncounts + scan_we) * sizeof(uint32_t) + 255) / 256 * 256;
+    K *tk[2];
+    uint32_t *tp[2];
+    for (int i = 0; i < 2; i++) {
+        tk[i] = reinterpret_cast<K *>(pp);
+        pp += (n * sizeof(K) + 255) / 256 * 256;
+        tp[i] = reinterpret_cast<uint32_t *>(pp);
+        pp += (n * sizeof(uint32_t) + 255) / 256 * 256;
+    }
+    const size_t smem = (size_t)kPTile * (sizeof(K) + sizeof(uint32_t) + 1);
+    auto scat = part_scatter_kernel<K, false>;
+    cudaError_t e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) st = cuda_fail(e, "cudaFuncSetAttribute");
+    GroupKeyParams gp;
+    gp.kind = kPartRadix;
+    gp.cbits = 8;
+    const K *ik = d_keys;
+    const uint32_t *ip = nullptr;  // the first pass numbers the input itself
+    for (int p = 0; p < passes && st == BT_OK; p++) {
+        gp.shift = 8 * p;
+        K *ok = p == passes - 1 ? out_keys : tk[p & 1];
+        uint32_t *op = tp[p & 1];
+        count_launch();
+        part_hist_kernel<K, false><<<(unsigned)ntiles, kPT, 0, s>>>(ik, nullptr, n, gp, 0, counts, ntiles);
+        st = scan_run<uint32_t>(counts, counts, ncounts, nullptr, scan_ws, s);
+        if (st != BT_OK) break;
+        count_launch();
+        scat<<<(unsigned)ntiles, kPT, smem, s>>>(ik, nullptr, ip, n, gp, 0, counts, ntiles, ok, nullptr, op);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "radix sort pass");
+        ik = ok;
+        ip = op;
+    }
+    if (st == BT_OK) {
+        count_launch();
+        gather_kernel<V><<<(unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16), 256, 0, s>>>(
+            d_vals, ip, n, out_vals);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) st = cuda_fail(e, "value gather");
+    }
+    ws_free(ws, s);
+    return st;
+}
+
 // Single-pass point partition into caller-provided memory (no allocation):
 // counts and scan scratch come from `ws` (partition_ws_bytes bytes).
 template <typename K>
@@ -611,6 +681,23 @@ bt_status launch_partition(const bt_tree *t, int kind, const void *d_a, const vo
                                                (uint64_t *)d_out_b, d_perm, s)
               : partition_impl<uint64_t, false>(t, kind, (const uint64_t *)d_a, nullptr, nq,
                                                 (uint64_t *)d_out_a, nullptr, d_perm, s);
+}
+
+bt_status launch_sort_pairs(int key_bytes, int value_bytes, const void *d_keys, const void *d_vals,
+                            uint64_t n, void *out_keys, void *out_vals, cudaStream_t s) {
+    if (n == 0) return BT_OK;
+    if (n >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "sort needs fewer than 2^32 pairs");
+    if (key_bytes == 4)
+        return value_bytes == 4
+                   ? sort_pairs_impl<uint32_t, uint32_t>((const uint32_t *)d_keys, (const uint32_t *)d_vals, n,
+                                                         (uint32_t *)out_keys, (uint32_t *)out_vals, s)
+                   : sort_pairs_impl<uint32_t, uint64_t>((const uint32_t *)d_keys, (const uint64_t *)d_vals, n,
+                                                         (uint32_t *)out_keys, (uint64_t *)out_vals, s);
+    return value_bytes == 4
+               ? sort_pairs_impl<uint64_t, uint32_t>((const uint64_t *)d_keys, (const uint32_t *)d_vals, n,
+                                                     (uint64_t *)out_keys, (uint32_t *)out_vals, s)
+               : sort_pairs_impl<uint64_t, uint64_t>((const uint64_t *)d_keys, (const uint64_t *)d_vals, n,
+                                                     (uint64_t *)out_keys, (uint64_t *)out_vals, s);
 }
 
 size_t partition_point_ws_bytes(uint64_t nq) {

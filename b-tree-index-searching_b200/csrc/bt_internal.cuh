@@ -174,6 +174,12 @@ bt_status launch_partition_point_prealloc(const bt_tree *t, const void *d_q, uin
                                           cudaStream_t s);
 bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64_t *d_counts,
                             const uint64_t *d_offsets, uint64_t nq, void *d_ids, cudaStream_t s);
+// Stable sort of n (key, value) pairs by key on the device: LSD radix sort
+// with 8-bit digits (key_bytes passes of the partition kernels, carrying the
+// input index), then one gather of the values.  Equal keys keep their input
+// order.  n < 2^32; outputs must not alias inputs.
+bt_status launch_sort_pairs(int key_bytes, int value_bytes, const void *d_keys, const void *d_vals,
+                            uint64_t n, void *out_keys, void *out_vals, cudaStream_t s);
 // Sorts each segment ids[offsets[i] .. + counts[i]) ascending (value width
 // of t).  small_sorted: segments of up to 256 values are sorted already.
 bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
@@ -189,7 +195,7 @@ int search_cfg_rounds(int cfg);
 void free_learned(bt::LearnedState *s);
 
 // Partition kinds for launch_partition.
-enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2 };
+enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2, kPartRadix = 3 };
 // Digit bits used by the grouping passes.
 constexpr int kPointGroupBits = 8;
 constexpr int kRangeGroupBits = 8;

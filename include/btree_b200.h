@@ -105,6 +105,21 @@ BT_API bt_status bt_build(const void *d_sorted_keys, const void *d_values, uint6
 BT_API bt_status bt_build_host(const void *h_sorted_keys, const void *h_values, uint64_t n,
                         int key_bytes, int value_bytes, void *stream, bt_tree **out);
 
+/*
+ * Stable sort of n (key, value) pairs by key on the device into separate
+ * output arrays (which must not alias the inputs): an LSD radix sort with
+ * 8-bit digits; equal keys keep their input order.  Replaces the
+ * cub::DeviceRadixSort::SortPairs call the reference's main.cu runs before
+ * its build (main.cu:109-118).  n < 2^32.  Asynchronous on `stream`.
+ */
+BT_API bt_status bt_sort_pairs(const void *d_keys, const void *d_values, uint64_t n, int key_bytes,
+                               int value_bytes, void *d_keys_out, void *d_values_out, void *stream);
+
+/* bt_build from unsorted device pairs: bt_sort_pairs into engine scratch,
+ * then bt_build (the reference's main.cu:109-129 sequence). */
+BT_API bt_status bt_build_unsorted(const void *d_keys, const void *d_values, uint64_t n,
+                                   int key_bytes, int value_bytes, void *stream, bt_tree **out);
+
 /* Free every device resource of a tree.  NULL is accepted. */
 BT_API bt_status bt_destroy(bt_tree *tree);
 
