@@ -111,6 +111,8 @@ _PROTOS = {
     "bt_measure_gather": (_I, [_U64, _U64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "bt_sort_pairs": (_I, [_P, _P, _U64, _I, _I, _P, _P, _P]),
     "bt_build_unsorted": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
+    "bt_save": (_I, [_P, ctypes.c_char_p]),
+    "bt_load": (_I, [ctypes.c_char_p, _P, ctypes.POINTER(_P)]),
     "bt_set_search_config": (_I, [_P, _I, _I]),
     "bt_point_search_grouped_noalloc": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_train": (_I, [_P, ctypes.POINTER(bt_learned_config), _P,
@@ -210,6 +212,21 @@ class Tree:
             st = L.bt_build_host(keys.ctypes.data_as(_P), values.ctypes.data_as(_P), n, kb, vb,
                                  _stream_ptr(stream), ctypes.byref(out))
         _check(st, "bt_build")
+        info = bt_info()
+        _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
+        return cls(out.value, info)
+
+    def save(self, path):
+        """Write the built tree to one file (bt_save)."""
+        _check(lib().bt_save(self._h, os.fsencode(path)), "bt_save")
+
+    @classmethod
+    def load(cls, path):
+        """A tree read back from a file written by save (bt_load), on the
+        current device."""
+        L = lib()
+        out = ctypes.c_void_p()
+        _check(L.bt_load(os.fsencode(path), None, ctypes.byref(out)), "bt_load")
         info = bt_info()
         _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
         return cls(out.value, info)

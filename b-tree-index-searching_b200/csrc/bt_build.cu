@@ -7,7 +7,9 @@
 // below; nothing is pointer-linked, so the whole build is a few streaming
 // passes with no host round trip between levels.
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "bt_internal.cuh"
 
@@ -288,6 +290,147 @@ bt_status bt_build_host(const void *h_sorted_keys, const void *h_values, uint64_
     ws_free(dk, s);
     ws_free(dv, s);
     return st;
+}
+
+// ---- tree image: the built arrays and their descriptor in one file --------
+
+namespace {
+
+constexpr char kImageMagic[8] = {'B', 'T', 'B', '2', '0', '0', 'I', 'M'};
+constexpr uint32_t kImageVersion = 1;
+
+struct ImageHeader {
+    char magic[8];
+    uint32_t version;
+    int32_t key_bytes, val_bytes, values_sorted;
+    uint64_t n, n_sectors, seps_elems, min_key, max_key;
+    uint64_t lvl_nodes[bt::kMaxLevels], lvl_entries[bt::kMaxLevels], lvl_off[bt::kMaxLevels];
+    int32_t nlevels, smem_level;
+    uint32_t smem_entries, smem_bytes;
+    uint64_t leaf_bytes, sep_bytes;
+};
+
+// Copies `bytes` between a device buffer and a file through a host bounce
+// buffer of at most 64 MiB.
+bt_status stream_file(FILE *f, void *dptr, uint64_t bytes, bool write) {
+    using namespace bt;
+    const uint64_t chunk = std::min<uint64_t>(bytes, 64ull << 20);
+    std::vector<unsigned char> buf(chunk ? chunk : 1);
+    for (uint64_t o = 0; o < bytes; o += chunk) {
+        const uint64_t m = std::min(chunk, bytes - o);
+        if (write) {
+            BT_CUDA(cudaMemcpy(buf.data(), (const unsigned char *)dptr + o, m, cudaMemcpyDeviceToHost));
+            if (fwrite(buf.data(), 1, m, f) != m) return fail(BT_ERR_INVALID_ARGUMENT, "tree image: write failed");
+        } else {
+            if (fread(buf.data(), 1, m, f) != m) return fail(BT_ERR_INVALID_ARGUMENT, "tree image: file is truncated");
+            BT_CUDA(cudaMemcpy((unsigned char *)dptr + o, buf.data(), m, cudaMemcpyHostToDevice));
+        }
+    }
+    return BT_OK;
+}
+
+}  // namespace
+
+bt_status bt_save(const bt_tree *t, const char *path) {
+    using namespace bt;
+    if (!t || !path) return fail(BT_ERR_INVALID_ARGUMENT, "tree or path is NULL");
+    ImageHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, kImageMagic, 8);
+    h.version = kImageVersion;
+    h.key_bytes = t->key_bytes;
+    h.val_bytes = t->val_bytes;
+    h.values_sorted = t->values_sorted;
+    h.n = t->n;
+    h.n_sectors = t->n_sectors;
+    h.seps_elems = t->seps_elems;
+    h.min_key = t->min_key;
+    h.max_key = t->max_key;
+    for (int l = 0; l < kMaxLevels; l++) {
+        h.lvl_nodes[l] = t->lvl_nodes[l];
+        h.lvl_entries[l] = t->lvl_entries[l];
+        h.lvl_off[l] = t->dev.lvl_off[l];
+    }
+    h.nlevels = t->dev.nlevels;
+    h.smem_level = t->dev.smem_level;
+    h.smem_entries = t->dev.smem_entries;
+    h.smem_bytes = t->dev.smem_bytes;
+    h.leaf_bytes = t->n ? t->n_sectors * (uint64_t)leaf_stride(t->key_bytes, t->val_bytes) : 0;
+    h.sep_bytes = t->n ? t->seps_elems * (uint64_t)t->key_bytes : 0;
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(BT_ERR_INVALID_ARGUMENT, std::string("tree image: cannot open ") + path);
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(t->device);
+    bt_status st = fwrite(&h, sizeof(h), 1, f) == 1 ? BT_OK
+                                                    : fail(BT_ERR_INVALID_ARGUMENT, "tree image: write failed");
+    if (st == BT_OK && h.leaf_bytes) st = stream_file(f, t->d_leaves, h.leaf_bytes, true);
+    if (st == BT_OK && h.sep_bytes) st = stream_file(f, t->d_seps, h.sep_bytes, true);
+    cudaSetDevice(prev);
+    if (fclose(f) != 0 && st == BT_OK) st = fail(BT_ERR_INVALID_ARGUMENT, "tree image: close failed");
+    return st;
+}
+
+bt_status bt_load(const char *path, void *stream, bt_tree **out) {
+    using namespace bt;
+    (void)stream;
+    if (!path || !out) return fail(BT_ERR_INVALID_ARGUMENT, "path or out is NULL");
+    *out = nullptr;
+    int dev = 0;
+    BT_CUDA(cudaGetDevice(&dev));
+    bt_status st = require_device(dev);
+    if (st != BT_OK) return st;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(BT_ERR_INVALID_ARGUMENT, std::string("tree image: cannot open ") + path);
+    ImageHeader h;
+    if (fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, kImageMagic, 8) != 0 ||
+        h.version != kImageVersion || (h.key_bytes != 4 && h.key_bytes != 8) ||
+        (h.val_bytes != 4 && h.val_bytes != 8) || h.nlevels < 0 || h.nlevels > kMaxLevels ||
+        h.leaf_bytes != (h.n ? h.n_sectors * (uint64_t)leaf_stride(h.key_bytes, h.val_bytes) : 0) ||
+        h.sep_bytes != (h.n ? h.seps_elems * (uint64_t)h.key_bytes : 0)) {
+        fclose(f);
+        return fail(BT_ERR_INVALID_ARGUMENT, "tree image: not a tree image of this version");
+    }
+    bt_tree *t = new bt_tree();
+    std::memset(t, 0, sizeof(*t));
+    t->device = dev;
+    t->key_bytes = h.key_bytes;
+    t->val_bytes = h.val_bytes;
+    t->values_sorted = h.values_sorted;
+    t->n = h.n;
+    t->n_sectors = h.n_sectors;
+    t->seps_elems = h.seps_elems;
+    t->min_key = h.min_key;
+    t->max_key = h.max_key;
+    t->search_cfg = default_search_cfg(h.key_bytes);
+    for (int l = 0; l < kMaxLevels; l++) {
+        t->lvl_nodes[l] = h.lvl_nodes[l];
+        t->lvl_entries[l] = h.lvl_entries[l];
+        t->dev.lvl_off[l] = h.lvl_off[l];
+    }
+    cudaError_t e = cudaSuccess;
+    if (h.leaf_bytes) e = cudaMalloc(&t->d_leaves, h.leaf_bytes);
+    if (e == cudaSuccess && h.sep_bytes) e = cudaMalloc(&t->d_seps, h.sep_bytes);
+    st = e == cudaSuccess ? BT_OK : cuda_fail(e, "tree image: device allocation");
+    if (st == BT_OK && h.leaf_bytes) st = stream_file(f, t->d_leaves, h.leaf_bytes, false);
+    if (st == BT_OK && h.sep_bytes) st = stream_file(f, t->d_seps, h.sep_bytes, false);
+    fclose(f);
+    if (st != BT_OK) {
+        free_tree(t);
+        return st;
+    }
+    DevTree &dt = t->dev;
+    dt.leaves = t->d_leaves;
+    dt.seps = t->d_seps;
+    dt.n = t->n;
+    dt.max_key = t->max_key;
+    dt.n_sectors = t->n_sectors;
+    dt.nlevels = h.nlevels;
+    dt.smem_level = h.smem_level;
+    dt.smem_entries = h.smem_entries;
+    dt.smem_bytes = h.smem_bytes;
+    *out = t;
+    return BT_OK;
 }
 
 bt_status bt_destroy(bt_tree *tree) {

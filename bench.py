@@ -451,6 +451,35 @@ def forest_section(args, device, bt, flush):
     }
 
 
+def build_section(device, bt, keys, vals):
+    """Bulk build of the benchmark tree from device-resident pairs: from
+    sorted keys (bt_build), and from the same pairs shuffled (bt_build_unsorted:
+    device radix sort, then the build).  Wall time around the synchronous
+    calls, best of three."""
+    import torch
+    dk = torch.from_numpy(keys).to(device)
+    dv = torch.from_numpy(vals).to(device)
+    p = torch.randperm(len(keys), device=device)
+    uk, uv = dk[p].contiguous(), dv[p].contiguous()
+
+    def best(fn):
+        ts = []
+        for _ in range(3):
+            torch.cuda.synchronize(device)
+            t0 = time.perf_counter()
+            t = fn()
+            torch.cuda.synchronize(device)
+            ts.append(time.perf_counter() - t0)
+            t.close()
+        return 1e3 * min(ts)
+
+    sorted_ms = best(lambda: bt.Tree.build(dk, dv))
+    unsorted_ms = best(lambda: bt.Tree.build_unsorted(uk, uv))
+    return {"keys": len(keys), "sorted_ms": sorted_ms, "unsorted_ms": unsorted_ms,
+            "keys_per_s_sorted": len(keys) / (sorted_ms / 1e3),
+            "keys_per_s_unsorted": len(keys) / (unsorted_ms / 1e3)}
+
+
 def range_section(args, device, bt, flush, tree, keys):
     """Range search on the benchmark tree (2^26 u32 keys, value = rank): 2^22
     ranges [key[r], key[min(r + w - 1, n - 1)]], r uniform, w uniform in
@@ -693,6 +722,7 @@ def run_ours(args):
     tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
 
     ranges = range_section(args, device, bt, flush, tree, keys) if world == 1 else None
+    build = build_section(device, bt, keys, vals) if world == 1 else None
     learned = forest = rect = None
     if world == 1 and not args.no_learned:
         learned = learned_section(args, device, bt, flush)
@@ -748,6 +778,7 @@ def run_ours(args):
             "forest": forest,
             "rectangles": rect,
             "ranges": ranges,
+            "build": build,
         }
         print(json.dumps(line), flush=True)
     tree.close()

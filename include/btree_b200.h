@@ -120,6 +120,18 @@ BT_API bt_status bt_sort_pairs(const void *d_keys, const void *d_values, uint64_
 BT_API bt_status bt_build_unsorted(const void *d_keys, const void *d_values, uint64_t n,
                                    int key_bytes, int value_bytes, void *stream, bt_tree **out);
 
+/*
+ * Tree image (no counterpart in the reference, which rebuilds from its input
+ * files every run): bt_save writes the built leaf blocks, separator levels
+ * and their descriptor to one file; bt_load reads it back onto the current
+ * device as a tree that searches exactly like the saved one (its search
+ * configuration is the default; a trained learned model is not saved).
+ * The image is raw device layout: read it on a machine of the same
+ * endianness.  Both are synchronous.
+ */
+BT_API bt_status bt_save(const bt_tree *tree, const char *path);
+BT_API bt_status bt_load(const char *path, void *stream, bt_tree **out);
+
 /* Free every device resource of a tree.  NULL is accepted. */
 BT_API bt_status bt_destroy(bt_tree *tree);
 
