@@ -459,8 +459,9 @@ def build_section(device, bt, keys, vals):
     import torch
     dk = torch.from_numpy(keys).to(device)
     dv = torch.from_numpy(vals).to(device)
-    p = torch.randperm(len(keys), device=device)
-    uk, uv = dk[p].contiguous(), dv[p].contiguous()
+    perm = np.random.default_rng(5).permutation(len(keys))
+    uk = torch.from_numpy(keys[perm]).to(device)
+    uv = torch.from_numpy(vals[perm]).to(device)
 
     def best(fn):
         ts = []
