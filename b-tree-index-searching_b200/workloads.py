@@ -204,6 +204,45 @@ def forest(num_trees=4096, size_log2=(10, 20), batch_log2=(6, 16), hit=0.8, rang
     return keys, vals, koff.astype(u64), q, qoff.astype(u64), lo, hi, roff.astype(u64)
 
 
+def reference_queries(kind, n, max_number, seed=KEY_SEED + 3):
+    """Query families of the reference's generator (randomgenator/randgen.cu),
+    seeded here where the original is seeded from the clock:
+
+      uniform        -- integers uniform in [0, max_number] (randgen.cu:75-91);
+      normal         -- normal around max_number / 2 with sigma 0.35 x that
+                        mean, draws outside [0, max_number] replaced by the
+                        mean (:104-128);
+      normal_wide    -- the same with sigma 0.63 x the mean (:186-205);
+      zipf           -- Zipf(1.0) ranks over 1..max_number used as keys
+                        (:138-147; sampled here by rejection-inversion);
+      multi_gaussian -- five equal parts, each a normal of sigma 0.1 around
+                        its own uniform centre in [0, max_number], i.e. five
+                        clusters of (nearly) one value each (:159-175).
+    Returns u64."""
+    g = rng(seed)
+    mx = float(max_number)
+    if kind == "uniform":
+        return g.integers(0, int(max_number), size=n, dtype=np.uint64, endpoint=True)
+    if kind in ("normal", "normal_wide"):
+        mean = float(int(max_number) // 2)
+        x = g.normal(mean, (0.35 if kind == "normal" else 0.63) * mean, size=n)
+        x = np.where((x < 0) | (x > mx), mean, x)
+        return np.floor(x).astype(np.uint64)
+    if kind == "zipf":
+        return zipf_ranks(n, int(max_number), 1.0, g).astype(np.uint64)
+    if kind == "multi_gaussian":
+        out = np.empty(n, dtype=np.uint64)
+        part = n // 5
+        for i in range(5):
+            c = float(g.integers(0, int(max_number), endpoint=True))
+            m = part if i < 4 else n - 4 * part
+            x = g.normal(c, 0.1, size=m)
+            x = np.where((x < 0) | (x > mx), c, x)
+            out[i * part:i * part + m] = np.floor(x).astype(np.uint64)
+        return out
+    raise ValueError(f"unknown query family {kind!r}")
+
+
 def range_queries(keys, n_queries, max_width_ranks, seed=KEY_SEED + 2):
     """Ranges [key[r], key[min(r + w - 1, n - 1)]] with w uniform in
     [1, max_width_ranks] (width in ranks), plus their exact counts."""

@@ -155,3 +155,18 @@ def test_wrong_query_width_rejected(bt, cuda):
     with bt.Tree.build(dev(keys, cuda), dev(keys, cuda)) as t:
         with pytest.raises(ValueError):
             t.point_search(dev(np.arange(3, dtype=np.uint32), cuda))
+
+
+@pytest.mark.parametrize("family", ["uniform", "normal", "normal_wide", "zipf", "multi_gaussian"])
+def test_reference_query_families(bt, orc, wl, cuda, family):
+    """The reference generator's query families (seeded) on u64 keys drawn
+    from the same value range: both point modes against the oracle."""
+    mx = 1 << 40
+    g = np.random.default_rng(17)
+    keys = np.unique(g.integers(0, mx, size=1 << 20, dtype=np.uint64, endpoint=True))
+    vals = np.arange(len(keys), dtype=np.uint64)
+    q = wl.reference_queries(family, (1 << 21) + 3, mx)
+    exp = orc.point_search(keys, vals, q)
+    with bt.Tree.build(dev(keys, cuda), dev(vals, cuda)) as t:
+        for mode in ("basic", "grouped"):
+            assert np.array_equal(t.point_search(dev(q, cuda), mode=mode).cpu().numpy(), exp), mode

@@ -168,3 +168,23 @@ def test_refc_buckets(orc):
     assert orc.bucket2d(a, b, 1) == 0xF * 0x3
     assert orc.zorder_interval(0xFFFFFFFF) == 1
     assert orc.zorder_interval(1 << 33) == 2
+
+
+def test_reference_query_families(wl):
+    """The seeded restatements of the reference generator's query families."""
+    import numpy as np
+    mx = 10**9
+    n = 200000
+    u = wl.reference_queries("uniform", n, mx)
+    assert u.max() <= mx and abs(u.mean() / mx - 0.5) < 0.01
+    for kind, sig in (("normal", 0.35), ("normal_wide", 0.63)):
+        x = wl.reference_queries(kind, n, mx).astype(np.float64)
+        assert x.min() >= 0 and x.max() <= mx
+        inside = x[x != mx // 2]
+        assert abs(np.median(x) / (mx / 2) - 1) < 0.02
+        assert abs(inside.std() / (sig * mx / 2) - 1) < (0.05 if kind == "normal" else 0.5)
+    z = wl.reference_queries("zipf", n, mx)
+    assert z.min() >= 1 and (z == 1).mean() > 0.03  # rank 1 is the most frequent
+    mg = wl.reference_queries("multi_gaussian", n, mx)
+    assert len(np.unique(mg)) <= 10  # five clusters of nearly one value each
+    assert np.array_equal(wl.reference_queries("zipf", 1000, mx), wl.reference_queries("zipf", 1000, mx))
