@@ -111,9 +111,10 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     BT_CUDA(cudaMalloc(&t->d_leaves, leaf_bytes));
     BT_CUDA(cudaMemsetAsync(t->d_leaves, 0, leaf_bytes, s));  // block padding bytes
     BT_CUDA(cudaMalloc(&t->d_seps, t->seps_elems * sizeof(K)));
-    unsigned int *d_flags = nullptr;
-    bt_status st = ws_alloc((void **)&d_flags, sizeof(unsigned int), s);
+    WsGuard g_flags(s);
+    bt_status st = g_flags.alloc(sizeof(unsigned int));
     if (st != BT_OK) return st;
+    unsigned int *d_flags = g_flags.as<unsigned int>();
     BT_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(unsigned int), s));
 
     K *seps = (K *)t->d_seps;
@@ -144,7 +145,6 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
     BT_CUDA(cudaMemcpyAsync(&kmax,
                             lv + ((n - 1) / S) * LeafGeom<K, V>::BS + ((n - 1) % S) * sizeof(K),
                             sizeof(K), cudaMemcpyDeviceToHost, s));
-    ws_free(d_flags, s);
     BT_CUDA(cudaStreamSynchronize(s));
     if (flags & 1u) return fail(BT_ERR_UNSORTED, "build keys are not sorted ascending");
     t->values_sorted = (flags & 2u) ? 0 : 1;

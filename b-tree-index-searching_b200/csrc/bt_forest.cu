@@ -197,9 +197,10 @@ bt_status forest_build_impl(bt_forest *f, const void *d_keys, const void *d_vals
     if (seps) BT_CUDA(cudaMalloc(&f->d_seps, seps * sizeof(K)));
     BT_CUDA(cudaMalloc((void **)&f->d_desc, T * sizeof(FTree)));
     BT_CUDA(cudaMemcpyAsync(f->d_desc, f->h_desc.data(), T * sizeof(FTree), cudaMemcpyHostToDevice, s));
-    unsigned int *d_flags = nullptr;
-    bt_status st = ws_alloc((void **)&d_flags, sizeof(unsigned int), s);
+    WsGuard g_flags(s);
+    bt_status st = g_flags.alloc(sizeof(unsigned int));
     if (st != BT_OK) return st;
+    unsigned int *d_flags = g_flags.as<unsigned int>();
     BT_CUDA(cudaMemsetAsync(d_flags, 0, sizeof(unsigned int), s));
     const unsigned grid = (unsigned)std::min<uint64_t>(std::max<uint64_t>(1, (blocks * LG::S + 255) / 256),
                                                        (uint64_t)sm_count() * 16);
@@ -254,7 +255,6 @@ bt_status forest_build_impl(bt_forest *f, const void *d_keys, const void *d_vals
     }
     unsigned int flags = 0;
     BT_CUDA(cudaMemcpyAsync(&flags, d_flags, sizeof(flags), cudaMemcpyDeviceToHost, s));
-    ws_free(d_flags, s);
     BT_CUDA(cudaMemcpyAsync(f->h_desc.data(), f->d_desc, T * sizeof(FTree), cudaMemcpyDeviceToHost, s));
     BT_CUDA(cudaStreamSynchronize(s));
     BT_CUDA(cudaGetLastError());

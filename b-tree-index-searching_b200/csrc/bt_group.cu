@@ -747,15 +747,12 @@ bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64
 bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,
                               uint64_t nq, void *d_ids, cudaStream_t s, bool small_sorted) {
     if (nq == 0) return BT_OK;
-    unsigned int *stat = nullptr;
-    uint64_t *med = nullptr;
-    bt_status st = ws_alloc((void **)&stat, 2 * sizeof(unsigned int), s);
+    WsGuard g_stat(s), g_med(s);
+    bt_status st = g_stat.alloc(2 * sizeof(unsigned int));
+    if (st == BT_OK) st = g_med.alloc(kMedListCap * sizeof(uint64_t));
     if (st != BT_OK) return st;
-    st = ws_alloc((void **)&med, kMedListCap * sizeof(uint64_t), s);
-    if (st != BT_OK) {
-        ws_free(stat, s);
-        return st;
-    }
+    unsigned int *stat = g_stat.as<unsigned int>();
+    uint64_t *med = g_med.as<uint64_t>();
     BT_CUDA(cudaMemsetAsync(stat, 0, 2 * sizeof(unsigned int), s));
     const unsigned gw = (unsigned)std::min<uint64_t>((nq + kWSortThreads / 32 - 1) / (kWSortThreads / 32),
                                                      (uint64_t)sm_count() * 8);
@@ -785,20 +782,14 @@ bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const 
                                                              n, (uint64_t *)d_ids);
         BT_CUDA(cudaGetLastError());
     }
-    ws_free(med, s);
-    unsigned int *flag = stat;
-    if (!h[1]) {
-        ws_free(flag, s);
-        return BT_OK;
-    }
+    if (!h[1]) return BT_OK;
     // some segments exceed the shared-memory sort: list and sort them one CTA each
     const unsigned int max_list = 1u << 16;
-    uint64_t *d_list = nullptr;
-    st = ws_alloc((void **)&d_list, 2 * (size_t)max_list * sizeof(uint64_t), s);
-    if (st != BT_OK) {
-        ws_free(flag, s);
-        return st;
-    }
+    WsGuard g_list(s);
+    st = g_list.alloc(2 * (size_t)max_list * sizeof(uint64_t));
+    if (st != BT_OK) return st;
+    unsigned int *flag = stat;
+    uint64_t *d_list = g_list.as<uint64_t>();
     BT_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned int), s));
     count_launch();
     list_long_segments<<<(unsigned)std::min<uint64_t>((nq + 255) / 256, 4096), 256, 0, s>>>(
@@ -806,30 +797,25 @@ bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const 
     unsigned int n_long = 0;
     BT_CUDA(cudaMemcpyAsync(&n_long, flag, sizeof(n_long), cudaMemcpyDeviceToHost, s));
     BT_CUDA(cudaStreamSynchronize(s));
-    ws_free(flag, s);
-    if (n_long > max_list) {
-        ws_free(d_list, s);
+    if (n_long > max_list)
         return fail(BT_ERR_NOT_SUPPORTED, "more than 65536 result sets exceed 4096 unsorted values");
-    }
     std::vector<uint64_t> list(2 * (size_t)n_long);
     BT_CUDA(cudaMemcpyAsync(list.data(), d_list, list.size() * sizeof(uint64_t),
                             cudaMemcpyDeviceToHost, s));
     BT_CUDA(cudaStreamSynchronize(s));
-    ws_free(d_list, s);
     const size_t vb = (size_t)t->val_bytes;
     for (unsigned int k = 0; k < n_long && st == BT_OK; k++) {
         const uint64_t off = list[2 * k], c = list[2 * k + 1];
         uint64_t p2 = 1;
         while (p2 < c) p2 <<= 1;
-        void *tmp = nullptr;
-        st = ws_alloc(&tmp, p2 * vb, s);
+        WsGuard g_tmp(s);
+        st = g_tmp.alloc(p2 * vb);
         if (st != BT_OK) break;
         count_launch();
         if (vb == 4)
-            long_segment_sort<uint32_t><<<1, 1024, 0, s>>>((uint32_t *)d_ids, off, c, (uint32_t *)tmp, p2);
+            long_segment_sort<uint32_t><<<1, 1024, 0, s>>>((uint32_t *)d_ids, off, c, g_tmp.as<uint32_t>(), p2);
         else
-            long_segment_sort<uint64_t><<<1, 1024, 0, s>>>((uint64_t *)d_ids, off, c, (uint64_t *)tmp, p2);
-        ws_free(tmp, s);
+            long_segment_sort<uint64_t><<<1, 1024, 0, s>>>((uint64_t *)d_ids, off, c, g_tmp.as<uint64_t>(), p2);
     }
     BT_CUDA(cudaGetLastError());
     return st;

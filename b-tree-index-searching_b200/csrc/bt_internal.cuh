@@ -134,6 +134,22 @@ bt_status cuda_fail(cudaError_t e, const char *what);
 bt_status ws_alloc(void **p, size_t bytes, cudaStream_t s);
 void ws_free(void *p, cudaStream_t s);
 
+// A workspace allocation returned to the pool (stream-ordered) when the
+// guard leaves scope, on every path out of the function.
+struct WsGuard {
+    void *p = nullptr;
+    cudaStream_t s;
+    explicit WsGuard(cudaStream_t st) : s(st) {}
+    WsGuard(const WsGuard &) = delete;
+    WsGuard &operator=(const WsGuard &) = delete;
+    ~WsGuard() {
+        if (p) ws_free(p, s);
+    }
+    bt_status alloc(size_t bytes) { return ws_alloc(&p, bytes, s); }
+    template <typename T>
+    T *as() const { return static_cast<T *>(p); }
+};
+
 // Counts one kernel launch (bt_kernel_launches).
 void count_launch();
 // Number of SMs of the current device (cached).
