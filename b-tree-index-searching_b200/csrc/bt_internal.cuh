@@ -90,8 +90,7 @@ struct LearnedDev {
     int hidden;
     uint32_t nseg;
     int level;             // separator level scanned in the window
-    uint64_t kpe;          // keys per entry of that level (a power of two)
-    int kpe_shift;         // log2(kpe)
+    uint64_t kpe;          // keys per entry of that level
     uint64_t level_entries;
 };
 

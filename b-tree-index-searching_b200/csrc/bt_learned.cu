@@ -303,8 +303,8 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         const int64_t A = (int64_t)sg.r_lo + (int64_t)floor(prc) - (int64_t)sg.eps - 1;
         const int64_t B = (int64_t)sg.r_lo + (int64_t)ceil(prc) + (int64_t)sg.eps + 1;
         const int64_t last = (int64_t)m.level_entries - 1;
-        int64_t ja = (A < 0 ? 0 : A >> m.kpe_shift) - 1;  // A / kpe for A >= 0
-        int64_t jb = (B < 0 ? 0 : B >> m.kpe_shift) + 1;
+        int64_t ja = (A < 0 ? 0 : A / (int64_t)m.kpe) - 1;
+        int64_t jb = (B < 0 ? 0 : B / (int64_t)m.kpe) + 1;
         ja = ja < 0 ? 0 : (ja > last ? last : ja);
         jb = jb < ja ? ja : (jb > last ? last : jb);
         const uint32_t my_ja = (uint32_t)ja, my_jb = (uint32_t)jb;
@@ -538,8 +538,6 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     uint64_t kpe = LeafGeom<K, V>::S;
     for (int l = t->dev.nlevels - 1; l > d.level; l--) kpe *= (uint64_t)(kLineBytes / sizeof(K));
     d.kpe = kpe;
-    d.kpe_shift = 0;
-    while ((1ull << d.kpe_shift) < kpe) d.kpe_shift++;  // S and the fanout are powers of two
     d.level_entries = t->lvl_entries[d.level];
 
     if (rep) {
