@@ -112,6 +112,7 @@ _PROTOS = {
     "bt_sort_pairs": (_I, [_P, _P, _U64, _I, _I, _P, _P, _P]),
     "bt_build_unsorted": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
     "bt_save": (_I, [_P, ctypes.c_char_p]),
+    "bt_build_from_files": (_I, [ctypes.c_char_p, ctypes.c_char_p, _U64, _P, ctypes.POINTER(_P)]),
     "bt_load": (_I, [ctypes.c_char_p, _P, ctypes.POINTER(_P)]),
     "bt_set_search_config": (_I, [_P, _I, _I]),
     "bt_point_search_grouped_noalloc": (_I, [_P, _P, _U64, _P, _P]),
@@ -212,6 +213,18 @@ class Tree:
             st = L.bt_build_host(keys.ctypes.data_as(_P), values.ctypes.data_as(_P), n, kb, vb,
                                  _stream_ptr(stream), ctypes.byref(out))
         _check(st, "bt_build")
+        info = bt_info()
+        _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
+        return cls(out.value, info)
+
+    @classmethod
+    def build_from_files(cls, keys_path, values_path, n):
+        """Build from raw u64 key and value files in the reference program's
+        format (bt_build_from_files)."""
+        L = lib()
+        out = ctypes.c_void_p()
+        _check(L.bt_build_from_files(os.fsencode(keys_path), os.fsencode(values_path), n, None,
+                                     ctypes.byref(out)), "bt_build_from_files")
         info = bt_info()
         _check(L.bt_get_info(out, ctypes.byref(info)), "bt_get_info")
         return cls(out.value, info)

@@ -331,6 +331,39 @@ bt_status stream_file(FILE *f, void *dptr, uint64_t bytes, bool write) {
 
 }  // namespace
 
+bt_status bt_build_from_files(const char *keys_path, const char *values_path, uint64_t n,
+                              void *stream, bt_tree **out) {
+    using namespace bt;
+    if (!keys_path || !values_path || !out) return fail(BT_ERR_INVALID_ARGUMENT, "path or out is NULL");
+    *out = nullptr;
+    if (n == 0) return bt_build(nullptr, nullptr, 0, 8, 8, stream, out);
+    std::vector<uint64_t> hk(n), hv(n);
+    const char *paths[2] = {keys_path, values_path};
+    std::vector<uint64_t> *bufs[2] = {&hk, &hv};
+    for (int i = 0; i < 2; i++) {
+        FILE *f = fopen(paths[i], "rb");
+        if (!f) return fail(BT_ERR_INVALID_ARGUMENT, std::string("cannot open ") + paths[i]);
+        const size_t got = fread(bufs[i]->data(), sizeof(uint64_t), n, f);
+        fclose(f);
+        if (got != n)
+            return fail(BT_ERR_INVALID_ARGUMENT, std::string(paths[i]) + " holds fewer than n values");
+    }
+    int dev = 0;
+    BT_CUDA(cudaGetDevice(&dev));
+    bt_status st = require_device(dev);
+    if (st != BT_OK) return st;
+    cudaStream_t s = (cudaStream_t)stream;
+    WsGuard gk(s), gv(s);
+    st = gk.alloc(n * sizeof(uint64_t));
+    if (st == BT_OK) st = gv.alloc(n * sizeof(uint64_t));
+    if (st != BT_OK) return st;
+    BT_CUDA(cudaMemcpyAsync(gk.p, hk.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    BT_CUDA(cudaMemcpyAsync(gv.p, hv.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    st = bt_build_unsorted(gk.p, gv.p, n, 8, 8, stream, out);
+    BT_CUDA(cudaStreamSynchronize(s));  // the host copies outlive the uploads
+    return st;
+}
+
 bt_status bt_save(const bt_tree *t, const char *path) {
     using namespace bt;
     if (!t || !path) return fail(BT_ERR_INVALID_ARGUMENT, "tree or path is NULL");

@@ -121,6 +121,16 @@ BT_API bt_status bt_build_unsorted(const void *d_keys, const void *d_values, uin
                                    int key_bytes, int value_bytes, void *stream, bt_tree **out);
 
 /*
+ * Build from the reference program's input files: `keys_path` and
+ * `values_path` each hold at least n raw host-endian 64-bit values with no
+ * header (the files main.cu:33-55 reads); the pairs need not be sorted.
+ * Reads both, uploads them, sorts on the device and builds (main.cu:64-129
+ * with genBPlusTree).  u64 keys and values.  Synchronous.
+ */
+BT_API bt_status bt_build_from_files(const char *keys_path, const char *values_path, uint64_t n,
+                                     void *stream, bt_tree **out);
+
+/*
  * Tree image (no counterpart in the reference, which rebuilds from its input
  * files every run): bt_save writes the built leaf blocks, separator levels
  * and their descriptor to one file; bt_load reads it back onto the current

@@ -54,3 +54,25 @@ def test_load_rejects_bad_files(bt, cuda, tmp_path):
         bt.Tree.load(str(cut))
     with pytest.raises(bt.BTreeError):
         bt.Tree.load(str(tmp_path / "missing.img"))
+
+
+def test_build_from_reference_input_files(bt, orc, cuda, tmp_path):
+    """Raw u64 key and data files as the reference program reads them
+    (unsorted, no header); the files may hold more values than n."""
+    g = np.random.default_rng(31)
+    n = 200000
+    keys = np.unique(g.integers(0, 1 << 63, size=n + 1000, dtype=np.uint64))[: n + 10]
+    g.shuffle(keys)
+    data = g.integers(0, 1 << 63, size=len(keys), dtype=np.uint64)
+    kp, dp = tmp_path / "keys.bin", tmp_path / "data.bin"
+    keys.tofile(kp)
+    data.tofile(dp)
+    q = np.concatenate([keys[g.integers(0, n, size=5000)],
+                        g.integers(0, 1 << 63, size=5000, dtype=np.uint64)])
+    o = np.argsort(keys[:n], kind="stable")
+    exp = orc.point_search(keys[:n][o], data[:n][o], q)
+    with bt.Tree.build_from_files(str(kp), str(dp), n) as t:
+        assert t.info.num_keys == n
+        assert np.array_equal(t.point_search(dev(q, cuda)).cpu().numpy(), exp)
+    with pytest.raises(bt.BTreeError):
+        bt.Tree.build_from_files(str(kp), str(dp), len(keys) + 1)
