@@ -231,7 +231,7 @@ BT_API bt_status bt_range_search(const bt_tree *tree, int mode, const void *d_lo
                           uint64_t ids_capacity, uint64_t *h_total, void *stream);
 
 /*
- * Rectangle search over 2-D points (north-star extension; the reference only
+ * Rectangle search over 2-D points (an extension beyond the reference's path; the reference only
  * reorders 1-D range queries by a Z-order of (start, end), zOrder2d.cu:27-54).
  * The tree's keys are 32-bit Morton codes of (x, y) in u16 (x in the even
  * bits, y in the odd bits), its values point IDs; rectangle i is
@@ -251,7 +251,7 @@ BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *
                               const void *h_hi, uint64_t nq, uint64_t *h_counts,
                               void *stream);
 
-/* ---- learned position model (north-star extension; the reference has no
+/* ---- learned position model (an extension beyond the reference's path; the reference has no
  * counterpart: its descent is always the page walk of
  * BPTreeExactSearch.cu:39-68) ------------------------------------------ */
 
@@ -317,7 +317,7 @@ BT_API bt_status bt_mlp_loss_grad(const float *d_params, uint32_t hidden, const 
                                   const float *d_y, uint64_t n, float *d_loss, float *d_grad,
                                   void *stream);
 
-/* ---- batched forest of uneven trees (north-star extension; in the
+/* ---- batched forest of uneven trees (an extension beyond the reference's path; in the
  * reference each tree is its own genBPlusTree + search host calls) ------ */
 
 typedef struct bt_forest bt_forest;
@@ -355,7 +355,7 @@ BT_API bt_status bt_forest_plan_create(const bt_forest *forest, const void *d_qu
 BT_API bt_status bt_forest_plan_run(bt_forest_plan *plan, void *stream);
 BT_API bt_status bt_forest_plan_destroy(bt_forest_plan *plan);
 
-/* ---- continuous-batching request loop (north-star extension; the reference
+/* ---- continuous-batching request loop (an extension beyond the reference's path; the reference
  * runs one synchronous batch per host call, BPTreeExactSearch.cu:409-484) */
 
 typedef struct bt_server bt_server;
