@@ -22,6 +22,7 @@
 // A pass is stable, so the order is deterministic (the reference's in-block
 // atomicAdd scatter is not, grouping.cu:451-452).
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "bt_internal.cuh"
@@ -391,14 +392,14 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
     }
     const size_t smem = (size_t)kPTile * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t) + 1);
     auto scat = part_scatter_kernel<K, HAS_B>;
-    static bool attr_done[64] = {};  // per device, per instantiation
+    static std::atomic<bool> attr_done[64] = {};  // per device, per instantiation; any host thread
     int dev = 0;
     cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_done[dev]) {
+    if (dev < 0 || dev >= 64 || !attr_done[dev].load(std::memory_order_acquire)) {
         cudaError_t e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaFuncSetAttribute");
-        else if (dev >= 0 && dev < 64) attr_done[dev] = true;
+        else if (dev >= 0 && dev < 64) attr_done[dev].store(true, std::memory_order_release);
     }
     const K *ia = d_a, *ib = d_b;
     const uint32_t *ip = nullptr;
