@@ -112,7 +112,7 @@ __device__ __forceinline__ uint32_t block_exscan256(uint32_t v, uint32_t *warp_t
 }
 
 template <typename K, bool HAS_B>
-__global__ void __launch_bounds__(kPT)
+__global__ void __launch_bounds__(kPT, 3)
 part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
                     const uint32_t *__restrict__ perm_in, uint64_t n, GroupKeyParams gp, int pass,
                     const uint32_t *__restrict__ base, uint64_t ntiles, K *__restrict__ oa,
