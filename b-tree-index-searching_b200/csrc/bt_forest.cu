@@ -282,7 +282,7 @@ struct ForestDev {
 // search there resolves every level above it, the remaining levels and the
 // leaf are walked by lane groups as in the single-tree kernels.
 template <typename K, typename V, int G, int R>
-__global__ void __launch_bounds__(kFThreads, 3)
+__global__ void __launch_bounds__(kFThreads, 4)
 forest_kernel(const __grid_constant__ ForestDev f, const FItem *__restrict__ items, uint64_t n_items,
               unsigned long long *__restrict__ counter, const K *__restrict__ q,
               V *__restrict__ out, const K *__restrict__ lo, const K *__restrict__ hi,
