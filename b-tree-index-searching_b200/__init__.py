@@ -62,16 +62,18 @@ class bt_info(ctypes.Structure):
 
 
 class bt_learned_config(ctypes.Structure):
-    _fields_ = [("num_segments", ctypes.c_uint32), ("hidden", ctypes.c_uint32),
-                ("iterations", ctypes.c_uint32), ("sample_stride", ctypes.c_uint32),
+    _fields_ = [("num_segments", ctypes.c_uint32), ("max_error", ctypes.c_uint32),
+                ("hidden", ctypes.c_uint32), ("iterations", ctypes.c_uint32),
                 ("learning_rate", ctypes.c_float)]
 
 
 class bt_learned_report(ctypes.Structure):
     _fields_ = [("root_loss_initial", ctypes.c_float), ("root_loss_final", ctypes.c_float),
-                ("num_segments", ctypes.c_uint32), ("model_level", ctypes.c_uint32),
-                ("keys_per_entry", ctypes.c_uint64), ("eps_mean", ctypes.c_double),
-                ("eps_max", ctypes.c_uint64), ("window_lines_mean", ctypes.c_double),
+                ("root_error", ctypes.c_uint32), ("root_error_initial", ctypes.c_uint32),
+                ("num_segments", ctypes.c_uint32), ("max_error", ctypes.c_uint32),
+                ("eps_max", ctypes.c_uint64), ("eps_mean", ctypes.c_double),
+                ("code_lines_mean", ctypes.c_double), ("index_bytes", ctypes.c_uint64),
+                ("keys_per_unit", ctypes.c_uint32), ("pad", ctypes.c_uint32),
                 ("train_ms", ctypes.c_double)]
 
 
@@ -108,7 +110,6 @@ _PROTOS = {
     "bt_range_count_host": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
     "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
     "bt_kernel_launches": (ctypes.c_uint64, []),
-    "bt_measure_gather": (_I, [_U64, _U64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "bt_sort_pairs": (_I, [_P, _P, _U64, _I, _I, _P, _P, _P]),
     "bt_build_unsorted": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
     "bt_save": (_I, [_P, ctypes.c_char_p]),
@@ -318,15 +319,15 @@ class Tree:
         return out
 
     # -- learned position model -------------------------------------------
-    def learned_train(self, num_segments=65536, hidden=16, iterations=400, sample_stride=0,
+    def learned_train(self, num_segments=65536, max_error=0, hidden=16, iterations=400,
                       learning_rate=0.01, stream=None):
-        """Train the two-stage model on this tree's keys; returns the report
-        as a dict (losses, error bounds, window size, training time)."""
-        cfg = bt_learned_config(num_segments, hidden, iterations, sample_stride, learning_rate)
+        """Build the learned index of this tree (segmentation, root training,
+        unit thresholds); returns the report as a dict."""
+        cfg = bt_learned_config(num_segments, max_error, hidden, iterations, learning_rate)
         rep = bt_learned_report()
         _check(lib().bt_learned_train(self._h, ctypes.byref(cfg), _stream_ptr(stream),
                                       ctypes.byref(rep)), "bt_learned_train")
-        return {k: getattr(rep, k) for k, _ in bt_learned_report._fields_}
+        return {k: getattr(rep, k) for k, _ in bt_learned_report._fields_ if k != "pad"}
 
     def point_search_learned(self, queries, out=None, stream=None):
         """Point search through the learned model (same results as point_search)."""
@@ -340,7 +341,7 @@ class Tree:
         return out
 
     def learned_last_stats(self):
-        """(queries answered through the model window, queries that fell back)."""
+        """(leaf units read beyond the first, queries that took the full descent)."""
         w, f = _U64(), _U64()
         _check(lib().bt_learned_last_stats(self._h, ctypes.byref(w), ctypes.byref(f)),
                "bt_learned_last_stats")
@@ -613,9 +614,47 @@ def sort_pairs(keys, values, stream=None):
     return ok, ov
 
 
+PROBE_LIB_PATH = os.path.join(PKG_DIR, "lib", "libbt_probe.so")
+_probe = None
+
+
+def probe_lib():
+    """The benchmark's memory-system probes (lib/libbt_probe.so, built from
+    probe/bt_probe.cu).  A measurement aid: no search path uses it."""
+    global _probe
+    if _probe is None:
+        if not os.path.exists(PROBE_LIB_PATH):
+            raise RuntimeError(f"{PROBE_LIB_PATH} is not built (run build.py)")
+        h = ctypes.CDLL(PROBE_LIB_PATH)
+        h.btp_last_error.restype = ctypes.c_char_p
+        h.btp_measure_gather.restype = _I
+        h.btp_measure_gather.argtypes = [_U64, _U64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
+        h.btp_measure_chain.restype = _I
+        h.btp_measure_chain.argtypes = [_U64, _U64, _U64, ctypes.c_uint32, ctypes.c_uint32,
+                                        ctypes.c_uint32, _I, ctypes.POINTER(ctypes.c_double)]
+        _probe = h
+    return _probe
+
+
+def _probe_check(st, where):
+    if st != 0:
+        raise BTreeError(1, where, probe_lib().btp_last_error().decode())
+
+
 def measure_gather(region_bytes, n_reads=1 << 24, block_bytes=64):
-    """Random block reads per second the current GPU sustains (bt_measure_gather)."""
+    """Random block reads per second the current GPU sustains (btp_measure_gather)."""
     r = ctypes.c_double(0)
-    _check(lib().bt_measure_gather(region_bytes, n_reads, block_bytes, ctypes.byref(r)),
-           "bt_measure_gather")
+    _probe_check(probe_lib().btp_measure_gather(region_bytes, n_reads, block_bytes, ctypes.byref(r)),
+                 "btp_measure_gather")
+    return r.value
+
+
+def measure_chain(line_bytes, leaf_bytes, n_queries=1 << 24, leaf_read=128, lines_per_query=1,
+                  in_flight=2, warm=True):
+    """Queries per second of "random 128-byte line(s) from an L2-sized array,
+    then one dependent random leaf read" (btp_measure_chain)."""
+    r = ctypes.c_double(0)
+    _probe_check(probe_lib().btp_measure_chain(line_bytes, leaf_bytes, n_queries, leaf_read,
+                                               lines_per_query, in_flight, int(warm),
+                                               ctypes.byref(r)), "btp_measure_chain")
     return r.value

@@ -1,6 +1,8 @@
 """Build recipe for the engine's shared library (sm_100a only).
 
     python b-tree-index-searching_b200/build.py        # -> lib/libbtree_b200.so
+                                                       #    lib/btree (the reference's CLI)
+                                                       #    lib/libbt_probe.so (bench probes)
 
 nvcc cross-compiles for sm_100a without a GPU.  The library is built in-tree
 so it travels with the working tree; nothing is installed.
@@ -14,7 +16,10 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libbtree_b200.so")
-COMPAT_DRIVER = os.path.join(LIBDIR, "compat_driver")
+CLI_SRC = os.path.join(PKG, "cli", "btree_main.cpp")
+CLI = os.path.join(LIBDIR, "btree")
+PROBE_SRC = os.path.join(PKG, "probe", "bt_probe.cu")
+PROBE_LIB = os.path.join(LIBDIR, "libbt_probe.so")
 
 SOURCES = [
     "bt_runtime.cu",
@@ -28,7 +33,6 @@ SOURCES = [
     "bt_server.cu",
     "bt_forest.cu",
     "bt_rect.cu",
-    "bt_probe.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -80,11 +84,16 @@ def build(verbose=False, force=False, ptxas_info=False):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    drv_src = os.path.join(ROOT, "tests", "compat_driver.cpp")
-    if os.path.exists(drv_src) and (force or _stale(COMPAT_DRIVER, [drv_src, LIB] + headers)):
-        cmd = ["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), drv_src,
-               "-o", COMPAT_DRIVER, "-L", LIBDIR, "-lbtree_b200",
-               "-Wl,-rpath,$ORIGIN"]
+    # the benchmark's probes: a separate library the engine does not link
+    if force or _stale(PROBE_LIB, [PROBE_SRC]):
+        cmd = [nvcc] + NVCC_FLAGS + ["-shared", PROBE_SRC, "-o", PROBE_LIB]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    # the reference program's command line over the compat API (lib/btree)
+    if force or _stale(CLI, [CLI_SRC, LIB] + headers):
+        cmd = [nvcc] + ARCH + ["-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"), CLI_SRC,
+                               "-o", CLI, "-L", LIBDIR, "-lbtree_b200", "-Xlinker", "-rpath=$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

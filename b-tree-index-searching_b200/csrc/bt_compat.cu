@@ -1,5 +1,6 @@
 // The reference's C++ host API (BPTree.h:26-55) on top of the C ABI.  See
 // include/btree_b200_compat.h for the conventions kept and the differences.
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -56,6 +57,14 @@ void found_report(const ulli *res, const ulli *q, ulli n) {
     }
     std::cout << "Search step checking complete" << std::endl;
     std::cout << "Found:" << (1 - ((float)miss) / ((float)n)) * 100 << "% of key" << std::endl;
+}
+
+// perm[i] = i: the grouped batch search writes result i to position perm[i],
+// so an identity permutation keeps the results in grouped order.
+__global__ void iota_kernel(uint32_t *perm, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        perm[i] = (uint32_t)i;
 }
 
 void *range_common(ulli *lo, ulli *hi, ulli n, BTPage *pool, int mode, const char *banner) {
@@ -145,8 +154,13 @@ BT_API void *SearchingBTreeGPUCombineStep(ulli *input_key, ulli inputSize, ulli 
         cudaMemcpy(dq, input_key, inputSize * 8, cudaMemcpyHostToDevice);
         double t0 = now_ms();
         check(bt_group_queries(t, dq, inputSize, dg, dperm, nullptr), "genGrouping");
-        // searching the grouped array in place returns results in grouped order
-        check(bt_point_search(t, BT_POINT_BASIC, dg, inputSize, dout, nullptr), "grouped search");
+        // the grouped search kernels (a CTA per run of one group; from 2^21
+        // queries the per-group separator window), results kept in grouped
+        // order as the reference returns them
+        bt::count_launch();
+        iota_kernel<<<(unsigned)std::min<uint64_t>((inputSize + 255) / 256, 4096), 256>>>(dperm,
+                                                                                          inputSize);
+        check(bt_point_search_grouped_batch(t, dg, dperm, inputSize, dout, nullptr), "grouped search");
         if (cudaDeviceSynchronize() != cudaSuccess) check(BT_ERR_CUDA, "grouped search");
         std::cout << "combi Running time Searching State2:" << (now_ms() - t0) << std::endl;
         cudaMemcpy(input_key, dg, inputSize * 8, cudaMemcpyDeviceToHost);

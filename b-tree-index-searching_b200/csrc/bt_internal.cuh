@@ -65,33 +65,55 @@ struct DevTree {
     uint32_t smem_bytes;           // bytes staged (a multiple of 16)
 };
 
-// One leaf model of the learned index (32 bytes): the segment's keys are
+// ---- learned index (see bt_learned.cu) ----------------------------------
+
+constexpr int kSegPerLine = 4;      // segments per segment line
+constexpr int kCodesPerLine = 59;   // thresholds per code line
+constexpr int kUnitBytes = 128;     // a leaf unit: the 128-byte aligned piece of the leaf array
+
+// Four consecutive segments (leaf models) in one 128-byte line, fields
+// side by side: segment i covers the keys [key[i], next segment's key),
 // ranks r_lo .. r_lo + cnt - 1; rank ~ r_lo + clamp(icpt + slope * (key -
-// base), 0, cnt), within eps of the truth for every key of the segment.
-struct SegParam {
+// key[i]), 0, cnt) within eps of the truth for every key of the segment.
+// Unused slots of the last line: key all-ones, r_lo = n, cnt = 0.
+struct SegLine {
+    uint64_t key[kSegPerLine];
+    uint32_t r_lo[kSegPerLine];
+    uint32_t cnt[kSegPerLine];
+    float slope[kSegPerLine];
+    float icpt[kSegPerLine];
+    uint32_t eps[kSegPerLine];
+    uint32_t pad[kSegPerLine];
+};
+
+// Thresholds between consecutive leaf units, 59 per 128-byte line.
+// Threshold j separates unit j from unit j + 1: T_j = base + (code << shift)
+// is the smallest such value above the largest key of unit j, so q >= T_j
+// iff q >= base and ((q - base) >> shift) >= code.
+struct CodeLine {
     uint64_t base;
-    float slope;
-    float icpt;
-    uint32_t r_lo;
-    uint32_t eps;
-    uint32_t cnt;
-    uint32_t pad;
+    uint16_t shift;
+    uint16_t code[kCodesPerLine];
 };
 
 constexpr int kMaxHidden = 32;
 
 // Device view of a trained learned index.
 struct LearnedDev {
-    const float *mlp;      // 3*hidden+1 root parameters
-    const SegParam *seg;   // num_segments leaf models
-    unsigned long long *stats;  // [windowed, fallback] of the last search
-    uint64_t kmin;
+    const float *mlp;        // root parameters (3*hidden+1)
+    const SegLine *seg;      // segment lines
+    const CodeLine *codes;   // code lines
+    const void *stage;       // first key of every segment line (key type), nls entries
+    unsigned long long *stats;  // [extra leaf-unit reads, full-descent fallbacks] of the last search
+    uint64_t kmin;           // root input: x = (key - kmin) * xscale
     float xscale;
     int hidden;
-    uint32_t nseg;
-    int level;             // separator level scanned in the window
-    uint64_t kpe;          // keys per entry of that level
-    uint64_t level_entries;
+    uint32_t nseg;           // segments
+    uint32_t nls;            // segment lines
+    uint32_t root_err;       // |root's line prediction - line| <= root_err at every staged key
+    uint32_t kpu;            // keys per leaf unit
+    uint64_t units;          // leaf units
+    uint32_t stage_bytes;    // shared-memory bytes of the staged keys (whole bank rows)
 };
 
 struct LearnedState;

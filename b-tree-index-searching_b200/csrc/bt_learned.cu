@@ -1,24 +1,34 @@
-// Learned position model: training kernels and the learned point search.
+// Learned index: build kernels (segmentation, root training, unit codes) and
+// the learned point search.
 //
-// No counterpart in the reference (its descent is always the page walk of
-// BPTreeExactSearch.cu:39-68).  Two stages over the tree's (key, rank)
-// pairs:
-//   root   y = b2 + sum_j w2[j] * relu(w1[j] * x + b1[j]),  x = key normalised
-//          to [0,1], y = rank normalised to [0,1); w1, w2 >= 0 keep it
-//          monotone, so the segments it routes to are contiguous key ranges.
-//          Trained by full-batch Adam on MSE with mlp_loss_grad_kernel /
-//          adam_kernel below.
-//   leaves rank = r_lo + icpt + slope * (key - base) per segment, fitted by
-//          least squares; eps = max error over the segment's keys, measured
-//          with the very same FP32 operations the search uses (explicit
-//          round-to-nearest intrinsics, no contraction), so the bound holds
-//          bit for bit.
-// The search turns the predicted rank window into a window of entries on the
-// separator level one above the bottom, scans those lines with the lane
-// group, then descends normally.  If the scan cannot prove the lower bound is
-// inside the window, that query takes the full descent (scalar, per lane).
+// No counterpart in the reference: its descent is always the page walk of
+// BPTreeExactSearch.cu:39-68, here the tree of bt_search.cu.  The learned
+// index sends a point query straight to the 128-byte leaf unit holding its
+// key, so the only DRAM read of a query is that unit; everything before it
+// is on chip (shared memory and L2):
+//
+//   1. root (shared memory): a monotone MLP y = b2 + sum_j w2[j] *
+//      relu(w1[j] * x + b1[j]) (w1, w2 >= 0) of the normalised key predicts
+//      the key's segment line among the nls lines; its worst error root_err
+//      over the lines' first keys bounds a binary search over those keys,
+//      staged in shared memory, to 2 * root_err + 3 entries.
+//   2. segment line (one L2 read): four leaf models; the key's segment gives
+//      a predicted rank p and its bound eps, so the key's rank lies in
+//      [p - eps - 1, p + eps + 1].
+//   3. code lines (one or two L2 reads): the thresholds between the leaf
+//      units of that window; the thresholds at or below the key count the
+//      units to skip.
+//   4. leaf unit (the DRAM read): the key's block(s) and values.
+//
+// Exactness.  Every bound used above is measured on the device with the
+// search's own FP32 operations (explicit round-to-nearest intrinsics, no
+// contraction), and every function of the key involved is monotone, so a
+// bound measured at the keys holds for every query between them.  A query
+// whose key lies just above a unit's threshold bucket lands one unit early
+// and reads the next one; a query that would leave its window (impossible
+// with correct bounds) takes the tree's full descent.  Results therefore
+// always equal the plain search.
 #include <algorithm>
-#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -28,26 +38,37 @@
 namespace bt {
 
 struct LearnedState {
-    float *d_mlp = nullptr;        // 3H+1
-    SegParam *d_seg = nullptr;     // nseg
-    unsigned long long *d_stats = nullptr;  // 2 counters
+    float *d_mlp = nullptr;
+    SegLine *d_seg = nullptr;
+    CodeLine *d_codes = nullptr;
+    void *d_stage = nullptr;
+    unsigned long long *d_stats = nullptr;
+    uint64_t bytes = 0;
     LearnedDev dev;
 };
 
 void free_learned(LearnedState *s) {
     if (!s) return;
-    if (s->d_mlp) cudaFree(s->d_mlp);
-    if (s->d_seg) cudaFree(s->d_seg);
-    if (s->d_stats) cudaFree(s->d_stats);
+    cudaFree(s->d_mlp);
+    cudaFree(s->d_seg);
+    cudaFree(s->d_codes);
+    cudaFree(s->d_stage);
+    cudaFree(s->d_stats);
     delete s;
 }
 
 namespace {
 
+constexpr uint64_t kPlaChunk = 1ull << 14;  // keys per segmentation thread
+constexpr int kHullCap = 32;                 // points per convex hull
+constexpr int kLThreads = 512;               // search CTA (one per SM: the staged keys)
+constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
+constexpr int kMaxWalk = 8;                  // extra units read before the full descent
+
 // ---------------------------------------------------------------- model ---
 
 // Root model in FP32 with explicit round-to-nearest operations (the same
-// arithmetic in training-time assignment, eps measurement and search).
+// arithmetic at training-time error measurement and in the search).
 __device__ __forceinline__ float mlp_eval(const float *p, int H, float x) {
     float out = p[3 * H];
     for (int j = 0; j < H; j++) {
@@ -61,22 +82,22 @@ __device__ __forceinline__ float norm_key(uint64_t key, uint64_t kmin, float xsc
     return __fmul_rn(__ull2float_rn(key > kmin ? key - kmin : 0ull), xscale);
 }
 
-__device__ __forceinline__ uint32_t root_segment(const float *p, int H, uint32_t nseg, float x) {
-    const float y = __fmul_rn(mlp_eval(p, H, x), (float)nseg);
-    if (!(y > 0.f)) return 0;  // also catches NaN
+// Segment line predicted by the root for normalised key x.
+__device__ __forceinline__ int root_line(const float *p, int H, uint32_t nls, float x) {
+    const float y = __fmul_rn(mlp_eval(p, H, x), (float)nls);
+    if (!(y > 0.f)) return 0;  // also NaN
     const float f = floorf(y);
-    return f >= (float)nseg ? nseg - 1 : (uint32_t)f;
+    return f >= (float)nls ? (int)nls - 1 : (int)f;
 }
 
-// Relative rank predicted by a leaf model for a key (FP32, round to
-// nearest), clamped to the segment's rank range [0, cnt]: a key in the gap
-// after the segment's last key (lognormal gaps can be 10^6 wide) must not be
-// extrapolated along the line, its lower bound is at most the next segment's
-// first rank.
-__device__ __forceinline__ float leaf_pred(const SegParam &s, uint64_t key) {
-    const uint64_t d = key > s.base ? key - s.base : 0ull;
-    const float p = __fadd_rn(s.icpt, __fmul_rn(s.slope, __ull2float_rn(d)));
-    return fminf(fmaxf(p, 0.f), (float)s.cnt);
+// Rank offset predicted by a leaf model, clamped to its rank range [0, cnt]
+// (a key in the gap after the segment's last key must not be extrapolated
+// along the line: its lower bound is the next segment's first rank).
+__device__ __forceinline__ float seg_pred(float slope, float icpt, uint32_t cnt, uint64_t fk,
+                                          uint64_t key) {
+    const uint64_t d = key > fk ? key - fk : 0ull;
+    const float p = __fadd_rn(icpt, __fmul_rn(slope, __ull2float_rn(d)));
+    return fminf(fmaxf(p, 0.f), (float)cnt);
 }
 
 template <typename K, typename V>
@@ -85,18 +106,590 @@ __device__ __forceinline__ K leaf_key(const unsigned char *leaves, uint64_t pos)
     return reinterpret_cast<const K *>(leaves + (pos / LG::S) * LG::BS)[pos % LG::S];
 }
 
-// ------------------------------------------------------------- training ---
+// Keys of one 128-byte leaf unit.
+template <typename K, typename V>
+__host__ __device__ constexpr int unit_keys() {
+    return (kUnitBytes / LeafGeom<K, V>::BS) * LeafGeom<K, V>::S;
+}
+
+// ------------------------------------------------------- segmentation -----
+
+struct PlaPt {
+    uint64_t x;  // key - segment's first key
+    int64_t y;   // rank - segment's first rank, +/- eps
+};
+
+// > 0 when b lies above the directed line o -> a (x increasing); exact.
+__device__ __forceinline__ __int128 pla_cross(const PlaPt &o, const PlaPt &a, const PlaPt &b) {
+    const __int128 ax = (__int128)a.x - (__int128)o.x, bx = (__int128)b.x - (__int128)o.x;
+    const __int128 ay = (__int128)a.y - (__int128)o.y, by = (__int128)b.y - (__int128)o.y;
+    return ax * by - ay * bx;
+}
+
+// Slope of the line through a and b and its value at x = 0, in double with
+// explicit rounding (no contraction); flat for two points of one key.
+__device__ __forceinline__ double pla_line_at0(const PlaPt &a, const PlaPt &b, double *slope) {
+    if (b.x == a.x) {  // duplicate keys: a flat line through the middle
+        *slope = 0.0;
+        return __dmul_rn(__dadd_rn(__ll2double_rn(a.y), __ll2double_rn(b.y)), 0.5);
+    }
+    const double dx = __ull2double_rn(b.x - a.x);
+    const double sl = __ddiv_rn(__dsub_rn(__ll2double_rn(b.y), __ll2double_rn(a.y)), dx);
+    *slope = sl;
+    return __dsub_rn(__ll2double_rn(a.y), __dmul_rn(sl, __ull2double_rn(a.x)));
+}
+
+// Error-bounded segmentation of the points (key[i], i) of one chunk of
+// kPlaChunk keys, one thread per chunk: greedy maximal segments, each with a
+// line within eps of all its points (the optimal streaming fit of O'Rourke,
+// CACM 1981, as in the PGM-index, Ferragina & Vinciguerra, VLDB 2020).  An
+// open segment keeps the upper convex hull of its lower points (x, y - eps),
+// the lower convex hull of its upper points (x, y + eps), and the feasible
+// lines of largest (M = Ma-Mb) and smallest (N = Na-Nb) slope; a point is
+// feasible iff its lower point is not above M and its upper point not below
+// N.  A segment also closes when a hull would exceed kHullCap points.
+// COUNT: counts[c] = segments of chunk c.  Otherwise writes segment k of
+// chunk c at offsets[c] + k: first rank and the mean of M and N as
+// rank - first = icpt + slope * (key - first key).
+template <typename K, typename V, bool COUNT>
+__global__ void pla_kernel(const unsigned char *__restrict__ leaves, uint64_t n, uint32_t eps,
+                           uint64_t nchunks, uint64_t *__restrict__ counts,
+                           const uint64_t *__restrict__ offsets, uint32_t *__restrict__ starts,
+                           double *__restrict__ slopes, double *__restrict__ icpts) {
+    const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c >= nchunks) return;
+    PlaPt lh[kHullCap], uh[kHullCap];
+    const int64_t e = (int64_t)eps;
+    const uint64_t end = min(n, (c + 1) * kPlaChunk);
+    uint64_t nseg = 0, out = COUNT ? 0 : offsets[c];
+    uint64_t i = c * kPlaChunk;
+    while (i < end) {
+        const uint64_t s = i;
+        const uint64_t x0 = (uint64_t)leaf_key<K, V>(leaves, s);
+        int nl = 1, nu = 1;
+        lh[0] = {0, -e};
+        uh[0] = {0, e};
+        PlaPt Ma = lh[0], Mb = uh[0], Na = uh[0], Nb = lh[0];
+        uint64_t j = s + 1;
+        if (j < end) {
+            const PlaPt L = {(uint64_t)leaf_key<K, V>(leaves, j) - x0, 1 - e};
+            const PlaPt U = {L.x, 1 + e};
+            Mb = U;
+            Nb = L;
+            lh[nl++] = L;
+            uh[nu++] = U;
+            for (j = s + 2; j < end; j++) {
+                const int64_t y = (int64_t)(j - s);
+                const uint64_t x = (uint64_t)leaf_key<K, V>(leaves, j) - x0;
+                const PlaPt L2 = {x, y - e}, U2 = {x, y + e};
+                if (pla_cross(Ma, Mb, L2) > 0 || pla_cross(Na, Nb, U2) < 0) break;
+                int nl2 = nl, nu2 = nu;
+                while (nl2 >= 2 && pla_cross(lh[nl2 - 2], lh[nl2 - 1], L2) >= 0) nl2--;
+                while (nu2 >= 2 && pla_cross(uh[nu2 - 2], uh[nu2 - 1], U2) <= 0) nu2--;
+                if (nl2 >= kHullCap || nu2 >= kHullCap) break;
+                if (pla_cross(Ma, Mb, U2) < 0) {  // M now pivots on U2
+                    int b = 0;
+                    for (int k = 1; k < nl; k++)
+                        if (pla_cross(lh[b], U2, lh[k]) > 0) b = k;
+                    Ma = lh[b];
+                    Mb = U2;
+                }
+                if (pla_cross(Na, Nb, L2) > 0) {  // N now pivots on L2
+                    int b = 0;
+                    for (int k = 1; k < nu; k++)
+                        if (pla_cross(uh[b], L2, uh[k]) < 0) b = k;
+                    Na = uh[b];
+                    Nb = L2;
+                }
+                lh[nl2] = L2;
+                nl = nl2 + 1;
+                uh[nu2] = U2;
+                nu = nu2 + 1;
+            }
+        }
+        if (!COUNT) {
+            double sl = 0.0, ic = 0.0;
+            if (j - s >= 2) {
+                double sm, sn;
+                const double m0 = pla_line_at0(Ma, Mb, &sm);
+                const double n0 = pla_line_at0(Na, Nb, &sn);
+                sl = __dmul_rn(__dadd_rn(sm, sn), 0.5);
+                ic = __dmul_rn(__dadd_rn(m0, n0), 0.5);
+            }
+            starts[out] = (uint32_t)s;
+            slopes[out] = sl;
+            icpts[out] = ic;
+            out++;
+        }
+        nseg++;
+        i = j;
+    }
+    if (COUNT) counts[c] = nseg;
+}
+
+// Segment lines from the segmentation (one thread per line): first keys,
+// ranks, FP32 lines (slope >= 0 keeps the prediction monotone).  eps is
+// filled by seg_eps_kernel.
+template <typename K, typename V>
+__global__ void seg_fill_kernel(const unsigned char *__restrict__ leaves, uint64_t n,
+                                uint32_t nseg, uint32_t nls, const uint32_t *__restrict__ starts,
+                                const double *__restrict__ slopes, const double *__restrict__ icpts,
+                                SegLine *__restrict__ seg) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nls; l += gridDim.x * blockDim.x) {
+        SegLine sl;
+        for (int k = 0; k < kSegPerLine; k++) {
+            const uint32_t g = l * kSegPerLine + k;
+            if (g < nseg) {
+                const uint32_t a = starts[g];
+                const uint32_t b = g + 1 < nseg ? starts[g + 1] : (uint32_t)n;
+                sl.key[k] = (uint64_t)leaf_key<K, V>(leaves, a);
+                sl.r_lo[k] = a;
+                sl.cnt[k] = b - a;
+                sl.slope[k] = __double2float_rn(fmax(slopes[g], 0.0));
+                sl.icpt[k] = __double2float_rn(icpts[g]);
+            } else {
+                sl.key[k] = ~0ull;
+                sl.r_lo[k] = (uint32_t)n;
+                sl.cnt[k] = 0;
+                sl.slope[k] = 0.f;
+                sl.icpt[k] = 0.f;
+            }
+            sl.eps[k] = 0;
+            sl.pad[k] = 0;
+        }
+        seg[l] = sl;
+    }
+}
+
+// Exact error bound of every segment with the search's arithmetic, one warp
+// per segment: eps = ceil(max |seg_pred(key_i) - (i - r_lo)|).
+template <typename K, typename V>
+__global__ void seg_eps_kernel(const unsigned char *__restrict__ leaves, uint32_t nseg,
+                               SegLine *__restrict__ seg) {
+    const int lane = threadIdx.x & 31;
+    for (uint64_t g = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; g < nseg;
+         g += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        SegLine &sl = seg[g / kSegPerLine];
+        const int k = (int)(g % kSegPerLine);
+        const uint64_t fk = sl.key[k];
+        const uint32_t a = sl.r_lo[k], cnt = sl.cnt[k];
+        const float slope = sl.slope[k], icpt = sl.icpt[k];
+        float err = 0.f;
+        for (uint32_t i = lane; i < cnt; i += 32) {
+            const float p = seg_pred(slope, icpt, cnt, fk, (uint64_t)leaf_key<K, V>(leaves, a + i));
+            err = fmaxf(err, fabsf(__fsub_rn(p, (float)i)));
+        }
+        for (int o = 16; o > 0; o >>= 1) err = fmaxf(err, __shfl_xor_sync(0xffffffffu, err, o));
+        if (lane == 0) {
+            const float ce = ceilf(err);
+            sl.eps[k] = ce >= 4.0e9f ? 0xFFFFFFFFu : (uint32_t)ce;
+        }
+    }
+}
+
+// Staged keys (first key of every segment line) and the root's training
+// pairs (x = normalised key, y = the line's centre in [0, 1)).
+template <typename K>
+__global__ void stage_kernel(const SegLine *__restrict__ seg, uint32_t nls, uint64_t kmin,
+                             float xscale, K *__restrict__ stage, float *__restrict__ x,
+                             float *__restrict__ y) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nls; l += gridDim.x * blockDim.x) {
+        const uint64_t k = seg[l].key[0];
+        stage[l] = (K)k;
+        x[l] = norm_key(k, kmin, xscale);
+        y[l] = (float)(((double)l + 0.5) / (double)nls);
+    }
+}
+
+// Worst |root_line(x_l) - l| over the staged keys.
+__global__ void root_err_kernel(const float *__restrict__ p, int H, const float *__restrict__ x,
+                                uint32_t nls, unsigned int *__restrict__ err) {
+    __shared__ float sp[3 * kMaxHidden + 1];
+    for (int k = threadIdx.x; k < 3 * H + 1; k += blockDim.x) sp[k] = p[k];
+    __syncthreads();
+    unsigned int e = 0;
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nls; l += gridDim.x * blockDim.x) {
+        const int pl = root_line(sp, H, nls, x[l]);
+        const int d = pl - (int)l;
+        e = max(e, (unsigned int)(d < 0 ? -d : d));
+    }
+    for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(err, e);
+}
+
+// Code lines, one thread per line: thresholds j = 59 l .. 59 l + 58 (j <
+// units - 1) between unit j and unit j + 1.  base = first key of the line's
+// first unit; shift = the least that fits the line's span in 16 bits; code
+// = ((last key of unit j - base) >> shift) + 1, so T_j = base + (code <<
+// shift) is the least multiple above unit j's keys.
+template <typename K, typename V>
+__global__ void code_kernel(const unsigned char *__restrict__ leaves, uint64_t n, uint64_t units,
+                            uint64_t ncl, CodeLine *__restrict__ codes) {
+    constexpr uint64_t KPU = unit_keys<K, V>();
+    for (uint64_t l = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; l < ncl;
+         l += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t j0 = l * kCodesPerLine;
+        const uint64_t j1 = min(j0 + kCodesPerLine, units - 1);  // exclusive
+        CodeLine cl;
+        cl.base = (uint64_t)leaf_key<K, V>(leaves, j0 * KPU);
+        const uint64_t top = (uint64_t)leaf_key<K, V>(leaves, min(j1 * KPU, n) - 1);
+        const uint64_t span = top - cl.base;
+        int sh = 0;
+        while ((span >> sh) >= 0xFFFFull) sh++;
+        cl.shift = (uint16_t)sh;
+        for (uint64_t j = j0; j < j0 + kCodesPerLine; j++) {
+            uint16_t c = 0xFFFF;
+            if (j < j1) {
+                const uint64_t last = (uint64_t)leaf_key<K, V>(leaves, (j + 1) * KPU - 1);
+                c = (uint16_t)(((last - cl.base) >> sh) + 1);
+            }
+            cl.code[j - j0] = c;
+        }
+        codes[l] = cl;
+    }
+}
+
+// ------------------------------------------------------------- search -----
+
+// 32-byte load of an index line piece: read-only path, no L1 allocation,
+// kept in L2 ahead of the streaming leaf reads (evict-last).
+__device__ __forceinline__ void load_line32(const void *p, uint32_t (&w)[8]) {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile(
+        "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]),
+          "=r"(w[7])
+        : "l"(p), "l"(pol));
+}
+
+// 32-byte load of a leaf-unit piece (touched once per query): evict-first.
+__device__ __forceinline__ void load_unit32(const void *p, uint32_t (&w)[8]) {
+    asm volatile(
+        "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]),
+          "=r"(w[7])
+        : "l"(p), "l"(l2_evict_first()));
+}
+
+__device__ __forceinline__ uint32_t sel4(const uint32_t *w, int i) {
+    return i == 0 ? w[0] : i == 1 ? w[1] : i == 2 ? w[2] : w[3];
+}
+
+// Last staged index in [a, b] whose key is below q (a when none: then a == 0
+// by the root's bound).  Routing by "first key < q" sends a key equal to a
+// segment's first key to the segment before, whose window reaches one rank
+// past its end; with duplicate keys it finds the first occurrence.
+template <typename K>
+__device__ __forceinline__ uint32_t stage_search(const K *__restrict__ s, uint32_t a, uint32_t b,
+                                                 K q) {
+    uint32_t base = a, len = b - a + 1;
+    while (len > 1) {
+        const uint32_t half = len >> 1;
+        base = s[swz<K>(base + half)] < q ? base + half : base;
+        len -= half;
+    }
+    return base;
+}
+
+// Scalar full descent of the tree for one query (the fallback).
+template <typename K, typename V>
+__device__ V tree_point(const DevTree &t, K q) {
+    using LG = LeafGeom<K, V>;
+    const K tmax = (K)t.max_key;
+    if (q > tmax) return key_max<V>();
+    const uint32_t blk = block_lower_bound<K>(t, q);
+    const unsigned char *b = static_cast<const unsigned char *>(t.leaves) + (size_t)blk * LG::BS;
+    const K *kb = reinterpret_cast<const K *>(b);
+    for (int i = 0; i < LG::S; i++)
+        if (kb[i] == q && (uint64_t)blk * LG::S + i < t.n)
+            return reinterpret_cast<const V *>(b + kSectorBytes)[i];
+    return key_max<V>();
+}
+
+// One warp tile = 32 queries; a group of 4 lanes owns queries grp, grp + 8,
+// grp + 16, grp + 24 of the tile and keeps all four in flight.
+template <typename K, typename V>
+__global__ void __launch_bounds__(kLThreads, 1)
+learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
+               const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
+    using LG = LeafGeom<K, V>;
+    constexpr int NQ = 4;                       // queries per group
+    constexpr int KPU = unit_keys<K, V>();      // keys per unit
+    constexpr int BPU = kUnitBytes / LG::BS;    // blocks per unit (1 or 2)
+    extern __shared__ uint4 smem_l[];
+    K *s_stage = reinterpret_cast<K *>(smem_l);
+    float *s_mlp = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem_l) + m.stage_bytes);
+    {
+        const K *src = static_cast<const K *>(m.stage);
+        const uint32_t ns = m.stage_bytes / sizeof(K);
+        for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x)
+            s_stage[swz<K>(i)] = i < m.nls ? src[i] : key_max<K>();
+        for (int k = threadIdx.x; k < 3 * m.hidden + 1; k += blockDim.x) s_mlp[k] = m.mlp[k];
+    }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int grp = lane >> 2, gl = lane & 3, g0 = grp * 4;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    const uint64_t leaf_bytes = t.n_sectors * (uint64_t)LG::BS;
+    const uint64_t n = t.n;
+    const uint64_t U = m.units;
+    const uint64_t ntiles = (nq + 31) / 32;
+    unsigned long long n_extra = 0, n_fallback = 0;
+
+    for (uint64_t tile = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; tile < ntiles;
+         tile += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        const uint64_t base = tile * 32;
+        // ---- 1. root + staged keys: the query's segment line (one lane per query)
+        const uint64_t my = base + lane;
+        const K myq = my < nq ? q[my] : (K)0;
+        uint32_t my_sl;
+        {
+            const int pl = root_line(s_mlp, m.hidden, m.nls, norm_key((uint64_t)myq, m.kmin, m.xscale));
+            const int e = (int)m.root_err + 1;
+            const uint32_t a = (uint32_t)max(0, pl - e);
+            const uint32_t b = (uint32_t)min((int)m.nls - 1, pl + e);
+            my_sl = stage_search<K>(s_stage, a, b, myq);
+        }
+        K qv[NQ];
+        bool live[NQ];
+        uint32_t w[NQ][8];
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            const int k = s * 8 + grp;
+            qv[s] = __shfl_sync(0xffffffffu, myq, k);
+            live[s] = base + k < nq;
+            const uint32_t sl = __shfl_sync(0xffffffffu, my_sl, k);
+            if (live[s]) load_line32(reinterpret_cast<const unsigned char *>(m.seg + sl) + gl * 32, w[s]);
+        }
+        // ---- 2. segment -> rank window -> unit window [ua, ub]
+        uint32_t ua[NQ], ub[NQ];
+        int nlines[NQ];
+        int maxl = 0;
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            int c = 0;
+            if (gl == 0) {
+#pragma unroll
+                for (int i = 1; i < kSegPerLine; i++) {
+                    const uint64_t k = ((uint64_t)w[s][2 * i + 1] << 32) | w[s][2 * i];
+                    c += k < (uint64_t)qv[s] ? 1 : 0;
+                }
+            }
+            c = __shfl_sync(0xffffffffu, c, g0);
+            uint32_t a = 0, b = 0;
+            if (gl == 0) {
+                a = c == 0 ? w[s][0] : c == 1 ? w[s][2] : c == 2 ? w[s][4] : w[s][6];
+                b = c == 0 ? w[s][1] : c == 1 ? w[s][3] : c == 2 ? w[s][5] : w[s][7];
+            } else if (gl == 3) {
+                a = sel4(w[s], c);  // eps
+            } else {
+                a = sel4(w[s], c);      // r_lo (lane 1) or slope (lane 2)
+                b = sel4(w[s] + 4, c);  // cnt (lane 1) or icpt (lane 2)
+            }
+            const uint64_t fk = ((uint64_t)__shfl_sync(0xffffffffu, b, g0) << 32) |
+                                __shfl_sync(0xffffffffu, a, g0);
+            const uint32_t r_lo = __shfl_sync(0xffffffffu, a, g0 + 1);
+            const uint32_t cnt = __shfl_sync(0xffffffffu, b, g0 + 1);
+            const float slope = __uint_as_float(__shfl_sync(0xffffffffu, a, g0 + 2));
+            const float icpt = __uint_as_float(__shfl_sync(0xffffffffu, b, g0 + 2));
+            const uint32_t eps = __shfl_sync(0xffffffffu, a, g0 + 3);
+            const float p = seg_pred(slope, icpt, cnt, fk, (uint64_t)qv[s]);
+            const int64_t ra = (int64_t)r_lo + (int64_t)floorf(p) - (int64_t)eps - 1;
+            const int64_t rb = (int64_t)r_lo + (int64_t)ceilf(p) + (int64_t)eps + 1;
+            const uint64_t a_u = ra <= 0 ? 0 : min((uint64_t)ra / KPU, U - 1);
+            const uint64_t b_u = rb <= 0 ? 0 : min((uint64_t)rb / KPU, U - 1);
+            ua[s] = (uint32_t)a_u;
+            ub[s] = (uint32_t)(b_u < a_u ? a_u : b_u);
+            nlines[s] = (live[s] && ub[s] > ua[s])
+                            ? (int)((ub[s] - 1) / kCodesPerLine - ua[s] / kCodesPerLine) + 1
+                            : 0;
+            maxl = max(maxl, nlines[s]);
+        }
+        // ---- 3. code lines of the window: thresholds at or below the key
+        maxl = (int)__reduce_max_sync(0xffffffffu, (unsigned)maxl);
+        uint32_t skip[NQ];
+#pragma unroll
+        for (int s = 0; s < NQ; s++) skip[s] = 0;
+        for (int l = 0; l < maxl; l++) {
+            uint32_t cw[NQ][8];
+#pragma unroll
+            for (int s = 0; s < NQ; s++)
+                if (l < nlines[s])
+                    load_line32(reinterpret_cast<const unsigned char *>(m.codes + ua[s] / kCodesPerLine + l) +
+                                    gl * 32,
+                                cw[s]);
+#pragma unroll
+            for (int s = 0; s < NQ; s++) {
+                const bool act = l < nlines[s];
+                const uint32_t b0 = __shfl_sync(0xffffffffu, act ? cw[s][0] : 0u, g0);
+                const uint32_t b1 = __shfl_sync(0xffffffffu, act ? cw[s][1] : 0u, g0);
+                const uint32_t shw = __shfl_sync(0xffffffffu, act ? cw[s][2] : 0u, g0);
+                if (!act) continue;
+                const uint64_t lbase = ((uint64_t)b1 << 32) | b0;
+                const uint32_t j0 = (ua[s] / kCodesPerLine + l) * kCodesPerLine;
+                const uint64_t key = (uint64_t)qv[s];
+                if (key < lbase) continue;  // every threshold of the line is above the key
+                const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
+                const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
+                // lane 0: codes 0..10 (half-words 5..15: after the base and the
+                // shift); lane g > 0: codes 16 g - 5 .. 16 g + 10
+#pragma unroll
+                for (int h2 = 0; h2 < 16; h2++) {
+                    if (gl == 0 && h2 < 5) continue;
+                    const uint32_t j = j0 + (uint32_t)(16 * gl + h2 - 5);
+                    const uint32_t code = (cw[s][h2 >> 1] >> ((h2 & 1) * 16)) & 0xFFFFu;
+                    skip[s] += (j >= ua[s] && j < ub[s] && code <= qd) ? 1u : 0u;
+                }
+            }
+        }
+        // ---- 4. the leaf unit (walking right past a threshold bucket)
+        uint32_t unit[NQ];
+#pragma unroll
+        for (int s = 0; s < NQ; s++) {
+            uint32_t c = skip[s];
+            c += __shfl_xor_sync(0xffffffffu, c, 1);
+            c += __shfl_xor_sync(0xffffffffu, c, 2);
+            unit[s] = ua[s] + c;
+        }
+        bool pend[NQ];
+#pragma unroll
+        for (int s = 0; s < NQ; s++) pend[s] = live[s];
+        for (int it = 0; it <= kMaxWalk; it++) {
+            uint32_t u[NQ][8];
+#pragma unroll
+            for (int s = 0; s < NQ; s++) {
+                const uint64_t off = (uint64_t)unit[s] * kUnitBytes + gl * 32;
+                if (pend[s] && off < leaf_bytes) {
+                    load_unit32(leaves + off, u[s]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 8; k++) u[s][k] = 0xFFFFFFFFu;  // padding keys
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < NQ; s++) {
+                // key pieces: lanes 0 and 2 (two blocks) or lane 0 (one block)
+                const bool key_lane = BPU == 2 ? (gl == 0 || gl == 2) : gl == 0;
+                const int blk = BPU == 2 ? gl / 2 : 0;
+                int below = 0;
+                bool eq = false;
+                K last = 0;
+                if (key_lane) {
+#pragma unroll
+                    for (int i = 0; i < LG::S; i++) {
+                        const K k = key_at<K>(u[s], i);
+                        const uint64_t rank = (uint64_t)unit[s] * KPU + (uint64_t)blk * LG::S + i;
+                        const bool real = rank < n;
+                        below += (real && k < qv[s]) ? 1 : 0;
+                        eq |= real && k == qv[s];
+                        if (real) last = k;
+                    }
+                }
+                const unsigned gm = 0xFu << g0;
+                const bool found = (__ballot_sync(0xffffffffu, pend[s] && eq) & gm) != 0;
+                int pos = __shfl_sync(0xffffffffu, below, g0);
+                if (BPU == 2) pos += __shfl_sync(0xffffffffu, below, g0 + 2);
+                // the unit's largest key (only read for units before the last,
+                // whose blocks are all full): the last key of its last block
+                const int ll = BPU == 2 ? g0 + 2 : g0;
+                K lastk = (K)__shfl_sync(0xffffffffu, (uint32_t)last, ll);
+                if constexpr (sizeof(K) == 8)
+                    lastk |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)last >> 32), ll) << 32;
+                const bool walk = pend[s] && !found && qv[s] > lastk && unit[s] + 1 < U &&
+                                  unit[s] + 1 <= ub[s];
+                const bool lost = pend[s] && !found && qv[s] > lastk && unit[s] + 1 < U &&
+                                  unit[s] + 1 > ub[s];
+                if (pend[s] && !walk && !lost) {
+                    // the lane holding the value writes the result
+                    int vl, vw;
+                    if (BPU == 2) {
+                        const int b = pos / LG::S, i = pos % LG::S;
+                        vl = 2 * b + 1;
+                        vw = i * (int)(sizeof(V) / 4);
+                    } else {
+                        const int byte = kSectorBytes + pos * (int)sizeof(V);
+                        vl = byte / 32;
+                        vw = (byte % 32) / 4;
+                    }
+                    if (!found) {
+                        if (gl == 0) out[base + s * 8 + grp] = key_max<V>();
+                    } else if (gl == vl) {
+                        V val;
+                        if constexpr (sizeof(V) == 4) {
+                            val = u[s][0];
+#pragma unroll
+                            for (int k = 1; k < 8; k++)
+                                if (k == vw) val = u[s][k];
+                        } else {
+                            val = ((uint64_t)u[s][1] << 32) | u[s][0];
+#pragma unroll
+                            for (int k = 2; k < 8; k += 2)
+                                if (k == vw) val = ((uint64_t)u[s][k + 1] << 32) | u[s][k];
+                        }
+                        out[base + s * 8 + grp] = val;
+                    }
+                    pend[s] = false;
+                } else if (walk) {
+                    unit[s]++;
+                    if (gl == 0 && it < kMaxWalk) n_extra++;
+                }
+                if (lost || (walk && it == kMaxWalk)) {
+                    // outside the window: the tree's full descent
+                    if (gl == 0) {
+                        out[base + s * 8 + grp] = tree_point<K, V>(t, qv[s]);
+                        n_fallback++;
+                    }
+                    pend[s] = false;
+                }
+            }
+            bool any = false;
+#pragma unroll
+            for (int s = 0; s < NQ; s++) any |= pend[s];
+            if (!__any_sync(0xffffffffu, any)) break;
+        }
+    }
+    if (m.stats && (n_extra | n_fallback)) {
+        atomicAdd(&m.stats[0], n_extra);
+        atomicAdd(&m.stats[1], n_fallback);
+    }
+}
 
 template <typename K, typename V>
-__global__ void sample_kernel(const unsigned char *__restrict__ leaves, uint64_t n, uint64_t m,
-                              uint64_t stride, uint64_t kmin, float xscale, float *__restrict__ x,
-                              float *__restrict__ y) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t pos = i * stride;
-        x[i] = norm_key((uint64_t)leaf_key<K, V>(leaves, pos), kmin, xscale);
-        y[i] = (float)((double)pos / (double)n);
+bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
+                         cudaStream_t s) {
+    const LearnedDev &m = t->learned->dev;
+    auto fn = learned_kernel<K, V>;
+    const size_t smem = (size_t)m.stage_bytes + (3 * kMaxHidden + 1) * sizeof(float);
+    static int set_for[64] = {0};
+    int dev = t->device;
+    if (dev >= 0 && dev < 64 && set_for[dev] < (int)smem) {
+        BT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        set_for[dev] = (int)smem;
     }
+    const uint64_t ntiles = (nq + 31) / 32;
+    const uint64_t want = (ntiles + kLThreads / 32 - 1) / (kLThreads / 32);
+    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, sm_count()));
+    count_launch();
+    fn<<<grid, kLThreads, smem, s>>>(t->dev, m, (const K *)d_q, nq, (V *)d_out);
+    BT_CUDA(cudaGetLastError());
+    return BT_OK;
+}
+
+// ------------------------------------------------------------- training ---
+
+struct DevBuf {
+    void *p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+unsigned grid_of(uint64_t n, int block, int per_sm = 8) {
+    uint64_t g = (n + block - 1) / block;
+    const uint64_t cap = (uint64_t)sm_count() * per_sm;
+    return (unsigned)std::max<uint64_t>(1, std::min(g, cap));
 }
 
 // loss = mean((f(x) - y)^2) and its gradient w.r.t. the 3H+1 parameters,
@@ -162,326 +755,125 @@ __global__ void adam_kernel(float *p, const float *grad, float *m, float *v, int
     p[k] = w;
 }
 
-// r_lo[s] = first rank routed to segment >= s (r_lo[nseg] = n).  The root is
-// monotone and keys ascend, so segments are contiguous rank ranges.
-template <typename K, typename V>
-__global__ void assign_kernel(const unsigned char *__restrict__ leaves, uint64_t n,
-                              const float *__restrict__ p, int H, uint32_t nseg, uint64_t kmin,
-                              float xscale, uint32_t *__restrict__ r_lo) {
-    __shared__ float sp[3 * kMaxHidden + 1];
-    for (int k = threadIdx.x; k < 3 * H + 1; k += blockDim.x) sp[k] = p[k];
-    __syncthreads();
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = root_segment(sp, H, nseg,
-                                        norm_key((uint64_t)leaf_key<K, V>(leaves, i), kmin, xscale));
-        const uint32_t prev =
-            i == 0 ? 0u
-                   : root_segment(sp, H, nseg,
-                                  norm_key((uint64_t)leaf_key<K, V>(leaves, i - 1), kmin, xscale)) + 1;
-        for (uint32_t t = (i == 0 ? 0u : prev); t <= s; t++) r_lo[t] = (uint32_t)i;
-        if (i == n - 1)
-            for (uint32_t t = s + 1; t <= nseg; t++) r_lo[t] = (uint32_t)n;
-    }
-}
-
-// Least-squares leaf models and their exact error bounds, one warp per segment.
-template <typename K, typename V>
-__global__ void fit_kernel(const unsigned char *__restrict__ leaves, uint64_t n, uint32_t nseg,
-                           const uint32_t *__restrict__ r_lo, SegParam *__restrict__ seg) {
-    const int lane = threadIdx.x & 31;
-    for (uint64_t s = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; s < nseg;
-         s += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
-        const uint32_t a = r_lo[s], b = r_lo[s + 1];
-        SegParam sp;
-        sp.base = a < n ? (uint64_t)leaf_key<K, V>(leaves, a) : (uint64_t)leaf_key<K, V>(leaves, n - 1);
-        sp.r_lo = a;
-        sp.cnt = b - a;
-        sp.pad = 0;
-        double sx = 0, sy = 0, sxx = 0, sxy = 0;
-        for (uint32_t i = a + lane; i < b; i += 32) {
-            const uint64_t k = (uint64_t)leaf_key<K, V>(leaves, i);
-            const double xv = (double)__ull2float_rn(k - sp.base);
-            const double yv = (double)(i - a);
-            sx += xv;
-            sy += yv;
-            sxx += xv * xv;
-            sxy += xv * yv;
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            sx += __shfl_xor_sync(0xffffffffu, sx, o);
-            sy += __shfl_xor_sync(0xffffffffu, sy, o);
-            sxx += __shfl_xor_sync(0xffffffffu, sxx, o);
-            sxy += __shfl_xor_sync(0xffffffffu, sxy, o);
-        }
-        const double c = (double)(b - a);
-        const double den = c * sxx - sx * sx;
-        double slope = 0.0;
-        if (c >= 2 && den > 0) slope = (c * sxy - sx * sy) / den;
-        const double icpt = c > 0 ? (sy - slope * sx) / c : 0.0;
-        sp.slope = (float)slope;
-        sp.icpt = (float)icpt;
-        // exact bound with the search's own arithmetic
-        float e = 0.f;
-        for (uint32_t i = a + lane; i < b; i += 32) {
-            const float pr = leaf_pred(sp, (uint64_t)leaf_key<K, V>(leaves, i));
-            e = fmaxf(e, fabsf(__fsub_rn(pr, (float)(i - a))));
-        }
-        for (int o = 16; o > 0; o >>= 1) e = fmaxf(e, __shfl_xor_sync(0xffffffffu, e, o));
-        const float ce = ceilf(e);
-        sp.eps = ce >= 4.0e9f ? 0xFFFFFFFFu : (uint32_t)ce;
-        if (lane == 0) seg[s] = sp;
-    }
-}
-
-// --------------------------------------------------------------- search ---
-
-constexpr int kThreads = 256;
-constexpr int kMaxWindowLines = 8;
-
-// Full descent for one query by one thread (the fallback): binary search in
-// each node line from global memory, then the leaf block.
-template <typename K, typename V>
-__device__ uint64_t scalar_lower_bound(const DevTree &t, K qe) {
-    constexpr int F = kLineBytes / (int)sizeof(K);
-    using LG = LeafGeom<K, V>;
-    const K *gs = static_cast<const K *>(t.seps);
-    uint64_t node = 0;
-    for (int lvl = 0; lvl < t.nlevels; lvl++) {
-        const K *line = gs + t.lvl_off[lvl] + node * F;
-        int lo = 0, len = F;
-        while (len > 1) {
-            const int half = len >> 1;
-            lo = line[lo + half - 1] < qe ? lo + half : lo;
-            len -= half;
-        }
-        node = node * F + lo;
-    }
-    const K *kb = reinterpret_cast<const K *>(static_cast<const unsigned char *>(t.leaves) +
-                                              node * LG::BS);
-    int c = 0;
-    for (int j = 0; j < LG::S; j++) c += kb[j] < qe;
-    return node * LG::S + c;
-}
-
-template <typename K, typename V, int G, int R>
-__global__ void __launch_bounds__(kThreads)
-learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
-               const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
-    __shared__ float sp[3 * kMaxHidden + 1];
-    __shared__ uint8_t s_bad[kThreads];
-    for (int k = threadIdx.x; k < 3 * m.hidden + 1; k += blockDim.x) sp[k] = m.mlp[k];
-    __syncthreads();
-
-    using LG = LeafGeom<K, V>;
-    constexpr int F = kLineBytes / (int)sizeof(K);
-    constexpr int KPL = F / G;
-    constexpr int NG = 32 / G;
-    constexpr int I = G / R;
-    const int lane = threadIdx.x & 31;
-    const int grp = lane / G;
-    const int gl = lane % G;
-    uint8_t *bad = s_bad + (threadIdx.x & ~31);
-    const K tmax = (K)t.max_key;
-    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    const K *lvl_base = static_cast<const K *>(t.seps) + t.lvl_off[m.level];
-    const uint64_t ntiles = (nq + 31) / 32;
-    unsigned long long n_fallback = 0, n_window = 0;
-
-    for (uint64_t tile = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; tile < ntiles;
-         tile += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
-        const uint64_t base = tile * 32;
-        // phase 1: one lane per query, model -> window of entries on m.level
-        const uint64_t my = base + lane;
-        const K myq = my < nq ? q[my] : (K)0;
-        const K myqe = myq < tmax ? myq : tmax;
-        const uint32_t sid =
-            root_segment(sp, m.hidden, m.nseg, norm_key((uint64_t)myqe, m.kmin, m.xscale));
-        const SegParam sg = m.seg[sid];
-        const float pr = leaf_pred(sg, (uint64_t)myqe);
-        const double prc = fmin(fmax((double)pr, -1.0e12), 1.0e12);
-        const int64_t A = (int64_t)sg.r_lo + (int64_t)floor(prc) - (int64_t)sg.eps - 1;
-        const int64_t B = (int64_t)sg.r_lo + (int64_t)ceil(prc) + (int64_t)sg.eps + 1;
-        const int64_t last = (int64_t)m.level_entries - 1;
-        int64_t ja = (A < 0 ? 0 : A / (int64_t)m.kpe) - 1;
-        int64_t jb = (B < 0 ? 0 : B / (int64_t)m.kpe) + 1;
-        ja = ja < 0 ? 0 : (ja > last ? last : ja);
-        jb = jb < ja ? ja : (jb > last ? last : jb);
-        const uint32_t my_ja = (uint32_t)ja, my_jb = (uint32_t)jb;
-        const int my_lines = (int)(my_jb / F - my_ja / F) + 1;
-        bad[lane] = my_lines > kMaxWindowLines ? 1 : 0;
-        __syncwarp();
-
-        // phase 2: G lanes per query: scan the window, descend, leaf block
-#pragma unroll
-        for (int r = 0; r < R; r++) {
-            K qv[I], qe[I];
-            bool up[I];
-            uint32_t node[I], wa[I], wb[I];
-            bool sbad[I];
-            int lines = 1;
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                const int k = r * (NG * I) + s * NG + grp;
-                qv[s] = __shfl_sync(0xffffffffu, myq, k);
-                wa[s] = __shfl_sync(0xffffffffu, my_ja, k);
-                wb[s] = __shfl_sync(0xffffffffu, my_jb, k);
-                sbad[s] = bad[k] != 0;
-                qe[s] = qv[s] < tmax ? qv[s] : tmax;
-                up[s] = false;
-                const int l = sbad[s] ? 1 : (int)(wb[s] / F - wa[s] / F) + 1;
-                lines = l > lines ? l : lines;
-            }
-            lines = (int)__reduce_max_sync(0xffffffffu, (unsigned)lines);
-            int cnt[I];
-#pragma unroll
-            for (int s = 0; s < I; s++) cnt[s] = 0;
-            for (int w = 0; w < lines; w++) {
-#pragma unroll
-                for (int s = 0; s < I; s++) {
-                    const uint32_t line = wa[s] / F + w;
-                    const uint32_t e0 = line * F + gl * KPL;
-                    if (!sbad[s] && line * F <= wb[s]) {
-                        uint32_t c[KPL * sizeof(K) / 4];
-                        load_bytes<KPL * (int)sizeof(K)>(lvl_base + (size_t)e0, c);
-#pragma unroll
-                        for (int k = 0; k < KPL; k++) {
-                            const uint32_t e = e0 + k;
-                            cnt[s] += (e >= wa[s] && e <= wb[s] && key_at<K>(c, k) < qe[s]) ? 1 : 0;
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-#pragma unroll
-                for (int o = G / 2; o > 0; o >>= 1) cnt[s] += __shfl_xor_sync(0xffffffffu, cnt[s], o);
-                const uint32_t width = wb[s] - wa[s] + 1;
-                // the lower bound is proven inside [wa, wb] unless the scan is
-                // empty with entries left of wa, or full with entries right of wb
-                const bool outside = ((uint32_t)cnt[s] == 0 && wa[s] > 0) ||
-                                     ((uint32_t)cnt[s] == width && wb[s] < (uint32_t)last);
-                sbad[s] = sbad[s] || outside;
-                node[s] = sbad[s] ? 0u : wa[s] + (uint32_t)cnt[s];
-                if (gl == 0) bad[r * (NG * I) + s * NG + grp] = sbad[s] ? 1 : 0;
-            }
-            for (int lvl = m.level + 1; lvl < t.nlevels; lvl++)
-                level_step<K, G, I>(static_cast<const K *>(t.seps) + t.lvl_off[lvl], qe, up, node,
-                                    grp, gl);
-            leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
-                const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                return (qi < nq && !sbad[s]) ? out + qi : nullptr;
-            });
-        }
-        __syncwarp();
-        // fallback: the owning lane runs the full descent for its own query
-        const bool mine_bad = my < nq && bad[lane] != 0;
-        if (mine_bad) {
-            const uint64_t p = scalar_lower_bound<K, V>(t, myqe);
-            const K k = leaf_key<K, V>(leaves, p);
-            const bool found = myq <= tmax && k == myq;
-            out[my] = found ? reinterpret_cast<const V *>(leaves + (p / LG::S) * LG::BS +
-                                                          kSectorBytes)[p % LG::S]
-                            : key_max<V>();
-        }
-        const unsigned fb = __ballot_sync(0xffffffffu, mine_bad);
-        const unsigned valid = __ballot_sync(0xffffffffu, my < nq);
-        n_fallback += __popc(fb);
-        n_window += __popc(valid & ~fb);
-        __syncwarp();
-    }
-    if (lane == 0 && m.stats) {
-        atomicAdd(&m.stats[0], n_window);
-        atomicAdd(&m.stats[1], n_fallback);
-    }
-}
-
-template <typename K, typename V, int G, int R>
-bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                         cudaStream_t s) {
-    auto fn = learned_kernel<K, V, G, R>;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) != cudaSuccess ||
-        per_sm < 1)
-        per_sm = 1;
-    uint64_t want = (nq + kThreads - 1) / kThreads;
-    const uint64_t cap = (uint64_t)sm_count() * per_sm;
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min(want, cap));
-    count_launch();
-    fn<<<grid, kThreads, 0, s>>>(t->dev, t->learned->dev, (const K *)d_q, nq, (V *)d_out);
-    BT_CUDA(cudaGetLastError());
-    return BT_OK;
-}
-
-template <typename K, typename V>
-bt_status learned_cfg(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out, cudaStream_t s) {
-    switch (t->search_cfg) {
-        case 0: return learned_launch<K, V, 8, 1>(t, d_q, nq, d_out, s);
-        case 1: return learned_launch<K, V, 8, 2>(t, d_q, nq, d_out, s);
-        case 2: return learned_launch<K, V, 4, 1>(t, d_q, nq, d_out, s);
-        case 3: return learned_launch<K, V, 4, 2>(t, d_q, nq, d_out, s);
-        default: return learned_launch<K, V, 2, 1>(t, d_q, nq, d_out, s);
-    }
-}
-
-// ------------------------------------------------------------ training ----
-
-struct DevBuf {
-    void *p = nullptr;
-    ~DevBuf() {
-        if (p) cudaFree(p);
-    }
-};
-
-unsigned grid_of(uint64_t n, int block, int per_sm = 8) {
-    uint64_t g = (n + block - 1) / block;
-    const uint64_t cap = (uint64_t)sm_count() * per_sm;
-    return (unsigned)std::max<uint64_t>(1, std::min(g, cap));
-}
-
 template <typename K, typename V>
 bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
                      bt_learned_report *rep) {
+    using LG = LeafGeom<K, V>;
     const uint64_t n = t->n;
     const int H = (int)cfg.hidden;
     const int np = 3 * H + 1;
-    const uint32_t nseg = cfg.num_segments;
+    const uint32_t kpu = (uint32_t)unit_keys<K, V>();
+    const uint64_t units = (n + kpu - 1) / kpu;
     const unsigned char *leaves = (const unsigned char *)t->d_leaves;
-    // frees the new state on every early return; released on success
     struct Owner {
         LearnedState *p;
         ~Owner() { free_learned(p); }
     } own{new LearnedState()};
     LearnedState *st = own.p;
     cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    cudaEventRecord(e0, s);
+    BT_CUDA(cudaEventCreate(&e0));
+    BT_CUDA(cudaEventCreate(&e1));
+    struct Ev {
+        cudaEvent_t a, b;
+        ~Ev() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evs{e0, e1};
+    BT_CUDA(cudaEventRecord(e0, s));
 
-    // normalisation of the root's input
+    // ---- segmentation: the bound, then the segments
+    const uint64_t nchunks = (n + kPlaChunk - 1) / kPlaChunk;
+    DevBuf bcnt, boff, btot;
+    BT_CUDA(cudaMalloc(&bcnt.p, nchunks * sizeof(uint64_t)));
+    BT_CUDA(cudaMalloc(&boff.p, nchunks * sizeof(uint64_t)));
+    BT_CUDA(cudaMalloc(&btot.p, sizeof(uint64_t)));
+    uint64_t *cnt = (uint64_t *)bcnt.p, *off = (uint64_t *)boff.p, *tot = (uint64_t *)btot.p;
+    const unsigned pg = (unsigned)((nchunks + 63) / 64);
+    auto count_at = [&](uint32_t eps, uint64_t *total) -> bt_status {
+        count_launch();
+        pla_kernel<K, V, true><<<pg, 64, 0, s>>>(leaves, n, eps, nchunks, cnt, nullptr, nullptr,
+                                                 nullptr, nullptr);
+        BT_CUDA(cudaGetLastError());
+        bt_status r = launch_scan_u64(cnt, off, nchunks, tot, s);
+        if (r != BT_OK) return r;
+        BT_CUDA(cudaMemcpyAsync(total, tot, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        BT_CUDA(cudaStreamSynchronize(s));
+        return BT_OK;
+    };
+    uint32_t eps = cfg.max_error;
+    uint64_t nseg = 0;
+    bt_status r;
+    if (eps == 0) {
+        // the least bound whose segmentation has at most num_segments segments
+        uint32_t lo = 0, hi = 8;
+        for (;;) {
+            if ((r = count_at(hi, &nseg)) != BT_OK) return r;
+            if (nseg <= cfg.num_segments || hi >= (1u << 30)) break;
+            lo = hi;
+            hi *= 2;
+        }
+        while (hi - lo > 1) {
+            const uint32_t mid = lo + (hi - lo) / 2;
+            uint64_t c = 0;
+            if ((r = count_at(mid, &c)) != BT_OK) return r;
+            if (c <= cfg.num_segments) hi = mid;
+            else lo = mid;
+        }
+        eps = hi;
+    }
+    if ((r = count_at(eps, &nseg)) != BT_OK) return r;
+    const uint32_t nls = (uint32_t)((nseg + kSegPerLine - 1) / kSegPerLine);
+    const uint32_t row = 128;  // stage in whole bank rows (the swizzle permutes within rows)
+    const uint64_t stage_bytes = ((uint64_t)nls * sizeof(K) + row - 1) / row * row;
+    if (stage_bytes > kStageBudget)
+        return fail(BT_ERR_NOT_SUPPORTED,
+                    "the segmentation has " + std::to_string(nseg) +
+                        " segments; their lines' first keys exceed the search's shared memory "
+                        "(raise max_error or lower num_segments)");
+    DevBuf bst, bsl, bic;
+    BT_CUDA(cudaMalloc(&bst.p, nseg * sizeof(uint32_t)));
+    BT_CUDA(cudaMalloc(&bsl.p, nseg * sizeof(double)));
+    BT_CUDA(cudaMalloc(&bic.p, nseg * sizeof(double)));
+    count_launch();
+    pla_kernel<K, V, false><<<pg, 64, 0, s>>>(leaves, n, eps, nchunks, nullptr, off,
+                                              (uint32_t *)bst.p, (double *)bsl.p, (double *)bic.p);
+    BT_CUDA(cudaGetLastError());
+
+    // ---- segment lines and their exact bounds
+    BT_CUDA(cudaMalloc((void **)&st->d_seg, (size_t)nls * sizeof(SegLine)));
+    count_launch();
+    seg_fill_kernel<K, V><<<grid_of(nls, 256), 256, 0, s>>>(leaves, n, (uint32_t)nseg, nls,
+                                                           (const uint32_t *)bst.p,
+                                                           (const double *)bsl.p,
+                                                           (const double *)bic.p, st->d_seg);
+    count_launch();
+    seg_eps_kernel<K, V><<<grid_of(nseg * 32, 256), 256, 0, s>>>(leaves, (uint32_t)nseg, st->d_seg);
+    BT_CUDA(cudaGetLastError());
+
+    // ---- staged keys and the root's training pairs
     const uint64_t kmin = t->min_key;
     const double span = (double)(t->max_key - t->min_key);
     const float xscale = span > 0 ? (float)(1.0 / span) : 0.f;
-
-    // training sample
-    const uint64_t stride = std::max<uint64_t>(1, cfg.sample_stride ? cfg.sample_stride : n / (1u << 20));
-    const uint64_t m = (n + stride - 1) / stride;
-    DevBuf bx, by, bg, bm, bv, bl, brl;
-    BT_CUDA(cudaMalloc(&bx.p, m * sizeof(float)));
-    BT_CUDA(cudaMalloc(&by.p, m * sizeof(float)));
+    BT_CUDA(cudaMalloc(&st->d_stage, stage_bytes));
+    DevBuf bx, by, bg, bm, bv, berr;
+    BT_CUDA(cudaMalloc(&bx.p, nls * sizeof(float)));
+    BT_CUDA(cudaMalloc(&by.p, nls * sizeof(float)));
     BT_CUDA(cudaMalloc(&bg.p, (np + 1) * sizeof(float)));
     BT_CUDA(cudaMalloc(&bm.p, np * sizeof(float)));
     BT_CUDA(cudaMalloc(&bv.p, np * sizeof(float)));
-    BT_CUDA(cudaMalloc(&brl.p, (nseg + 1) * sizeof(uint32_t)));
+    BT_CUDA(cudaMalloc(&berr.p, 2 * sizeof(unsigned int)));
     BT_CUDA(cudaMalloc((void **)&st->d_mlp, np * sizeof(float)));
-    BT_CUDA(cudaMalloc((void **)&st->d_seg, nseg * sizeof(SegParam)));
     BT_CUDA(cudaMalloc((void **)&st->d_stats, 2 * sizeof(unsigned long long)));
     BT_CUDA(cudaMemsetAsync(st->d_stats, 0, 2 * sizeof(unsigned long long), s));
+    BT_CUDA(cudaMemsetAsync(berr.p, 0, 2 * sizeof(unsigned int), s));
     float *x = (float *)bx.p, *y = (float *)by.p, *grad = (float *)bg.p, *loss = grad + np;
+    unsigned int *err = (unsigned int *)berr.p;
     count_launch();
-    sample_kernel<K, V><<<grid_of(m, 256), 256, 0, s>>>(leaves, n, m, stride, kmin, xscale, x, y);
+    stage_kernel<K><<<grid_of(nls, 256), 256, 0, s>>>(st->d_seg, nls, kmin, xscale,
+                                                     (K *)st->d_stage, x, y);
 
-    // initial root: hinges spread over [0, 1), output weights 1/H
+    // ---- root: hinges spread over [0, 1), output weights 1/H, then Adam
     std::vector<float> p0(np);
     for (int j = 0; j < H; j++) {
         p0[j] = 1.f;
@@ -490,14 +882,16 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     }
     p0[3 * H] = 0.f;
     BT_CUDA(cudaMemcpyAsync(st->d_mlp, p0.data(), np * sizeof(float), cudaMemcpyHostToDevice, s));
+    count_launch();
+    root_err_kernel<<<grid_of(nls, 256, 4), 256, 0, s>>>(st->d_mlp, H, x, nls, err + 1);
     BT_CUDA(cudaMemsetAsync(bm.p, 0, np * sizeof(float), s));
     BT_CUDA(cudaMemsetAsync(bv.p, 0, np * sizeof(float), s));
     float l0 = 0.f, l1 = 0.f;
-    const unsigned lg = grid_of(m, 256, 4);
+    const unsigned lg = grid_of(nls, 256, 4);
     for (uint32_t it = 0; it <= cfg.iterations; it++) {
         BT_CUDA(cudaMemsetAsync(grad, 0, (np + 1) * sizeof(float), s));
         count_launch();
-        mlp_loss_grad_kernel<<<lg, 256, 0, s>>>(st->d_mlp, H, x, y, m, loss, grad);
+        mlp_loss_grad_kernel<<<lg, 256, 0, s>>>(st->d_mlp, H, x, y, nls, loss, grad);
         if (it == 0) BT_CUDA(cudaMemcpyAsync(&l0, loss, sizeof(float), cudaMemcpyDeviceToHost, s));
         if (it == cfg.iterations) {
             BT_CUDA(cudaMemcpyAsync(&l1, loss, sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -507,61 +901,69 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
         adam_kernel<<<1, 128, 0, s>>>(st->d_mlp, grad, (float *)bm.p, (float *)bv.p, H,
                                       cfg.learning_rate, (int)it + 1);
     }
+    count_launch();
+    root_err_kernel<<<grid_of(nls, 256, 4), 256, 0, s>>>(st->d_mlp, H, x, nls, err);
 
-    // segments: assignment, least-squares fit, exact error bounds
-    uint32_t *r_lo = (uint32_t *)brl.p;
-    count_launch();
-    assign_kernel<K, V><<<grid_of(n, 256), 256, 0, s>>>(leaves, n, st->d_mlp, H, nseg, kmin, xscale,
-                                                      r_lo);
-    count_launch();
-    fit_kernel<K, V><<<grid_of((uint64_t)nseg * 32, 256), 256, 0, s>>>(leaves, n, nseg, r_lo,
-                                                                     st->d_seg);
+    // ---- unit thresholds
+    const uint64_t ncl = units > 1 ? (units - 1 + kCodesPerLine - 1) / kCodesPerLine : 0;
+    BT_CUDA(cudaMalloc((void **)&st->d_codes, std::max<uint64_t>(1, ncl) * sizeof(CodeLine)));
+    if (ncl) {
+        count_launch();
+        code_kernel<K, V><<<grid_of(ncl, 256), 256, 0, s>>>(leaves, n, units, ncl, st->d_codes);
+    }
     BT_CUDA(cudaGetLastError());
-    cudaEventRecord(e1, s);
-    std::vector<SegParam> segs(nseg);
-    BT_CUDA(cudaMemcpyAsync(segs.data(), st->d_seg, nseg * sizeof(SegParam), cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaEventRecord(e1, s));
+    unsigned int herr[2] = {0, 0};
+    std::vector<SegLine> segs(nls);
+    BT_CUDA(cudaMemcpyAsync(herr, err, sizeof(herr), cudaMemcpyDeviceToHost, s));
+    BT_CUDA(cudaMemcpyAsync(segs.data(), st->d_seg, nls * sizeof(SegLine), cudaMemcpyDeviceToHost, s));
     BT_CUDA(cudaStreamSynchronize(s));
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
 
     LearnedDev &d = st->dev;
     d.mlp = st->d_mlp;
     d.seg = st->d_seg;
+    d.codes = st->d_codes;
+    d.stage = st->d_stage;
     d.stats = st->d_stats;
     d.kmin = kmin;
     d.xscale = xscale;
     d.hidden = H;
-    d.nseg = nseg;
-    d.level = t->dev.nlevels >= 2 ? t->dev.nlevels - 2 : 0;
-    uint64_t kpe = LeafGeom<K, V>::S;
-    for (int l = t->dev.nlevels - 1; l > d.level; l--) kpe *= (uint64_t)(kLineBytes / sizeof(K));
-    d.kpe = kpe;
-    d.level_entries = t->lvl_entries[d.level];
+    d.nseg = (uint32_t)nseg;
+    d.nls = nls;
+    d.root_err = herr[0];
+    d.kpu = kpu;
+    d.units = units;
+    d.stage_bytes = (uint32_t)stage_bytes;
+    st->bytes = (uint64_t)nls * sizeof(SegLine) + ncl * sizeof(CodeLine) + stage_bytes +
+                np * sizeof(float);
+    (void)LG::S;
 
     if (rep) {
         std::memset(rep, 0, sizeof(*rep));
         rep->root_loss_initial = l0;
         rep->root_loss_final = l1;
-        rep->num_segments = nseg;
-        rep->model_level = (uint32_t)d.level;
-        rep->keys_per_entry = kpe;
+        rep->root_error = herr[0];
+        rep->root_error_initial = herr[1];
+        rep->num_segments = (uint32_t)nseg;
+        rep->max_error = eps;
         double esum = 0, lsum = 0;
-        uint64_t emax = 0, used = 0;
-        const int F = kLineBytes / (int)sizeof(K);
-        for (uint32_t i = 0; i < nseg; i++) {
-            const uint64_t cnt = (i + 1 < nseg ? segs[i + 1].r_lo : n) - segs[i].r_lo;
-            if (!cnt) continue;
-            used++;
-            esum += segs[i].eps;
-            emax = std::max<uint64_t>(emax, segs[i].eps);
-            const double width_entries = (2.0 * segs[i].eps + 4.0) / (double)kpe + 3.0;
-            lsum += std::ceil(width_entries / F);
+        uint64_t emax = 0;
+        for (uint64_t g = 0; g < nseg; g++) {
+            const SegLine &sl = segs[g / kSegPerLine];
+            const int k = (int)(g % kSegPerLine);
+            esum += sl.eps[k];
+            emax = std::max<uint64_t>(emax, sl.eps[k]);
+            // window of 2 eps + 3 ranks: units it spans, then code lines
+            const double win_units = (2.0 * sl.eps[k] + 3.0) / kpu + 1.0;
+            lsum += (double)sl.cnt[k] * (1.0 + (win_units - 1.0) / kCodesPerLine);
         }
-        rep->eps_mean = used ? esum / used : 0;
+        rep->eps_mean = nseg ? esum / (double)nseg : 0;
         rep->eps_max = emax;
-        rep->window_lines_mean = used ? lsum / used : 0;
+        rep->code_lines_mean = n ? lsum / (double)n : 0;
+        rep->index_bytes = st->bytes;
+        rep->keys_per_unit = kpu;
         rep->train_ms = ms;
     }
     if (t->learned) free_learned(t->learned);
@@ -581,16 +983,16 @@ bt_status bt_learned_train(bt_tree *t, const bt_learned_config *cfg_in, void *st
     if (!t) return fail(BT_ERR_INVALID_ARGUMENT, "tree is NULL");
     if (t->n < 2) return fail(BT_ERR_INVALID_ARGUMENT, "a learned index needs at least 2 keys");
     if (t->n >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "learned index supports n < 2^32");
-    bt_learned_config cfg = {65536, 16, 400, 0, 0.01f};
+    bt_learned_config cfg = {65536, 0, 16, 400, 0.01f};
     if (cfg_in) {
         if (cfg_in->num_segments) cfg.num_segments = cfg_in->num_segments;
+        cfg.max_error = cfg_in->max_error;
         if (cfg_in->hidden) cfg.hidden = cfg_in->hidden;
         cfg.iterations = cfg_in->iterations;
-        cfg.sample_stride = cfg_in->sample_stride;
         if (cfg_in->learning_rate > 0) cfg.learning_rate = cfg_in->learning_rate;
     }
     if (cfg.hidden > (uint32_t)kMaxHidden) return fail(BT_ERR_INVALID_ARGUMENT, "hidden must be <= 32");
-    if (cfg.num_segments > (1u << 24)) return fail(BT_ERR_INVALID_ARGUMENT, "too many segments");
+    if (cfg.max_error > (1u << 30)) return fail(BT_ERR_INVALID_ARGUMENT, "max_error too large");
     int prev = 0;
     BT_CUDA(cudaGetDevice(&prev));
     if (prev != t->device) BT_CUDA(cudaSetDevice(t->device));
@@ -623,22 +1025,22 @@ bt_status bt_point_search_learned(const bt_tree *t, const void *d_q, uint64_t nq
     if (e != cudaSuccess) st = cuda_fail(e, "cudaMemsetAsync");
     if (st == BT_OK) {
         if (t->key_bytes == 4)
-            st = t->val_bytes == 4 ? learned_cfg<uint32_t, uint32_t>(t, d_q, nq, d_out, s)
-                                   : learned_cfg<uint32_t, uint64_t>(t, d_q, nq, d_out, s);
+            st = t->val_bytes == 4 ? learned_launch<uint32_t, uint32_t>(t, d_q, nq, d_out, s)
+                                   : learned_launch<uint32_t, uint64_t>(t, d_q, nq, d_out, s);
         else
-            st = t->val_bytes == 4 ? learned_cfg<uint64_t, uint32_t>(t, d_q, nq, d_out, s)
-                                   : learned_cfg<uint64_t, uint64_t>(t, d_q, nq, d_out, s);
+            st = t->val_bytes == 4 ? learned_launch<uint64_t, uint32_t>(t, d_q, nq, d_out, s)
+                                   : learned_launch<uint64_t, uint64_t>(t, d_q, nq, d_out, s);
     }
     if (prev != t->device) cudaSetDevice(prev);
     return st;
 }
 
-bt_status bt_learned_last_stats(const bt_tree *t, uint64_t *windowed, uint64_t *fallback) {
+bt_status bt_learned_last_stats(const bt_tree *t, uint64_t *extra, uint64_t *fallback) {
     using namespace bt;
     if (!t || !t->learned) return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
     unsigned long long h[2] = {0, 0};
     BT_CUDA(cudaMemcpy(h, t->learned->d_stats, sizeof(h), cudaMemcpyDeviceToHost));
-    if (windowed) *windowed = h[0];
+    if (extra) *extra = h[0];
     if (fallback) *fallback = h[1];
     return BT_OK;
 }

@@ -256,56 +256,75 @@ BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *
  * BPTreeExactSearch.cu:39-68) ------------------------------------------ */
 
 /*
- * A two-stage FP32 model over the tree's (key, rank) pairs:
- *  - root: a monotone MLP x -> y (1 input, `hidden` ReLU units, 1 output;
- *    input weights and output weights kept >= 0), x the key normalised to
- *    [0, 1], y the rank normalised to [0, 1); it routes a key to one of
- *    `num_segments` leaf models (segment = floor(y * num_segments)).  Trained
- *    on the GPU by full-batch gradient descent (Adam) on MSE with this
- *    library's own forward/backward kernels, on every `sample_stride`-th key;
- *  - leaves: per segment, rank = segment's first rank + intercept + slope *
- *    (key - segment's first key), fitted by least squares on the GPU; its max
- *    error eps over the segment's keys is computed exactly with the same FP32
- *    arithmetic the search uses.
- * The search predicts a rank window and scans it on the separator level one
- * above the bottom (one separator per leaf node), then descends normally;
- * a query whose lower bound is not provably inside the window takes the
- * full tree descent, so results never depend on the model (the tree stays
- * both the fallback and the source of truth).
+ * A learned index over the tree's sorted (key, rank) pairs that sends each
+ * point query to the one 128-byte piece of the leaf array ("leaf unit")
+ * holding its key, with the upper separator levels replaced by a model small
+ * enough to stay on chip:
+ *  - leaf models: an error-bounded piecewise-linear segmentation of
+ *    (key, rank) -- greedy maximal segments, each with a line within
+ *    `max_error` ranks of all its keys (the optimal streaming fit of
+ *    O'Rourke 1981, the segmentation of the PGM-index, Ferragina &
+ *    Vinciguerra 2020), computed on the GPU; a segment's bound eps is then
+ *    re-measured with the exact FP32 arithmetic of the search;
+ *  - root: a monotone MLP (1 input, `hidden` ReLU units, 1 output; input and
+ *    output weights kept >= 0) from the normalised key to the position of
+ *    the key's segment among the segment lines (4 segments per 128-byte
+ *    line), trained on the GPU by full-batch Adam with this library's own
+ *    forward/backward kernels; its worst error over the lines' first keys
+ *    bounds a shared-memory search over those keys;
+ *  - unit thresholds: one 16-bit code per leaf-unit boundary (59 per
+ *    128-byte line with a 64-bit base and a shift), an exact separator
+ *    between the units' key ranges.
+ * A query: the root and a short shared-memory search give the segment line
+ * (one L2 read), the segment's line and eps a window of ranks, the window's
+ * codes (one or two L2 lines) the leaf unit, which is the only DRAM read.
+ * A query whose key lies past the unit's last key reads the next unit; one
+ * that leaves the window takes the tree's full descent: results are always
+ * the plain search's.
  */
 typedef struct bt_learned_config {
-    uint32_t num_segments;  /* leaf models (default 65536) */
+    uint32_t num_segments;  /* target segment count: max_error is raised until
+                               the segmentation needs at most this many (default 65536) */
+    uint32_t max_error;     /* segmentation bound in ranks; 0 = chosen from num_segments.
+                               When set, num_segments is ignored */
     uint32_t hidden;        /* root hidden units, 1..32 (default 16) */
     uint32_t iterations;    /* root training steps (default 400) */
-    uint32_t sample_stride; /* train the root on every k-th key (default: n / 2^20) */
     float learning_rate;    /* Adam step size (default 0.01) */
 } bt_learned_config;
 
 typedef struct bt_learned_report {
     float root_loss_initial;  /* MSE of the root before training */
     float root_loss_final;    /* ... and after */
-    uint32_t num_segments;
-    uint32_t model_level;     /* separator level the window is scanned on */
-    uint64_t keys_per_entry;  /* keys under one separator of that level */
-    double eps_mean;          /* mean segment error bound, in keys */
-    uint64_t eps_max;
-    double window_lines_mean; /* mean 128-byte lines a window spans */
-    double train_ms;          /* device time of the whole training */
+    uint32_t root_error;      /* root's worst line-position error after training */
+    uint32_t root_error_initial; /* ... and of the untrained root */
+    uint32_t num_segments;    /* segments of the segmentation */
+    uint32_t max_error;       /* the segmentation's bound */
+    uint64_t eps_max;         /* largest measured segment bound (FP32 search arithmetic) */
+    double eps_mean;          /* mean measured segment bound */
+    double code_lines_mean;   /* mean code lines a query's window spans (over the keys) */
+    uint64_t index_bytes;     /* device bytes of the model, segment lines and codes */
+    uint32_t keys_per_unit;   /* keys in one 128-byte leaf unit */
+    uint32_t pad;
+    double train_ms;          /* device time of the whole build */
 } bt_learned_report;
 
-/* Train the model for `tree` (replacing a previous one).  cfg may be NULL
- * for defaults; report may be NULL.  Synchronizes `stream`. */
+/* Build the learned index of `tree` (replacing a previous one).  cfg may be
+ * NULL for defaults; report may be NULL.  BT_ERR_NOT_SUPPORTED when the
+ * segment lines' first keys do not fit the search's shared memory (more than
+ * about 2^16 segments for u64 keys: raise max_error).  Synchronizes `stream`. */
 BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, void *stream,
                                   bt_learned_report *report);
 
-/* Point search through the learned model (same results as bt_point_search).
- * BT_ERR_INVALID_ARGUMENT if the tree has no trained model. */
+/* Point search through the learned index (same results as bt_point_search).
+ * BT_ERR_INVALID_ARGUMENT if the tree has no trained index. */
 BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
                                          void *d_out, void *stream);
 
-/* Counters of the last learned search on this tree: queries answered through
- * the window and queries that took the full descent. */
-BT_API bt_status bt_learned_last_stats(const bt_tree *tree, uint64_t *windowed, uint64_t *fallback);
+/* Counters of the last learned search on this tree: leaf units read beyond
+ * the first one (keys just past a unit's threshold) and queries that took
+ * the full tree descent. */
+BT_API bt_status bt_learned_last_stats(const bt_tree *tree, uint64_t *extra_unit_reads,
+                                       uint64_t *fallback);
 
 /*
  * The root model's training kernels, exposed so their gradients can be
@@ -412,16 +431,6 @@ BT_API bt_status bt_server_replay(bt_server *srv, uint64_t nreq, const uint64_t 
 /* Number of kernel launches this library has issued in this process (all
  * devices, all threads).  Lets a caller count the device work behind a call. */
 BT_API uint64_t bt_kernel_launches(void);
-
-/* Measurement aid (no counterpart in the reference): reads n_reads blocks of
- * block_bytes (32, 64 or 128) at uniformly random aligned addresses of a
- * region_bytes buffer on the current device, 16 bytes per lane, L1 bypassed
- * and L2 flushed first, and returns the best of three timed runs in random
- * reads per second.  A point search that misses the cache makes one such read
- * per query, so this is the ceiling its throughput is set against.  Allocates
- * and frees its own buffers; synchronous. */
-BT_API bt_status bt_measure_gather(uint64_t region_bytes, uint64_t n_reads, uint32_t block_bytes,
-                                   double *reads_per_s);
 
 #ifdef __cplusplus
 }

@@ -520,3 +520,121 @@ int refc_zorder_interval(uint64_t max_value) {
     if ((float)c < f) c++;
     return c;
 }
+
+/* ---- error-bounded segmentation (learned index) ------------------------ */
+
+/* Points of a segment, relative to its first point: x = key - key[s] (exact
+ * in 64 bits), y = rank - s +/- eps. */
+typedef struct {
+    uint64_t x;
+    int64_t y;
+} pla_pt;
+
+/* Orientation of (o, a, b): > 0 when b lies above the directed line o -> a
+ * (x increasing).  Exact: 128-bit products of 64-bit x and 34-bit y spans. */
+static inline __int128 pla_cross(pla_pt o, pla_pt a, pla_pt b) {
+    __int128 ax = (__int128)a.x - (__int128)o.x, bx = (__int128)b.x - (__int128)o.x;
+    __int128 ay = (__int128)a.y - (__int128)o.y, by = (__int128)b.y - (__int128)o.y;
+    return ax * by - ay * bx;
+}
+
+static inline double pla_line_at0(pla_pt a, pla_pt b, double *slope) {
+    /* the line through a and b: slope and value at x = 0 (no contraction:
+     * the file is built with -ffp-contract=off) */
+    if (b.x == a.x) { /* duplicate keys: a flat line through the middle */
+        *slope = 0.0;
+        return ((double)a.y + (double)b.y) * 0.5;
+    }
+    double dx = (double)(b.x - a.x);
+    double s = ((double)b.y - (double)a.y) / dx;
+    *slope = s;
+    return (double)a.y - s * (double)a.x;
+}
+
+uint64_t orc_pla_segments(const void *keys, uint64_t n, int key_bytes, uint32_t eps,
+                          uint64_t chunk, int hull_cap, uint64_t *starts, double *slopes,
+                          double *icpts, uint64_t max_out) {
+    /* Greedy maximal segments with the optimal streaming fit (O'Rourke,
+     * "An on-line algorithm for fitting straight lines between data ranges",
+     * CACM 1981; the segmentation of the PGM-index, Ferragina & Vinciguerra,
+     * VLDB 2020).  State of an open segment: the upper convex hull of the
+     * lower points (x, y - eps), the lower convex hull of the upper points
+     * (x, y + eps), the feasible line of largest slope M = (Ma, Mb) and of
+     * smallest slope N = (Na, Nb).  A new point is feasible iff its lower
+     * point is not above M and its upper point not below N. */
+    if (hull_cap < 2) hull_cap = 2;
+    pla_pt *lh = (pla_pt *)malloc(sizeof(pla_pt) * (size_t)hull_cap);
+    pla_pt *uh = (pla_pt *)malloc(sizeof(pla_pt) * (size_t)hull_cap);
+    const int64_t e = (int64_t)eps;
+    uint64_t nseg = 0, i = 0;
+    while (i < n) {
+        const uint64_t s = i;
+        uint64_t end = n;
+        if (chunk) {
+            const uint64_t ce = (s / chunk + 1) * chunk;
+            if (ce < end) end = ce;
+        }
+        const uint64_t x0 = key_at(keys, key_bytes, s);
+        int nl = 1, nu = 1;
+        lh[0] = (pla_pt){0, -e};
+        uh[0] = (pla_pt){0, e};
+        pla_pt Ma = lh[0], Mb = uh[0], Na = uh[0], Nb = lh[0];
+        uint64_t j = s + 1;
+        if (j < end) {
+            const pla_pt L = {key_at(keys, key_bytes, j) - x0, 1 - e};
+            const pla_pt U = {L.x, 1 + e};
+            Ma = lh[0];
+            Mb = U;
+            Na = uh[0];
+            Nb = L;
+            lh[nl++] = L;
+            uh[nu++] = U;
+            for (j = s + 2; j < end; j++) {
+                const int64_t y = (int64_t)(j - s);
+                const pla_pt L2 = {key_at(keys, key_bytes, j) - x0, y - e};
+                const pla_pt U2 = {L2.x, y + e};
+                if (pla_cross(Ma, Mb, L2) > 0 || pla_cross(Na, Nb, U2) < 0) break;
+                int nl2 = nl, nu2 = nu;
+                while (nl2 >= 2 && pla_cross(lh[nl2 - 2], lh[nl2 - 1], L2) >= 0) nl2--;
+                while (nu2 >= 2 && pla_cross(uh[nu2 - 2], uh[nu2 - 1], U2) <= 0) nu2--;
+                if (nl2 >= hull_cap || nu2 >= hull_cap) break;
+                if (pla_cross(Ma, Mb, U2) < 0) { /* M pivots on U2: the lower point of least slope to it */
+                    int b = 0;
+                    for (int t = 1; t < nl; t++)
+                        if (pla_cross(lh[b], U2, lh[t]) > 0) b = t;
+                    Ma = lh[b];
+                    Mb = U2;
+                }
+                if (pla_cross(Na, Nb, L2) > 0) { /* N pivots on L2: the upper point of most slope to it */
+                    int b = 0;
+                    for (int t = 1; t < nu; t++)
+                        if (pla_cross(uh[b], L2, uh[t]) < 0) b = t;
+                    Na = uh[b];
+                    Nb = L2;
+                }
+                lh[nl2] = L2;
+                nl = nl2 + 1;
+                uh[nu2] = U2;
+                nu = nu2 + 1;
+            }
+        }
+        if (nseg < max_out) {
+            if (starts) starts[nseg] = s;
+            double sl = 0.0, ic = 0.0;
+            if (j - s >= 2) {
+                double sm, sn;
+                const double m0 = pla_line_at0(Ma, Mb, &sm);
+                const double n0 = pla_line_at0(Na, Nb, &sn);
+                sl = (sm + sn) * 0.5;
+                ic = (m0 + n0) * 0.5;
+            }
+            if (slopes) slopes[nseg] = sl;
+            if (icpts) icpts[nseg] = ic;
+        }
+        nseg++;
+        i = j;
+    }
+    free(lh);
+    free(uh);
+    return nseg;
+}

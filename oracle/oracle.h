@@ -70,6 +70,21 @@ int orc_rect_search(const uint32_t *z_sorted, const uint32_t *ids_sorted, uint64
 /* 32-bit Morton interleave of (x, y): x in even bits, y in odd bits. */
 uint32_t orc_morton2_u16(uint16_t x, uint16_t y);
 
+/* Error-bounded piecewise-linear segmentation of the points (key[i], i),
+ * i in [0, n) (keys ascending and unique, key_bytes 4 or 8): greedy maximal
+ * segments, each admitting a line within eps of all its points (the optimal
+ * streaming fit of O'Rourke 1981 as in the PGM-index, Ferragina &
+ * Vinciguerra 2020).  A segment never crosses a multiple of `chunk` (0: no
+ * limit) and is closed when either convex hull would exceed hull_cap
+ * points.  For the first max_out segments writes the start index and, when
+ * non-NULL, the line rank - start = icpt + slope * (key - key[start]): the
+ * mean of the steepest and the flattest feasible line (slope 0, icpt 0 for
+ * a one-point segment).  Returns the number of segments.  Restates the
+ * engine's GPU segmentation (its chunking and hull cap included). */
+uint64_t orc_pla_segments(const void *keys, uint64_t n, int key_bytes, uint32_t eps,
+                          uint64_t chunk, int hull_cap, uint64_t *starts, double *slopes,
+                          double *icpts, uint64_t max_out);
+
 /* ---- literal restatement of the reference ------------------------------ */
 
 #define REFC_PAGESIZE 5000

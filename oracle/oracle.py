@@ -48,6 +48,8 @@ class Oracle:
             "orc_bounds": (_I, [_P, _U64, _I, _P, _U64, _I, _P, _I]),
             "orc_rect_search": (_I, [_P, _P, _U64, _P, _P, _P, _P, _U64, _P, _P, _P, _I]),
             "orc_morton2_u16": (ctypes.c_uint32, [ctypes.c_uint16, ctypes.c_uint16]),
+            "orc_pla_segments": (_U64, [_P, _U64, _I, ctypes.c_uint32, _U64, _I, _P, _P, _P,
+                                        _U64]),
             "refc_build": (_P, [_P, _P, _U64, _P, _U64]),
             "refc_free": (None, [_P]),
             "refc_root": (_U64, [_P]),
@@ -121,6 +123,23 @@ class Oracle:
                                       _p(x1), _p(y1), nq, _p(c2), _p(offsets), _p(ids),
                                       nthreads) == 0
         return counts, offsets, ids
+
+    def pla_segments(self, keys, eps, chunk=0, hull_cap=1 << 30, lines=True):
+        """Error-bounded segmentation of (keys[i], i): (starts, slopes, icpts),
+        or the segment count alone with lines=False (orc_pla_segments)."""
+        keys = np.ascontiguousarray(keys)
+        kb = keys.dtype.itemsize
+        cap = min(hull_cap, len(keys) + 2)
+        if not lines:
+            return int(self.L.orc_pla_segments(_p(keys), len(keys), kb, eps, chunk, cap, None,
+                                               None, None, 0))
+        m = int(self.L.orc_pla_segments(_p(keys), len(keys), kb, eps, chunk, cap, None, None,
+                                        None, 0))
+        st = np.empty(m, dtype=np.uint64)
+        sl = np.empty(m, dtype=np.float64)
+        ic = np.empty(m, dtype=np.float64)
+        self.L.orc_pla_segments(_p(keys), len(keys), kb, eps, chunk, cap, _p(st), _p(sl), _p(ic), m)
+        return st, sl, ic
 
     def morton(self, x, y):
         return self.L.orc_morton2_u16(int(x), int(y))

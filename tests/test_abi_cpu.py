@@ -76,6 +76,14 @@ def test_reference_mangling_matches_reference_build():
         assert name in out
 
 
+def test_probe_library_is_separate(bt, lib):
+    """The benchmark's probes live in their own library, not in the engine."""
+    assert not hasattr(lib, "bt_measure_gather")
+    if os.path.exists(bt.PROBE_LIB_PATH):
+        p = bt.probe_lib()
+        assert hasattr(p, "btp_measure_gather") and hasattr(p, "btp_measure_chain")
+
+
 def test_version_and_status_strings(lib):
     assert lib.bt_version() == 10000
     assert lib.bt_status_string(0) == b"ok"

@@ -1,4 +1,5 @@
-"""The random-gather probe that bench.py sets the search kernels against."""
+"""The memory-system probes that bench.py sets the search kernels against
+(lib/libbt_probe.so, a separate library the engine does not link)."""
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -11,3 +12,13 @@ def test_gather_probe_measures_and_checks_arguments(bt, cuda):
         bt.measure_gather(64 << 20, 1 << 20, 48)
     with pytest.raises(bt.BTreeError):
         bt.measure_gather(0, 1 << 20, 64)
+
+
+def test_chain_probe_measures_and_checks_arguments(bt, cuda):
+    for lines in (0, 1, 2):
+        r = bt.measure_chain(8 << 20, 256 << 20, 1 << 20, 128, lines, 2)
+        assert 1e8 < r < 1e12
+    with pytest.raises(bt.BTreeError):
+        bt.measure_chain(8 << 20, 256 << 20, 1 << 20, 96, 1, 2)
+    with pytest.raises(bt.BTreeError):
+        bt.measure_chain(8 << 20, 256 << 20, 1 << 20, 128, 3, 2)
