@@ -23,7 +23,7 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "lib", "libbtree_b200.so")
 
-POINT_MODES = {"basic": 0, "grouped": 1}
+POINT_MODES = {"basic": 0, "grouped": 1, "learned": 2}
 RANGE_MODES = {"basic": 0, "2d": 1, "zorder": 2}
 
 STATUS = {
@@ -110,6 +110,8 @@ _PROTOS = {
     "bt_range_count_host": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
     "bt_point_search_grouped_batch": (_I, [_P, _P, _P, _U64, _P, _P]),
     "bt_kernel_launches": (ctypes.c_uint64, []),
+    "bt_workspace_allocations": (ctypes.c_uint64, []),
+    "bt_partition_lookback_timeouts": (ctypes.c_uint64, []),
     "bt_sort_pairs": (_I, [_P, _P, _U64, _I, _I, _P, _P, _P]),
     "bt_build_unsorted": (_I, [_P, _P, _U64, _I, _I, _P, ctypes.POINTER(_P)]),
     "bt_save": (_I, [_P, ctypes.c_char_p]),

@@ -84,3 +84,63 @@ def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, confi
         with open(cache_path, "w") as f:
             json.dump(data, f, indent=1, sort_keys=True)
     return g, i, ms
+
+
+FOREST_SHAPES = ((4, 1), (8, 1), (8, 2))
+FOREST_TILES = (512, 2048, 8192)
+
+
+def _forest_key(forest, nq, nr):
+    return (f"forest_t{forest.num_trees}_k{forest.key_bytes}_v{forest.value_bytes}"
+            f"_q2^{max(0, int(nq).bit_length() - 1)}_r2^{max(0, int(nr).bit_length() - 1)}")
+
+
+def tune_forest(forest, queries, q_offsets, out, lo=None, hi=None, r_offsets=None, counts=None,
+                shapes=FOREST_SHAPES, tiles=FOREST_TILES, repeats=3, flush=None,
+                cache_path=None):
+    """Pick the forest search plan's (lanes per query, rounds, tile) for this
+    batch: every candidate is planned (one captured CUDA-graph launch) and
+    timed with CUDA events (an L2 flush before each timed launch when
+    `flush`, a CUDA tensor, is given).  Returns (lanes, rounds, tile, {name:
+    ms}); with cache_path the decision is stored and reused per forest and
+    batch shape."""
+    import torch
+    key = _forest_key(forest, len(queries), 0 if lo is None else len(lo))
+    if cache_path and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            cached = json.load(f).get(key)
+        if cached:
+            lanes, rounds, tile = cached["best"]
+            return lanes, rounds, tile, cached["ms"]
+    stream = torch.cuda.current_stream(queries.device)
+    ms = {}
+    for lanes, rounds in shapes:
+        for tile in tiles:
+            with forest.plan(queries, q_offsets, out, lo, hi, r_offsets, counts, lanes, rounds,
+                             tile=tile) as p:
+                p.run(stream)
+                ts = []
+                for _ in range(repeats):
+                    if flush is not None:
+                        flush.zero_()
+                    a = torch.cuda.Event(enable_timing=True)
+                    b = torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    p.run(stream)
+                    b.record(stream)
+                    b.synchronize()
+                    ts.append(a.elapsed_time(b))
+                ms[f"{lanes}x{rounds}/t{tile}"] = statistics.median(ts)
+    best = min(ms, key=ms.get)
+    lanes, rounds = (int(x) for x in best.split("/")[0].split("x"))
+    tile = int(best.split("/t")[1])
+    if cache_path:
+        data = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                data = json.load(f)
+        data[key] = {"best": [lanes, rounds, tile], "ms": ms}
+        os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
+        with open(cache_path, "w") as f:
+            json.dump(data, f, indent=1, sort_keys=True)
+    return lanes, rounds, tile, ms

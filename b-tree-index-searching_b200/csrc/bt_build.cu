@@ -44,6 +44,12 @@ copy_pad_kernel(const K *__restrict__ keys, const V *__restrict__ vals, uint64_t
         unsigned char *blk = leaves + b * LG::BS;
         reinterpret_cast<K *>(blk)[j] = k;
         reinterpret_cast<V *>(blk + kSectorBytes)[j] = v;
+        if constexpr (kSectorBytes + LG::VB < LG::BS) {
+            // the block's padding after its values (zero, so tree images are
+            // deterministic)
+            constexpr int PW = (LG::BS - kSectorBytes - LG::VB) / 4;
+            if (j < PW) reinterpret_cast<uint32_t *>(blk + kSectorBytes + LG::VB)[j] = 0u;
+        }
         if (j == LG::S - 1) bottom_sep[b] = k;
     }
     unsigned int w = __reduce_or_sync(0xffffffffu, f);
@@ -109,7 +115,6 @@ bt_status build_impl(bt_tree *t, const void *d_keys, const void *d_vals, cudaStr
 
     const size_t leaf_bytes = t->n_sectors * (size_t)LeafGeom<K, V>::BS;
     BT_CUDA(cudaMalloc(&t->d_leaves, leaf_bytes));
-    BT_CUDA(cudaMemsetAsync(t->d_leaves, 0, leaf_bytes, s));  // block padding bytes
     BT_CUDA(cudaMalloc(&t->d_seps, t->seps_elems * sizeof(K)));
     WsGuard g_flags(s);
     bt_status st = g_flags.alloc(sizeof(unsigned int));

@@ -56,6 +56,7 @@ bt_status pipe_streams(int dev, cudaStream_t (&out)[kPipeSlots]) {
 bt_status point_device(const bt_tree *t, int mode, const void *d_q, uint64_t nq, void *d_out,
                        cudaStream_t s) {
     if (mode == BT_POINT_BASIC || t->n == 0) return launch_point_search(t, d_q, nullptr, nq, d_out, s);
+    if (mode == BT_POINT_LEARNED) return launch_learned_search(t, d_q, nq, d_out, s);
     void *gq = nullptr;
     uint32_t *perm = nullptr;
     bt_status st = ws_alloc(&gq, nq * t->key_bytes, s);
@@ -85,7 +86,9 @@ bt_status count_device(const bt_tree *t, int mode, const void *d_lo, const void 
     return st;
 }
 
-bool valid_point_mode(int m) { return m == BT_POINT_BASIC || m == BT_POINT_GROUPED; }
+bool valid_point_mode(int m) {
+    return m == BT_POINT_BASIC || m == BT_POINT_GROUPED || m == BT_POINT_LEARNED;
+}
 bool valid_range_mode(int m) {
     return m == BT_RANGE_BASIC || m == BT_RANGE_GROUPED_2D || m == BT_RANGE_ZORDER;
 }
@@ -161,10 +164,16 @@ bt_status bt_point_search(const bt_tree *t, int mode, const void *d_queries, uin
     bt_status st = check_tree(t);
     if (st != BT_OK) return st;
     if (!valid_point_mode(mode)) return fail(BT_ERR_INVALID_ARGUMENT, "unknown point mode");
+    if (mode == BT_POINT_LEARNED && !t->learned)
+        return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
     if (nq == 0) return BT_OK;
     if (!d_queries || !d_out) return fail(BT_ERR_INVALID_ARGUMENT, "queries or out is NULL");
     if (nq >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "nq must be below 2^32");
     DeviceGuard g(t->device);
+    if (mode == BT_POINT_LEARNED) {
+        st = reset_learned_stats(t, (cudaStream_t)stream);
+        if (st != BT_OK) return st;
+    }
     return point_device(t, mode, d_queries, nq, d_out, (cudaStream_t)stream);
 }
 
@@ -174,10 +183,16 @@ bt_status bt_point_search_host(const bt_tree *t, int mode, const void *h_queries
     bt_status st = check_tree(t);
     if (st != BT_OK) return st;
     if (!valid_point_mode(mode)) return fail(BT_ERR_INVALID_ARGUMENT, "unknown point mode");
+    if (mode == BT_POINT_LEARNED && !t->learned)
+        return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
     if (nq == 0) return BT_OK;
     if (!h_queries || !h_out) return fail(BT_ERR_INVALID_ARGUMENT, "queries or out is NULL");
     if (nq >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "nq must be below 2^32");
     DeviceGuard g(t->device);
+    if (mode == BT_POINT_LEARNED) {
+        st = reset_learned_stats(t, (cudaStream_t)stream);
+        if (st != BT_OK) return st;
+    }
     const void *ins[1] = {h_queries};
     const size_t w[1] = {(size_t)t->key_bytes};
     return host_pipeline(t, (cudaStream_t)stream, nq, pipeline_chunk(nq), 1, ins, w, h_out,

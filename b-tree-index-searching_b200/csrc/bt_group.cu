@@ -223,6 +223,223 @@ part_scatter_kernel(const K *__restrict__ a, const K *__restrict__ b,
     }
 }
 
+// ------------------------------------------- single-pass partition ----
+//
+// The kernels above take three launches per pass (tile histograms, a global
+// scan of the tile x digit table, the scatter), read the keys twice per pass
+// and load each tile's 256 digit bases from a table laid out digit-major
+// (256 scattered reads per tile).  The path below makes one read of the keys
+// for the global digit counts of every pass, then one scatter launch per
+// pass: tiles are taken in launch order from a counter, and each tile learns
+// where its digits start from the tiles before it by decoupled look-back
+// (Merrill & Garland, "Single-pass parallel prefix scan with decoupled
+// look-back", 2016; used per digit in the onesweep radix sort of Adinets &
+// Merrill, 2022): it publishes its digit counts, then walks back over its
+// predecessors' published values until it meets an inclusive prefix.
+
+constexpr int kMaxPasses = 8;
+constexpr unsigned long long kStAgg = 1ull << 62;   // tile aggregate published
+constexpr unsigned long long kStInc = 2ull << 62;   // inclusive prefix published
+constexpr unsigned long long kStVal = (1ull << 62) - 1;
+constexpr uint32_t kLookbackSpins = 1u << 22;       // polls of one predecessor before giving up
+
+// Look-backs that gave up (a predecessor never published: impossible while
+// tiles are taken in order, as they are here); read by
+// bt_partition_lookback_timeouts.
+__device__ unsigned int g_lookback_timeouts = 0;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Digit of pass p of an item: byte p of its group key (of the key itself for
+// the radix sort).
+template <typename K>
+__device__ __forceinline__ uint32_t pass_digit(K a, K b, const GroupKeyParams &gp, int p) {
+    if (gp.kind == kPartRadix) return (uint32_t)(((uint64_t)a >> (8 * p)) & 0xFFu);
+    return (group_key<K>(a, b, gp) >> (8 * p)) & 0xFFu;
+}
+
+// hist[p * 256 + d] += items whose pass-p digit is d, for every pass, in one
+// read of the items (the digits do not depend on the order the passes leave).
+template <typename K, bool HAS_B>
+__global__ void __launch_bounds__(kPT)
+part_hist_all_kernel(const K *__restrict__ a, const K *__restrict__ b, uint64_t n,
+                     GroupKeyParams gp, int passes, uint32_t *__restrict__ hist) {
+    constexpr int C = 4;  // copies, so that one hot digit is not one hot counter
+    __shared__ uint32_t h[C][kMaxPasses * 256];
+    for (int i = threadIdx.x; i < C * kMaxPasses * 256; i += kPT) (&h[0][0])[i] = 0;
+    __syncthreads();
+    uint32_t *hc = h[(threadIdx.x >> 5) & (C - 1)];
+    for (uint64_t i = blockIdx.x * (uint64_t)kPT + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kPT) {
+        const K av = a[i];
+        const K bv = HAS_B ? b[i] : (K)0;
+        for (int p = 0; p < passes; p++) atomicAdd(&hc[p * 256 + pass_digit<K>(av, bv, gp, p)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kPT) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < C; k++) c += h[k][i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// One pass of the stable partition: the tile taken from *tile_ctr (in launch
+// order) is ranked exactly as in part_scatter_kernel, its digit bases come
+// from the global digit starts (exclusive scan of hist) plus the look-back
+// over the tiles before it, and it is written out through shared memory.
+template <typename K, bool HAS_B>
+__global__ void __launch_bounds__(kPT, 3)
+part_onesweep_kernel(const K *__restrict__ a, const K *__restrict__ b,
+                     const uint32_t *__restrict__ perm_in, uint64_t n, GroupKeyParams gp, int pass,
+                     const uint32_t *__restrict__ hist, unsigned int *__restrict__ tile_ctr,
+                     unsigned long long *__restrict__ status, K *__restrict__ oa,
+                     K *__restrict__ ob, uint32_t *__restrict__ operm) {
+    __shared__ uint32_t cnt[kPWarps][256];
+    __shared__ uint32_t tile_start[256];
+    __shared__ uint32_t tile_base[256];
+    __shared__ uint32_t digit_tot[256];
+    __shared__ uint32_t warp_tot[8];
+    __shared__ uint32_t s_tile;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *sa = reinterpret_cast<K *>(smem_raw);
+    K *sb = sa + kPTile;
+    uint32_t *sp = reinterpret_cast<uint32_t *>(sb + (HAS_B ? kPTile : 0));
+    uint8_t *sd = reinterpret_cast<uint8_t *>(sp + kPTile);
+
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kPWarps * 256; i += kPT) (&cnt[0][0])[i] = 0;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    // global start of every digit: exclusive scan of this pass's counts
+    uint32_t gstart = 0;
+    if (threadIdx.x < 256) gstart = block_exscan256(hist[pass * 256 + threadIdx.x], warp_tot);
+    __syncthreads();
+    if (threadIdx.x < 256) {
+        uint32_t wp = 0;
+        for (int ww = 0; ww < (threadIdx.x >> 5); ww++) wp += warp_tot[ww];
+        gstart += wp;
+    }
+    const uint64_t tile = s_tile;
+    const uint64_t t0 = tile * kPTile;
+    K av[kIPL], bv[kIPL];
+    uint32_t pv[kIPL], dg[kIPL], rk[kIPL];
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        const uint64_t i = t0 + (uint64_t)w * kPerWarp + (uint64_t)j * 32 + lane;
+        dg[j] = 0xFFFFFFFFu;
+        av[j] = 0;
+        bv[j] = 0;
+        pv[j] = 0;
+        if (i < n) {
+            av[j] = a[i];
+            if (HAS_B) bv[j] = b[i];
+            pv[j] = perm_in ? perm_in[i] : (uint32_t)i;
+            dg[j] = pass_digit<K>(av[j], bv[j], gp, pass);
+        }
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    unsigned mm[kIPL];
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) mm[j] = __match_any_sync(0xffffffffu, dg[j]);
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        const unsigned m = mm[j];
+        const int leader = __ffs(m) - 1;
+        uint32_t c = 0;
+        if (dg[j] != 0xFFFFFFFFu && lane == leader) c = atomicAdd(&cnt[w][dg[j]], (uint32_t)__popc(m));
+        c = __shfl_sync(0xffffffffu, c, leader);
+        rk[j] = c + __popc(m & lt);
+    }
+    __syncthreads();
+    {
+        const int d = 16 * w + (lane & 15);
+        const int h = lane >> 4;
+        uint32_t v[kPWarps / 2];
+#pragma unroll
+        for (int k = 0; k < kPWarps / 2; k++) v[k] = cnt[(kPWarps / 2) * h + k][d];
+        uint32_t half_tot = 0;
+#pragma unroll
+        for (int k = 0; k < kPWarps / 2; k++) half_tot += v[k];
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, half_tot, 16);
+        uint32_t run = h ? other : 0u;
+#pragma unroll
+        for (int k = 0; k < kPWarps / 2; k++) {
+            cnt[(kPWarps / 2) * h + k][d] = run;
+            run += v[k];
+        }
+        if (h == 0) digit_tot[d] = half_tot + other;
+    }
+    __syncthreads();
+    // publish this tile's counts, then sum the predecessors' (look-back)
+    if (threadIdx.x < 256) {
+        const int d = threadIdx.x;
+        const uint32_t agg = digit_tot[d];
+        unsigned long long *mine = status + tile * 256 + d;
+        unsigned long long prefix = 0;
+        if (tile == 0) {
+            st_release_u64(mine, kStInc | agg);
+        } else {
+            st_release_u64(mine, kStAgg | agg);
+            uint64_t tp = tile - 1;
+            uint32_t spins = 0;
+            for (;;) {
+                const unsigned long long v = ld_acquire_u64(status + tp * 256 + d);
+                const unsigned long long f = v & ~kStVal;
+                if (f == 0) {
+                    if (++spins > kLookbackSpins) {  // never in a correct launch; bounded anyway
+                        atomicAdd(&g_lookback_timeouts, 1u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                spins = 0;
+                prefix += v & kStVal;
+                if (f == kStInc || tp == 0) break;
+                tp--;
+            }
+            st_release_u64(mine, kStInc | (prefix + agg));
+        }
+        tile_base[d] = gstart + (uint32_t)prefix;
+    }
+    uint32_t tot = threadIdx.x < 256 ? digit_tot[threadIdx.x] : 0u;
+    uint32_t ex = 0;
+    if (threadIdx.x < 256) ex = block_exscan256(tot, warp_tot + 0);
+    __syncthreads();
+    if (threadIdx.x < 256) {
+        uint32_t wp = 0;
+        for (int ww = 0; ww < (threadIdx.x >> 5); ww++) wp += warp_tot[ww];
+        tile_start[threadIdx.x] = ex + wp;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kIPL; j++) {
+        if (dg[j] != 0xFFFFFFFFu) {
+            const uint32_t lp = tile_start[dg[j]] + cnt[w][dg[j]] + rk[j];
+            sa[lp] = av[j];
+            if (HAS_B) sb[lp] = bv[j];
+            sp[lp] = pv[j];
+            sd[lp] = (uint8_t)dg[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t tn = t0 < n ? (uint32_t)min((uint64_t)kPTile, n - t0) : 0u;
+    for (uint32_t lp = threadIdx.x; lp < tn; lp += kPT) {
+        const uint32_t d = sd[lp];
+        const uint64_t g = (uint64_t)tile_base[d] + (lp - tile_start[d]);
+        oa[g] = sa[lp];
+        if (HAS_B) ob[g] = sb[lp];
+        operm[g] = sp[lp];
+    }
+}
+
 // ---------------------------------------------------------------- scan ----
 
 constexpr int kST = 512;
@@ -345,6 +562,88 @@ bt_status scan_impl(const T *d_in, T *d_out, uint64_t n, T *d_total, cudaStream_
 
 // -------------------------------------------------------- partition host --
 
+// Dynamic shared memory of part_scatter_kernel<K, HAS_B> and its one-time
+// raise above the 48 KB default (per device and instantiation; function
+// attributes are per device, and the server's worker and user threads may
+// partition at once).
+template <typename K, bool HAS_B>
+constexpr size_t scatter_smem() {
+    return (size_t)kPTile * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t) + 1);
+}
+
+template <typename K, bool HAS_B>
+bt_status scatter_smem_attr() {
+    static std::atomic<bool> done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return BT_OK;
+    BT_CUDA(cudaFuncSetAttribute(part_scatter_kernel<K, HAS_B>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem<K, HAS_B>()));
+    if (dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
+    return BT_OK;
+}
+
+template <typename K, bool HAS_B>
+bt_status onesweep_smem_attr() {
+    static std::atomic<bool> done[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && done[dev].load(std::memory_order_acquire)) return BT_OK;
+    BT_CUDA(cudaFuncSetAttribute(part_onesweep_kernel<K, HAS_B>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)scatter_smem<K, HAS_B>()));
+    if (dev >= 0 && dev < 64) done[dev].store(true, std::memory_order_release);
+    return BT_OK;
+}
+
+// Workspace of the single-pass partition: digit counts of every pass, one
+// tile counter per pass, the look-back status of one pass.
+struct SweepWs {
+    uint32_t *hist;
+    unsigned int *ctr;
+    unsigned long long *status;
+    static size_t bytes(uint64_t ntiles) {
+        return kMaxPasses * 256 * sizeof(uint32_t) + 256 + ntiles * 256 * sizeof(unsigned long long);
+    }
+    void carve(unsigned char *p) {
+        hist = reinterpret_cast<uint32_t *>(p);
+        ctr = reinterpret_cast<unsigned int *>(p + kMaxPasses * 256 * sizeof(uint32_t));
+        status = reinterpret_cast<unsigned long long *>(p + kMaxPasses * 256 * sizeof(uint32_t) + 256);
+    }
+};
+
+// Stable partition of n items by `passes` digits: pass p reads (ia, ib, ip)
+// and writes (oa[p], ob[p], op[p]); the histogram of every pass comes from
+// one read of the input.
+template <typename K, bool HAS_B>
+bt_status sweep_passes(const K *a, const K *b, uint64_t n, GroupKeyParams gp, int passes,
+                       K *const *oa, K *const *ob, uint32_t *const *op, SweepWs ws,
+                       cudaStream_t s) {
+    const uint64_t ntiles = (n + kPTile - 1) / kPTile;
+    BT_CUDA(cudaMemsetAsync(ws.hist, 0, kMaxPasses * 256 * sizeof(uint32_t) + 256, s));
+    bt_status st = onesweep_smem_attr<K, HAS_B>();
+    if (st != BT_OK) return st;
+    count_launch();
+    part_hist_all_kernel<K, HAS_B>
+        <<<(unsigned)std::min<uint64_t>(ntiles, (uint64_t)sm_count() * 4), kPT, 0, s>>>(
+            a, b, n, gp, passes, ws.hist);
+    const K *ia = a, *ib = b;
+    const uint32_t *ip = nullptr;
+    for (int p = 0; p < passes; p++) {
+        BT_CUDA(cudaMemsetAsync(ws.status, 0, ntiles * 256 * sizeof(unsigned long long), s));
+        count_launch();
+        part_onesweep_kernel<K, HAS_B><<<(unsigned)ntiles, kPT, scatter_smem<K, HAS_B>(), s>>>(
+            ia, ib, ip, n, gp, p, ws.hist, ws.ctr + p, ws.status, oa[p], HAS_B ? ob[p] : nullptr,
+            op[p]);
+        BT_CUDA(cudaGetLastError());
+        ia = oa[p];
+        ib = HAS_B ? ob[p] : nullptr;
+        ip = op[p];
+    }
+    return BT_OK;
+}
+
 template <typename K, bool HAS_B>
 bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b, uint64_t nq,
                          K *out_a, K *out_b, uint32_t *out_perm, cudaStream_t s) {
@@ -364,62 +663,29 @@ bt_status partition_impl(const bt_tree *t, int kind, const K *d_a, const K *d_b,
     const uint64_t ntiles = (nq + kPTile - 1) / kPTile;
     if (ntiles * 256 >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "batch too large");
 
-    // One workspace: digit counts, scan scratch and, for multi-pass sorts,
-    // ping-pong copies of the payload.
-    const uint64_t ncounts = ntiles * 256;
-    const uint64_t scan_we = scan_ws_elems(ncounts);
-    const size_t pp_bytes = passes > 1 ? 2 * nq * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t)) : 0;
-    const size_t ws_bytes = (ncounts + scan_we) * sizeof(uint32_t) + 256 + pp_bytes;
+    // One workspace: the single-pass partition's counts and look-back status
+    // and, for two passes, one intermediate copy of the payload.
+    const size_t sweep_bytes = (SweepWs::bytes(ntiles) + 255) / 256 * 256;
+    const size_t pp_bytes = passes > 1 ? nq * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t)) + 512 : 0;
     unsigned char *ws = nullptr;
-    bt_status st = ws_alloc((void **)&ws, ws_bytes, s);
+    bt_status st = ws_alloc((void **)&ws, sweep_bytes + pp_bytes, s);
     if (st != BT_OK) return st;
-    uint32_t *counts = reinterpret_cast<uint32_t *>(ws);
-    uint32_t *scan_ws = counts + ncounts;
-    unsigned char *pp = ws + ((ncounts + scan_we) * sizeof(uint32_t) + 255) / 256 * 256;
-    K *ta[2] = {nullptr, nullptr}, *tb[2] = {nullptr, nullptr};
-    uint32_t *tp[2] = {nullptr, nullptr};
-    if (passes > 1) {
-        for (int i = 0; i < 2; i++) {
-            ta[i] = reinterpret_cast<K *>(pp);
-            pp += nq * sizeof(K);
-            if (HAS_B) {
-                tb[i] = reinterpret_cast<K *>(pp);
-                pp += nq * sizeof(K);
-            }
-            tp[i] = reinterpret_cast<uint32_t *>(pp);
-            pp += nq * sizeof(uint32_t);
+    SweepWs sw;
+    sw.carve(ws);
+    K *oa[2] = {out_a, out_a}, *ob[2] = {out_b, out_b};
+    uint32_t *op[2] = {out_perm, out_perm};
+    if (passes > 1) {  // pass 0 into the intermediate copy, pass 1 into the caller's arrays
+        unsigned char *pp = ws + sweep_bytes;
+        oa[0] = reinterpret_cast<K *>(pp);
+        pp += (nq * sizeof(K) + 255) / 256 * 256;
+        if (HAS_B) {
+            ob[0] = reinterpret_cast<K *>(pp);
+            pp += (nq * sizeof(K) + 255) / 256 * 256;
         }
+        op[0] = reinterpret_cast<uint32_t *>(pp);
     }
-    const size_t smem = (size_t)kPTile * (sizeof(K) * (HAS_B ? 2 : 1) + sizeof(uint32_t) + 1);
-    auto scat = part_scatter_kernel<K, HAS_B>;
-    static std::atomic<bool> attr_done[64] = {};  // per device, per instantiation; any host thread
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_done[dev].load(std::memory_order_acquire)) {
-        cudaError_t e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) st = cuda_fail(e, "cudaFuncSetAttribute");
-        else if (dev >= 0 && dev < 64) attr_done[dev].store(true, std::memory_order_release);
-    }
-    const K *ia = d_a, *ib = d_b;
-    const uint32_t *ip = nullptr;
-    for (int p = 0; p < passes && st == BT_OK; p++) {
-        const bool last = p == passes - 1;
-        K *oa = last ? out_a : ta[p & 1];
-        K *ob = last ? out_b : tb[p & 1];
-        uint32_t *op = last ? out_perm : tp[p & 1];
-        count_launch();
-        part_hist_kernel<K, HAS_B><<<(unsigned)ntiles, kPT, 0, s>>>(ia, ib, nq, gp, p, counts, ntiles);
-        st = scan_run<uint32_t>(counts, counts, ncounts, nullptr, scan_ws, s);
-        if (st != BT_OK) break;
-        count_launch();
-        scat<<<(unsigned)ntiles, kPT, smem, s>>>(ia, ib, ip, nq, gp, p, counts, ntiles, oa, ob, op);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) st = cuda_fail(e, "partition kernels");
-        ia = oa;
-        ib = ob;
-        ip = op;
-    }
+    if (passes > 2) st = fail(BT_ERR_INTERNAL, "partition supports at most two passes");
+    if (st == BT_OK) st = sweep_passes<K, HAS_B>(d_a, d_b, nq, gp, passes, oa, ob, op, sw, s);
     ws_free(ws, s);
     return st;
 }
@@ -440,53 +706,34 @@ bt_status sort_pairs_impl(const K *d_keys, const V *d_vals, uint64_t n, K *out_k
                           cudaStream_t s) {
     const int passes = (int)sizeof(K);
     const uint64_t ntiles = (n + kPTile - 1) / kPTile;
-    const uint64_t ncounts = ntiles * 256;
-    const uint64_t scan_we = scan_ws_elems(ncounts);
-    const size_t ws_bytes = (ncounts + scan_we) * sizeof(uint32_t) + 256 +
-                            2 * n * (sizeof(K) + sizeof(uint32_t)) + 512;
+    const size_t sweep_bytes = (SweepWs::bytes(ntiles) + 255) / 256 * 256;
+    const size_t kbytes = (n * sizeof(K) + 255) / 256 * 256;
+    const size_t pbytes = (n * sizeof(uint32_t) + 255) / 256 * 256;
     unsigned char *ws = nullptr;
-    bt_status st = ws_alloc((void **)&ws, ws_bytes, s);
+    bt_status st = ws_alloc((void **)&ws, sweep_bytes + 2 * (kbytes + pbytes), s);
     if (st != BT_OK) return st;
-    uint32_t *counts = reinterpret_cast<uint32_t *>(ws);
-    uint32_t *scan_ws = counts + ncounts;
-    unsigned char *pp = ws + ((ncounts + scan_we) * sizeof(uint32_t) + 255) / 256 * 256;
-    K *tk[2];
-    uint32_t *tp[2];
-    for (int i = 0; i < 2; i++) {
-        tk[i] = reinterpret_cast<K *>(pp);
-        pp += (n * sizeof(K) + 255) / 256 * 256;
-        tp[i] = reinterpret_cast<uint32_t *>(pp);
-        pp += (n * sizeof(uint32_t) + 255) / 256 * 256;
+    SweepWs sw;
+    sw.carve(ws);
+    unsigned char *pp = ws + sweep_bytes;
+    K *tk[2] = {reinterpret_cast<K *>(pp), reinterpret_cast<K *>(pp + kbytes + pbytes)};
+    uint32_t *tp[2] = {reinterpret_cast<uint32_t *>(pp + kbytes),
+                       reinterpret_cast<uint32_t *>(pp + 2 * kbytes + pbytes)};
+    K *ok[kMaxPasses];
+    uint32_t *op[kMaxPasses];
+    for (int p = 0; p < passes; p++) {
+        ok[p] = p == passes - 1 ? out_keys : tk[p & 1];
+        op[p] = tp[p & 1];
     }
-    const size_t smem = (size_t)kPTile * (sizeof(K) + sizeof(uint32_t) + 1);
-    auto scat = part_scatter_kernel<K, false>;
-    cudaError_t e = cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) st = cuda_fail(e, "cudaFuncSetAttribute");
     GroupKeyParams gp;
     gp.kind = kPartRadix;
     gp.cbits = 8;
-    const K *ik = d_keys;
-    const uint32_t *ip = nullptr;  // the first pass numbers the input itself
-    for (int p = 0; p < passes && st == BT_OK; p++) {
-        gp.shift = 8 * p;
-        K *ok = p == passes - 1 ? out_keys : tk[p & 1];
-        uint32_t *op = tp[p & 1];
-        count_launch();
-        part_hist_kernel<K, false><<<(unsigned)ntiles, kPT, 0, s>>>(ik, nullptr, n, gp, 0, counts, ntiles);
-        st = scan_run<uint32_t>(counts, counts, ncounts, nullptr, scan_ws, s);
-        if (st != BT_OK) break;
-        count_launch();
-        scat<<<(unsigned)ntiles, kPT, smem, s>>>(ik, nullptr, ip, n, gp, 0, counts, ntiles, ok, nullptr, op);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) st = cuda_fail(e, "radix sort pass");
-        ik = ok;
-        ip = op;
-    }
+    gp.shift = 0;
+    st = sweep_passes<K, false>(d_keys, nullptr, n, gp, passes, ok, nullptr, op, sw, s);
     if (st == BT_OK) {
         count_launch();
         gather_kernel<V><<<(unsigned)std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count() * 16), 256, 0, s>>>(
-            d_vals, ip, n, out_vals);
-        e = cudaGetLastError();
+            d_vals, op[passes - 1], n, out_vals);
+        cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = cuda_fail(e, "value gather");
     }
     ws_free(ws, s);
@@ -506,9 +753,10 @@ bt_status partition_point_prealloc(const bt_tree *t, const K *d_q, uint64_t nq, 
     const uint64_t ncounts = ntiles * 256;
     uint32_t *counts = reinterpret_cast<uint32_t *>(ws);
     uint32_t *scan_ws = counts + ncounts;
-    const size_t smem = (size_t)kPTile * (sizeof(K) + sizeof(uint32_t) + 1);
+    const size_t smem = scatter_smem<K, false>();
     auto scat = part_scatter_kernel<K, false>;
-    BT_CUDA(cudaFuncSetAttribute(scat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    bt_status sa = scatter_smem_attr<K, false>();
+    if (sa != BT_OK) return sa;
     count_launch();
     part_hist_kernel<K, false><<<(unsigned)ntiles, kPT, 0, s>>>(d_q, nullptr, nq, gp, 0, counts, ntiles);
     bt_status st = scan_run<uint32_t>(counts, counts, ncounts, nullptr, scan_ws, s);
@@ -823,3 +1071,13 @@ bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const 
 }
 
 }  // namespace bt
+
+extern "C" {
+
+uint64_t bt_partition_lookback_timeouts(void) {
+    unsigned int v = 0;
+    if (cudaMemcpyFromSymbol(&v, bt::g_lookback_timeouts, sizeof(v)) != cudaSuccess) return ~0ull;
+    return v;
+}
+
+}  // extern "C"

@@ -231,6 +231,12 @@ int search_cfg_lanes(int cfg);
 int search_cfg_rounds(int cfg);
 
 void free_learned(bt::LearnedState *s);
+// Learned point search of d_q into d_out on s (the tree has a learned index;
+// the counters of bt_learned_last_stats accumulate).
+bt_status launch_learned_search(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
+                                cudaStream_t s);
+// Zeroes those counters (stream-ordered).
+bt_status reset_learned_stats(const bt_tree *t, cudaStream_t s);
 
 // Partition kinds for launch_partition.
 enum PartitionKind { kPartPoint = 0, kPart2D = 1, kPartZ = 2, kPartRadix = 3 };

@@ -973,6 +973,22 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
 }
 
 }  // namespace
+
+bt_status launch_learned_search(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
+                                cudaStream_t s) {
+    if (nq == 0) return BT_OK;
+    if (t->key_bytes == 4)
+        return t->val_bytes == 4 ? learned_launch<uint32_t, uint32_t>(t, d_q, nq, d_out, s)
+                                 : learned_launch<uint32_t, uint64_t>(t, d_q, nq, d_out, s);
+    return t->val_bytes == 4 ? learned_launch<uint64_t, uint32_t>(t, d_q, nq, d_out, s)
+                             : learned_launch<uint64_t, uint64_t>(t, d_q, nq, d_out, s);
+}
+
+bt_status reset_learned_stats(const bt_tree *t, cudaStream_t s) {
+    BT_CUDA(cudaMemsetAsync(t->learned->d_stats, 0, 2 * sizeof(unsigned long long), s));
+    return BT_OK;
+}
+
 }  // namespace bt
 
 extern "C" {
@@ -1010,29 +1026,7 @@ bt_status bt_learned_train(bt_tree *t, const bt_learned_config *cfg_in, void *st
 
 bt_status bt_point_search_learned(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
                                   void *stream) {
-    using namespace bt;
-    if (!t) return fail(BT_ERR_INVALID_ARGUMENT, "tree is NULL");
-    if (!t->learned) return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
-    if (nq == 0) return BT_OK;
-    if (!d_q || !d_out) return fail(BT_ERR_INVALID_ARGUMENT, "queries or out is NULL");
-    if (nq >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "nq must be below 2^32");
-    int prev = 0;
-    BT_CUDA(cudaGetDevice(&prev));
-    if (prev != t->device) BT_CUDA(cudaSetDevice(t->device));
-    cudaStream_t s = (cudaStream_t)stream;
-    bt_status st = BT_OK;
-    cudaError_t e = cudaMemsetAsync(t->learned->d_stats, 0, 2 * sizeof(unsigned long long), s);
-    if (e != cudaSuccess) st = cuda_fail(e, "cudaMemsetAsync");
-    if (st == BT_OK) {
-        if (t->key_bytes == 4)
-            st = t->val_bytes == 4 ? learned_launch<uint32_t, uint32_t>(t, d_q, nq, d_out, s)
-                                   : learned_launch<uint32_t, uint64_t>(t, d_q, nq, d_out, s);
-        else
-            st = t->val_bytes == 4 ? learned_launch<uint64_t, uint32_t>(t, d_q, nq, d_out, s)
-                                   : learned_launch<uint64_t, uint64_t>(t, d_q, nq, d_out, s);
-    }
-    if (prev != t->device) cudaSetDevice(prev);
-    return st;
+    return bt_point_search(t, BT_POINT_LEARNED, d_q, nq, d_out, stream);
 }
 
 bt_status bt_learned_last_stats(const bt_tree *t, uint64_t *extra, uint64_t *fallback) {

@@ -23,7 +23,8 @@
 //     different host threads, without ordering between them) race on it.
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture.
+//     before any stream capture.  The address is cached for the life of the
+//     process, so it does not survive a cudaDeviceReset of that device.
 #include <mutex>
 
 #include "bt_internal.cuh"

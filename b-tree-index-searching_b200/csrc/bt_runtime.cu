@@ -21,6 +21,7 @@ DeviceState g_dev[64];
 }  // namespace
 
 std::atomic<uint64_t> g_launches{0};
+std::atomic<uint64_t> g_ws_allocs{0};  // ws_alloc calls (bt_workspace_allocations)
 
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
@@ -72,6 +73,7 @@ int sm_count() {
 
 bt_status ws_alloc(void **p, size_t bytes, cudaStream_t s) {
     *p = nullptr;
+    g_ws_allocs.fetch_add(1, std::memory_order_relaxed);
     if (bytes == 0) bytes = 256;
     int d = current_device();
     cudaMemPool_t pool;
@@ -125,5 +127,7 @@ const char *bt_status_string(bt_status s) {
 const char *bt_last_error(void) { return bt::g_last_error.c_str(); }
 
 uint64_t bt_kernel_launches(void) { return bt::g_launches.load(std::memory_order_relaxed); }
+
+uint64_t bt_workspace_allocations(void) { return bt::g_ws_allocs.load(std::memory_order_relaxed); }
 
 }  // extern "C"

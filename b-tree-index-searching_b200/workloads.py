@@ -14,6 +14,8 @@ from fixed seeds with numpy's PCG64:
                     code, value = point ID, sorted by (code, ID); rectangles
                     with a uniform corner and sides uniform in [1, 256].
   lognormal_keys -- u64 keys = cumulative sum of floor(lognormal(4, 2)) + 1.
+  lognormal_point -- those keys (value = rank); queries 90% keys uniform over
+                    the ranks, 10% uniform in [min, max].
 
 Zipf sampling uses rejection-inversion (W. Hormann, G. Derflinger, "Rejection-
 inversion to generate variates from monotone discrete distributions", ACM
@@ -157,6 +159,19 @@ def lognormal_keys(n_keys=1 << 28, mu=4.0, sigma=2.0, seed=KEY_SEED, chunk=1 << 
         keys[i:i + m] = c
         acc = c[-1]
     return keys
+
+
+def lognormal_point(n_keys=1 << 28, n_queries=1 << 24, miss=0.10, seed=KEY_SEED, query_seed=None):
+    """Learned-index workload: lognormal_keys (value = rank, u64); queries
+    drawn uniformly over the ranks, a `miss` fraction uniform in [min, max]
+    (mostly absent keys).  query_seed varies the batch, not the keys."""
+    keys = lognormal_keys(n_keys, seed=seed)
+    vals = np.arange(n_keys, dtype=np.uint64)
+    g = rng((seed + 7) if query_seed is None else query_seed)
+    q = keys[g.integers(0, n_keys, size=n_queries)]
+    m = g.random(n_queries) < miss
+    q[m] = g.integers(int(keys[0]), int(keys[-1]) + 1, size=int(m.sum()), dtype=np.uint64)
+    return keys, vals, q
 
 
 def forest(num_trees=4096, size_log2=(10, 20), batch_log2=(6, 16), hit=0.8, range_frac=0.01,

@@ -1,22 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the B200 B+tree engine.
 
-Default workload (one "step" = one radix-grouped batch point search):
-2^26 unique uniform u32 keys (value = rank), bulk-built once; a batch of
-2^24 point queries, 90% keys drawn with Zipf(0.99) ranks, 10% uniform u32;
-queries radix-grouped by their top 8 bits, then searched.
+Default workload (one "step" = one batched point search through the learned
+index): 2^28 unique u64 keys, the cumulative sum of floor(lognormal(4, 2)) + 1
+gaps (value = rank), bulk-built once with a learned index of 2^16 leaf
+segments trained on the GPU; a batch of 2^24 point queries, 90% keys drawn
+uniformly over the ranks, 10% uniform in [min, max].
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Prints ONE JSON line on rank 0.  `value` is whole-job queries/s with the
-queries resident in HBM (device-timed with CUDA events, max over ranks);
-`e2e` is the same metric through the host-buffer C-ABI call
-bt_point_search_host (H2D of the queries and D2H of the results inside the
-timed region).  The path shards as independent replicas (every rank holds the
-tree and answers its own batch, no collective on the data path), so N GPUs
-report weak scaling.  `--impl reference` times the CPU restatement of the
-reference's algorithm (its fanout-5000 page tree, oracle/oracle.c) on the
-host cores.
+Prints ONE JSON line on rank 0.  `value` is whole-job queries/s of the learned
+search with the queries resident in HBM (device-timed with CUDA events, max
+over ranks); `plain` is the same batch through the plain tree search, and
+`learned_over_plain` their ratio; `e2e` is the learned search through the
+host-buffer C-ABI call bt_point_search_host(BT_POINT_LEARNED) (H2D of the
+queries and D2H of the results inside the timed region).  The path shards as
+independent replicas (every rank holds the tree and answers its own batch, no
+collective on the data path), so N GPUs report weak scaling.  `--impl
+reference` times the CPU restatement of the reference's algorithm (its
+fanout-5000 page tree, oracle/oracle.c) on the host cores, on the same
+workload.  Further objects: the reference's own kernels on this GPU
+(`reference_gpu`), the radix-grouped configuration (`grouped`), the
+L2-resident basic search (`small`), ranges, rectangles, the forest, the
+build and the request loop (`serving`).
 """
 import argparse
 import ctypes
@@ -44,20 +50,24 @@ def parse_args(argv=None):
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--keys-log2", type=int, default=26)
+    p.add_argument("--keys-log2", type=int, default=28, help="keys of the learned-index workload")
     p.add_argument("--queries-log2", type=int, default=24)
+    p.add_argument("--grouped-keys-log2", type=int, default=26,
+                   help="keys of the radix-grouped workload (u32)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-log2", type=int, default=22)
-    p.add_argument("--no-learned", action="store_true",
-                   help="skip the learned-index + serving section (2^28 u64 keys)")
-    p.add_argument("--learned-keys-log2", type=int, default=28)
+    p.add_argument("--segments-log2", type=int, default=16, help="learned index segments")
+    p.add_argument("--no-serving", action="store_true", help="skip the request loop")
+    p.add_argument("--no-grouped", action="store_true", help="skip the radix-grouped section")
+    p.add_argument("--no-reference-gpu", action="store_true",
+                   help="skip timing the reference's own kernels")
     p.add_argument("--serve-requests", type=int, default=3000)
     p.add_argument("--serve-rate", type=float, default=20000.0, help="requests per second")
     p.add_argument("--no-forest", action="store_true", help="skip the 4096-tree forest section")
     p.add_argument("--no-rect", action="store_true", help="skip the rectangle-search section")
     p.add_argument("--rect-boxes-log2", type=int, default=20, help="boxes in the rectangle section")
     p.add_argument("--forest-trees", type=int, default=4096, help="trees in the forest section")
-    p.add_argument("--only", choices=["learned", "forest", "rect"],
+    p.add_argument("--only", choices=["learned", "grouped", "forest", "rect", "small"],
                    help="run one extension section alone on cuda:0 and print its JSON object "
                         "(for profiling; not the bench line)")
     return p.parse_args(argv)
@@ -159,32 +169,48 @@ class ClockSampler:
 
 # -------------------------------------------------------------- workload ----
 
-def workload(keys_log2, queries_log2, rank):
-    wl = importlib.import_module(PKG + ".workloads")
+def _cached(tag, make):
     cache = os.path.join(tempfile.gettempdir(), "btree_b200_bench")
     os.makedirs(cache, exist_ok=True)
-    tag = f"zipf_k{keys_log2}_q{queries_log2}_r{rank}"
     f = os.path.join(cache, tag + ".npz")
     if os.path.exists(f):
         d = np.load(f)
         return d["keys"], d["vals"], d["q"]
-    keys, vals, q = wl.point_zipf(1 << keys_log2, 1 << queries_log2, seed=wl.KEY_SEED)
-    if rank:
-        # each replica answers its own batch (weak scaling)
-        _, _, q = wl.point_zipf(1 << keys_log2, 1 << queries_log2, seed=wl.KEY_SEED + 100 * rank)
+    keys, vals, q = make()
     np.savez(f, keys=keys, vals=vals, q=q)
     return keys, vals, q
 
 
+def lognormal_workload(keys_log2, queries_log2, rank):
+    """The learned-index workload; each replica answers its own batch."""
+    wl = importlib.import_module(PKG + ".workloads")
+    qs = None if rank == 0 else wl.KEY_SEED + 7 + 100 * rank
+    return _cached(f"lognormal_k{keys_log2}_q{queries_log2}_r{rank}",
+                   lambda: wl.lognormal_point(1 << keys_log2, 1 << queries_log2, query_seed=qs))
+
+
+def zipf_workload(keys_log2, queries_log2, rank):
+    """The radix-grouped workload; each replica answers its own batch."""
+    wl = importlib.import_module(PKG + ".workloads")
+
+    def make():
+        keys, vals, q = wl.point_zipf(1 << keys_log2, 1 << queries_log2, seed=wl.KEY_SEED)
+        if rank:
+            _, _, q = wl.point_zipf(1 << keys_log2, 1 << queries_log2, seed=wl.KEY_SEED + 100 * rank)
+        return keys, vals, q
+    return _cached(f"zipf_k{keys_log2}_q{queries_log2}_r{rank}", make)
+
+
 def workload_desc(args):
     return {
-        "workload": (f"radix-grouped point search: 2^{args.keys_log2} unique uniform u32 keys "
-                     f"(value = rank), batches of 2^{args.queries_log2} queries, 90% keys by "
-                     "Zipf(0.99) rank, 10% uniform u32; grouped by the top 8 key bits"),
+        "workload": (f"batched+learned point search: 2^{args.keys_log2} unique u64 keys = "
+                     "cumsum(floor(lognormal(4, 2)) + 1) (value = rank), learned index of "
+                     f"2^{args.segments_log2} segments; batches of 2^{args.queries_log2} queries, "
+                     "90% keys uniform over the ranks, 10% uniform in [min, max]"),
         "keys": 1 << args.keys_log2,
         "queries_per_step": 1 << args.queries_log2,
-        "key_type": "u32", "value_type": "u32",
-        "l2": "flushed before every timed step (512 MiB write); tree (512 MiB) > L2",
+        "key_type": "u64", "value_type": "u64",
+        "l2": "flushed before every timed step (512 MiB write); tree (4.5 GiB) > L2",
         "parallelism": f"replicas x{args.gpus}",
     }
 
@@ -236,7 +262,7 @@ def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    keys, vals, q = workload(args.keys_log2, args.queries_log2, 0)
+    keys, vals, q = lognormal_workload(args.keys_log2, args.queries_log2, 0)
     from oracle.oracle import Oracle
     orc = Oracle()
     t = orc.refc_build(keys.astype(np.uint64), vals.astype(np.uint64))
@@ -260,7 +286,7 @@ def run_reference(args):
         "data": "synthetic (seeded)", "config": workload_desc(args),
         "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
                          "sample": f"{sample} of the step's queries per step, reference page "
-                                   "tree (fanout 5000) restated in C, OpenMP"},
+                                   "tree (fanout 5000) restated in C, OpenMP on all cores"},
         "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -268,63 +294,17 @@ def run_reference(args):
     return 0
 
 
-# ------------------------------------------ learned index + serving --------
+# --------------------------------------------------------- request loop ----
 
-def learned_section(args, device, bt, flush):
-    """Learned index and serving workload: 2^28 unique u64 keys (cumulative sum of
-    floor(lognormal(4, 2)) + 1 gaps), value = rank; FP32 two-stage model with
-    2^16 leaf segments trained on the GPU.  Reports the plain and the learned
-    batched point-search throughput on a 2^24-query batch (90% hits uniform
-    over ranks, 10% uniform in [min, max]) and p50/p99 latency of a Poisson
-    request loop with batch sizes round(2^U), U ~ uniform[0, 16]."""
+def serving_section(args, bt, tree, keys, plain_cfg, learned_cfg):
+    """Poisson request loop on the learned-index tree: batch sizes round(2^U),
+    U ~ uniform[0, 16], 90% hits uniform over the ranks, 10% uniform in
+    [min, max]; pinned host buffers; p50/p99 from arrival to completion,
+    plain and learned."""
     import torch
     wl = importlib.import_module(PKG + ".workloads")
-    at = importlib.import_module(PKG + ".autotune")
-    n = 1 << args.learned_keys_log2
-    keys = wl.lognormal_keys(n)
-    vals = np.arange(n, dtype=np.uint64)
-    g = wl.rng(wl.KEY_SEED + 7)
-    nq = 1 << args.queries_log2
-    q = keys[g.integers(0, n, size=nq)]
-    miss = g.random(nq) < 0.10
-    q[miss] = g.integers(int(keys[0]), int(keys[-1]) + 1, size=int(miss.sum()), dtype=np.uint64)
-    stream = torch.cuda.current_stream(device)
-    tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
-    rep = tree.learned_train(num_segments=1 << 16, hidden=16, iterations=400)
-    dq = torch.from_numpy(q).to(device)
-    out = torch.empty(nq, dtype=torch.uint64, device=device)
-
-    def timed(fn, steps):
-        ts = []
-        for _ in range(steps):
-            flush.zero_()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            fn()
-            b.record(stream)
-            b.synchronize()
-            ts.append(a.elapsed_time(b))
-        return statistics.mean(ts)
-
-    lanes_p, rounds_p, _ = at.tune(tree, dq, mode="basic", repeats=3)
-    plain_ms = timed(lambda: tree.point_search(dq, mode="basic", out=out, stream=stream), args.steps)
-    plain_res = out.cpu().numpy()
-    learned_ms = {}
-    for cfg in tree.SEARCH_CONFIGS:  # the autotuner's choice for the learned kernel
-        tree.set_search_config(*cfg)
-        learned_ms[cfg] = timed(lambda: tree.point_search_learned(dq, out=out, stream=stream), 2)
-    best = min(learned_ms, key=learned_ms.get)
-    tree.set_search_config(*best)
-    l_ms = timed(lambda: tree.point_search_learned(dq, out=out, stream=stream), args.steps)
-    learned_res = out.cpu().numpy()
-    windowed, fallback = tree.learned_last_stats()
-    hits = int(np.count_nonzero(learned_res != np.uint64(0xFFFFFFFFFFFFFFFF)))
-    exact = bool(np.array_equal(learned_res, plain_res))
-    alg = nq * (8 + 8 + 32) + hits * 32
-    peak, _ = measured_peak()
-
-    # request loop: Poisson arrivals, log-uniform batch sizes, pinned buffers
+    g = wl.rng(wl.KEY_SEED + 9)
+    n = len(keys)
     sizes = np.rint(2.0 ** g.uniform(0, 16, size=args.serve_requests)).astype(np.int64)
     reqs = []
     for m in sizes:
@@ -334,39 +314,19 @@ def learned_section(args, device, bt, flush):
         reqs.append(torch.from_numpy(r).pin_memory().numpy())
     outs = [torch.empty(len(r), dtype=torch.uint64).pin_memory().numpy() for r in reqs]
     arrivals = np.cumsum(g.exponential(1e6 / args.serve_rate, size=len(reqs)))
-    serving = {}
+    res = {"requests": int(len(reqs)), "rate_per_s": args.serve_rate,
+           "batch_sizes": "round(2^U), U ~ uniform[0,16]"}
     for mode in ("basic", "learned"):
-        tree.set_search_config(*(best if mode == "learned" else (lanes_p, rounds_p)))
+        tree.set_search_config(*(learned_cfg if mode == "learned" else plain_cfg))
         with bt.Server(tree, mode=mode, slots=8, memory_budget_bytes=512 << 20) as srv:
             srv.replay(reqs[:200], arrivals[:200] - arrivals[0], outs[:200])  # warm-up
             lat, wall, _ = srv.replay(reqs, arrivals - arrivals[0], outs)
             st = srv.stats()
-        serving[mode] = {"p50_us": float(np.percentile(lat, 50)),
-                         "p99_us": float(np.percentile(lat, 99)),
-                         "mean_us": float(lat.mean()),
-                         "queries_per_s": float(sizes.sum() / (wall / 1e6)),
-                         "max_in_flight": st["max_in_flight"], "slots": st["slots"]}
-    tree.close()
-    return {
-        "workload": (f"2^{args.learned_keys_log2} unique u64 keys = cumsum(floor(lognormal(4,2))+1), "
-                     f"value = rank; batch of 2^{args.queries_log2} queries, 90% hits uniform over "
-                     "ranks, 10% uniform in [min, max]"),
-        "plain": {"value": nq / (plain_ms / 1e3), "unit": "queries/s", "ms": plain_ms,
-                  "lanes_per_query": lanes_p, "rounds": rounds_p},
-        "learned": {"value": nq / (l_ms / 1e3), "unit": "queries/s", "ms": l_ms,
-                    "lanes_per_query": best[0], "rounds": best[1],
-                    "windowed": windowed, "fallback": fallback,
-                    "roofline": {"bound": "hbm", "achieved": alg / (l_ms / 1e3) / 1e9,
-                                 "peak": peak, "unit": "GB/s",
-                                 "frac": alg / (l_ms / 1e3) / 1e9 / peak}},
-        "learned_over_plain": plain_ms / l_ms,
-        "exact": exact,
-        "model": {k: rep[k] for k in ("root_loss_initial", "root_loss_final", "eps_mean",
-                                      "eps_max", "window_lines_mean", "train_ms",
-                                      "keys_per_entry")},
-        "serving": {"requests": int(len(reqs)), "rate_per_s": args.serve_rate,
-                    "batch_sizes": "round(2^U), U ~ uniform[0,16]", **serving},
-    }
+        res["plain" if mode == "basic" else "learned"] = {
+            "p50_us": float(np.percentile(lat, 50)), "p99_us": float(np.percentile(lat, 99)),
+            "mean_us": float(lat.mean()), "queries_per_s": float(sizes.sum() / (wall / 1e6)),
+            "max_in_flight": st["max_in_flight"], "slots": st["slots"]}
+    return res
 
 
 # ------------------------------------------------ forest and rectangles ----
@@ -390,8 +350,8 @@ def forest_section(args, device, bt, flush):
     """Batched uneven forest workload: 4096 trees of round(2^U), U ~ [10, 20], u32
     keys; per tree round(2^U), U ~ [6, 16], point queries (80% hits) plus 1%
     range queries of width [1, 2^12] ranks; every batch is one launch of a
-    captured CUDA graph.  The plan's lanes/rounds and tile are chosen by
-    timing the candidates."""
+    captured CUDA graph.  The plan's lanes/rounds and tile come from the
+    autotuner (autotune.tune_forest)."""
     import torch
     wl = importlib.import_module(PKG + ".workloads")
     keys, vals, koff, q, qoff, lo, hi, roff = wl.forest(num_trees=args.forest_trees)
@@ -401,15 +361,9 @@ def forest_section(args, device, bt, flush):
     dlo, dhi = torch.from_numpy(lo).to(device), torch.from_numpy(hi).to(device)
     out = torch.empty(len(q), dtype=torch.uint32, device=device)
     counts = torch.empty(len(lo), dtype=torch.uint64, device=device)
-    tried = {}
-    for cfg in ((4, 1), (8, 1), (8, 2)):
-        for tile in (512, 2048, 8192):
-            with f.plan(dq, qoff, out, dlo, dhi, roff, counts, *cfg, tile=tile) as p:
-                p.run(stream)
-                tried[f"{cfg[0]}x{cfg[1]}/t{tile}"] = _timed_ms(lambda: p.run(stream), stream, flush, 3)
-    best = min(tried, key=tried.get)
-    lanes, rounds = (int(x) for x in best.split("/")[0].split("x"))
-    tile = int(best.split("/t")[1])
+    at = importlib.import_module(PKG + ".autotune")
+    lanes, rounds, tile, tried = at.tune_forest(f, dq, qoff, out, dlo, dhi, roff, counts,
+                                                flush=flush)
     with f.plan(dq, qoff, out, dlo, dhi, roff, counts, lanes, rounds, tile=tile) as p:
         l0 = bt.kernel_launches()
         ms = _timed_ms(lambda: p.run(stream), stream, flush, args.steps)
@@ -596,29 +550,30 @@ def rect_section(args, device, bt, flush):
     }
 
 
-# ------------------------------------------------------------ GPU leg -------
+# ------------------------------------------- radix-grouped configuration ----
 
-def run_ours(args):
+def grouped_section(args, device, bt, flush, stream, rank=0):
+    """Radix-grouped point search (2^26 unique uniform u32 keys, value =
+    rank; 2^24 queries, 90% keys by Zipf(0.99) rank through a random rank
+    permutation, 10% uniform u32; grouped by the top 8 key bits, then
+    searched), beside the ungrouped basic search of the same batch and the
+    grouped search through the host-buffer C-ABI call.  Returns the section
+    and the tree (for the range section) and its keys."""
     import torch
-    rank, world, local_rank = dist_env()
-    torch.cuda.set_device(local_rank)
-    device = torch.device("cuda", local_rank)
-    dist = init_dist(world, local_rank)
-    bt = importlib.import_module(PKG)
     L = bt.lib()
-
-    keys, vals, q = workload(args.keys_log2, args.queries_log2, rank)
+    keys, vals, q = zipf_workload(args.grouped_keys_log2, args.queries_log2, rank)
     nq = len(q)
-    stream = torch.cuda.current_stream(device)
     tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
     dq = torch.from_numpy(q).to(device)
     grouped = torch.empty_like(dq)
     perm = torch.empty(nq, dtype=torch.uint32, device=device)
     out = torch.empty(nq, dtype=torch.uint32, device=device)
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
-
     P = ctypes.c_void_p
     sp = P(stream.cuda_stream)
+    at = importlib.import_module(PKG + ".autotune")
+    b_lanes, b_slots, _ = at.tune(tree, dq, mode="basic", repeats=3)
+    g_lanes, g_slots, _ = at.tune(tree, dq, mode="grouped", repeats=3)
+    tree.set_search_config(g_lanes, g_slots)
 
     def group_into():
         bt._check(L.bt_group_queries(tree.handle, P(dq.data_ptr()), nq, P(grouped.data_ptr()),
@@ -629,69 +584,30 @@ def run_ours(args):
                                                   P(perm.data_ptr()), nq, P(out.data_ptr()), sp),
                   "search")
 
-    def search_basic():
-        bt._check(L.bt_point_search(tree.handle, 0, P(dq.data_ptr()), nq, P(out.data_ptr()), sp),
-                  "basic")
-
-    # clocks are sampled from here (GPU busy with tuning and warm-up) through
-    # the end of the timed region, which alone is shorter than one sample
-    clocks = ClockSampler(local_rank)
-    clocks.start()
-    # the project's autotuner picks the kernel shape per mode (untimed)
-    at = importlib.import_module(PKG + ".autotune")
-    b_lanes, b_slots, b_ms = at.tune(tree, dq, mode="basic", repeats=3)
-    g_lanes, g_slots, g_ms = at.tune(tree, dq, mode="grouped", repeats=3)
-
-    # warm-up (the result is compared with the CPU leg's sample on rank 0)
-    for _ in range(max(args.warmup, 3)):
+    for _ in range(3):
         group_into()
         search_grouped()
     torch.cuda.synchronize(device)
     res = out.cpu().numpy()
     hits = int(np.count_nonzero(res != np.uint32(0xFFFFFFFF)))
-    checked = None
-
-    # ---- timed region: K grouped steps, device time per step ----------------
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
-    barrier(dist, device)
-    torch.cuda.synchronize(device)
-    launches0 = L.bt_kernel_launches()
-    nvtx = torch.cuda.nvtx
-    for i in range(args.steps):
+    steps = max(3, args.steps)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    for i in range(steps):
         flush.zero_()
-        nvtx.range_push("timed_grouped")
         ev[i][0].record(stream)
         group_into()
         ev[i][1].record(stream)
         search_grouped()
         ev[i][2].record(stream)
-        nvtx.range_pop()
     torch.cuda.synchronize(device)
-    launches = L.bt_kernel_launches() - launches0
-    barrier(dist, device)
-    clk = clocks.stop()
-    step_ms = [ev[i][0].elapsed_time(ev[i][2]) for i in range(args.steps)]
-    search_ms = [ev[i][1].elapsed_time(ev[i][2]) for i in range(args.steps)]
-    group_ms = [ev[i][0].elapsed_time(ev[i][1]) for i in range(args.steps)]
-    ms = max_over_ranks(statistics.mean(step_ms), dist, device)
-    value = world * nq / (ms / 1000.0)
-
-    # ---- ungrouped basic search, same batch (the plain path) ----------------
+    step_ms = statistics.mean(e[0].elapsed_time(e[2]) for e in ev)
+    search_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    group_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
     tree.set_search_config(b_lanes, b_slots)
-    for _ in range(2):
-        search_basic()
-    bev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
-    for i in range(args.steps):
-        flush.zero_()
-        nvtx.range_push("timed_basic")
-        bev[i][0].record(stream)
-        search_basic()
-        bev[i][1].record(stream)
-        nvtx.range_pop()
-    torch.cuda.synchronize(device)
-    basic_ms = max_over_ranks(statistics.mean(b[0].elapsed_time(b[1]) for b in bev), dist, device)
-
-    # ---- end to end through the host-buffer C-ABI call ----------------------
+    basic_ms = _timed_ms(lambda: bt._check(L.bt_point_search(tree.handle, 0, P(dq.data_ptr()), nq,
+                                                             P(out.data_ptr()), sp), "basic"),
+                         stream, flush, steps)
+    # end to end: the grouped search through host buffers
     tree.set_search_config(g_lanes, g_slots)
     hq = torch.from_numpy(q).pin_memory()
     hout = torch.empty(nq, dtype=torch.uint32).pin_memory()
@@ -699,44 +615,265 @@ def run_ours(args):
     for _ in range(2):
         bt._check(L.bt_point_search_host(tree.handle, 1, hq_p, nq, hout_p, sp), "e2e")
     e2e_t = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         flush.zero_()
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         bt._check(L.bt_point_search_host(tree.handle, 1, hq_p, nq, hout_p, sp), "e2e")
         e2e_t.append(time.perf_counter() - t0)
-    e2e_s = max_over_ranks(statistics.mean(e2e_t), dist, device)
-    e2e_ok = bool(np.array_equal(hout.numpy(), res))
-
-    # ---- roofline of the dominant kernel (the grouped search kernel) --------
     kb = vb = 4
-    # per launch: key in, value out, the leaf block's key sector, and its
-    # value sector on a hit
-    alg_bytes = nq * (kb + vb + 32) + hits * 32
-    search_s = statistics.mean(search_ms) / 1000.0
-    achieved = alg_bytes / search_s / 1e9
-    peak, peak_kind = measured_peak()
-    # the ceiling for one random leaf-block read per query: random 64-byte
-    # reads over a region the size of the tree's leaves, measured here
+    alg = nq * (kb + vb + 32) + hits * 32
+    peak, _ = measured_peak()
     leaf_bytes = -(-len(keys) // (32 // kb)) * 64
     gather_rps = bt.measure_gather(leaf_bytes, 1 << 24, 64)
     tq = profiled_traffic("point_kernel_grouped_zipf_k26_q24")
+    sec = {
+        "workload": (f"radix-grouped point search: 2^{args.grouped_keys_log2} unique uniform u32 "
+                     f"keys (value = rank), batches of 2^{args.queries_log2} queries, 90% keys by "
+                     "Zipf(0.99) rank, 10% uniform u32; grouped by the top 8 key bits"),
+        "value": nq / (step_ms / 1e3), "unit": "queries/s", "ms_per_step": step_ms,
+        "breakdown_ms": {"group": group_ms, "search": search_ms},
+        "plain_basic": {"value": nq / (basic_ms / 1e3), "unit": "queries/s", "ms": basic_ms},
+        "e2e": {"value": nq / statistics.mean(e2e_t), "unit": "queries/s",
+                "h2d_bytes_per_step": nq * kb, "d2h_bytes_per_step": nq * vb,
+                "api": "bt_point_search_host (grouped), pinned host buffers",
+                "matches_device_result": bool(np.array_equal(hout.numpy(), res))},
+        "roofline": {"bound": "hbm", "kernel": "point_window_kernel (grouped batch)",
+                     "achieved": alg / (search_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (search_ms / 1e3) / 1e9 / peak,
+                     "traffic": None if tq is None else tq * nq,
+                     "traffic_source": "ncu dram bytes per query of the grouped search kernel "
+                                       "(profiles/search_kernels_zipf_k26_q22.md) x queries",
+                     "random_gather_ceiling": {"reads_per_s": gather_rps, "block_bytes": 64,
+                                               "frac": nq / (search_ms / 1e3) / gather_rps}},
+        "autotune": {"grouped": [g_lanes, g_slots], "basic": [b_lanes, b_slots]},
+        "hit_fraction": hits / nq,
+    }
+    return sec, tree, keys
 
-    ranges = range_section(args, device, bt, flush, tree, keys) if world == 1 else None
-    build = build_section(device, bt, keys, vals) if world == 1 else None
-    learned = forest = rect = None
-    if world == 1 and not args.no_learned:
-        learned = learned_section(args, device, bt, flush)
-    if world == 1 and not args.no_forest:
-        forest = forest_section(args, device, bt, flush)
-    if world == 1 and not args.no_rect:
-        rect = rect_section(args, device, bt, flush)
+
+def small_section(args, device, bt, flush, stream):
+    """The L2-resident basic search: 2^20 unique uniform u32 keys (value =
+    rank), 2^20 queries, even slots existing keys, odd slots uniform u32."""
+    import torch
+    wl = importlib.import_module(PKG + ".workloads")
+    keys, vals, q = wl.point_uniform(1 << 20, 1 << 20)
+    tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
+    dq = torch.from_numpy(q).to(device)
+    out = torch.empty(len(q), dtype=torch.uint32, device=device)
+    at = importlib.import_module(PKG + ".autotune")
+    lanes, rounds, _ = at.tune(tree, dq, mode="basic", repeats=3)
+    ms = _timed_ms(lambda: tree.point_search(dq, mode="basic", out=out, stream=stream), stream,
+                   flush, max(5, args.steps))
+    res = out.cpu().numpy()
+    from oracle.oracle import Oracle
+    ok = bool(np.array_equal(res, Oracle().point_search(keys, vals, q)))
+    tree.close()
+    return {"workload": "2^20 unique uniform u32 keys (value = rank), 2^20 queries: 50% keys, "
+                        "50% uniform u32; basic search; L2 flushed before every step",
+            "value": len(q) / (ms / 1e3), "unit": "queries/s", "ms": ms,
+            "lanes_per_query": lanes, "rounds": rounds, "equals_oracle": ok}
+
+
+def reference_gpu_section(args):
+    """The reference's own kernels on this GPU (its .cu sources compiled for
+    sm_100a into oracle/_ref/libbtref.so, launched with its wrappers' launch
+    shapes; kernel time only, median of 5 after one warm-up).  Keys are padded
+    with keys above the largest to a multiple of 5000 (the reference's last
+    leaf is always full, main.cu:126-129); the grouped kernel runs with value
+    = key (its leaf compares data[], BPTreeExactSearch.cu:269-276)."""
+    from oracle.oracle import REF_LIB, RefHarness
+    if not os.path.exists(REF_LIB):
+        return {"unavailable": "oracle/_ref/libbtref.so not built"}
+    wl = importlib.import_module(PKG + ".workloads")
+    h = RefHarness()
+
+    def pad(keys):
+        keys = keys.astype(np.uint64)
+        extra = (-len(keys)) % 5000
+        return np.concatenate([keys, keys[-1] + 1 + np.arange(extra, dtype=np.uint64)])
+
+    def med(fn, reps=5):
+        fn()
+        ts = []
+        for _ in range(reps):
+            fn()
+            ts.append(h.last_ms)
+        return statistics.median(ts)
+
+    res = {}
+    try:
+        keys, vals, q = wl.point_uniform(1 << 20, 1 << 20)
+        k = pad(keys)
+        h.build(k, np.arange(len(k), dtype=np.uint64))
+        ms = med(lambda: h.point_basic(q))
+        res["small_basic"] = {"kernel": "kernelSearchingNaiveOneStep (BPTreeExactSearch.cu:25)",
+                              "queries": len(q), "ms": ms, "queries_per_s": len(q) / (ms / 1e3)}
+        keys, vals, q = zipf_workload(args.grouped_keys_log2, args.queries_log2, 0)
+        k = pad(keys)
+        h.build(k, np.arange(len(k), dtype=np.uint64))
+        ms = med(lambda: h.point_basic(q))
+        res["grouped_config_basic"] = {
+            "kernel": "kernelSearchingNaiveOneStep (BPTreeExactSearch.cu:25)",
+            "queries": len(q), "ms": ms, "queries_per_s": len(q) / (ms / 1e3)}
+        lo, hi = wl.range_queries(keys, 1 << 22, 64)
+        ms = med(lambda: h.range_basic(lo, hi))
+        res["range_basic"] = {
+            "kernel": "kernelSearchingKeyRangeGroupStateTwo x2 + kernelGenerateSearchResult "
+                      "(BtreeRangeSearch.cu:215, :297)",
+            "ranges": len(lo), "ms": ms, "ranges_per_s": len(lo) / (ms / 1e3)}
+        h.build(k, k)  # value = key for the grouped kernel
+        qg = q[: 1 << 22]
+        ms = med(lambda: h.point_grouped(qg), reps=3)
+        res["grouped_config_grouped"] = {
+            "kernel": "kernelSearchingKeyGroupTwoStep (BPTreeExactSearch.cu:207), kernel only "
+                      "(its grouping runs on the host)",
+            "queries": len(qg), "ms": ms, "queries_per_s": len(qg) / (ms / 1e3)}
+        keys, vals, q = lognormal_workload(args.keys_log2, args.queries_log2, 0)
+        k = pad(keys)
+        h.build(k, np.arange(len(k), dtype=np.uint64))
+        ms = med(lambda: h.point_basic(q))
+        res["learned_config_basic"] = {
+            "kernel": "kernelSearchingNaiveOneStep (BPTreeExactSearch.cu:25)",
+            "queries": len(q), "ms": ms, "queries_per_s": len(q) / (ms / 1e3)}
+    finally:
+        h.free()
+    return res
+
+
+# ------------------------------------------------------------ GPU leg -------
+
+def run_ours(args):
+    import torch
+    rank, world, local_rank = dist_env()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    dist = init_dist(world, local_rank)
+    bt = importlib.import_module(PKG)
+    L = bt.lib()
+    P = ctypes.c_void_p
+
+    keys, vals, q = lognormal_workload(args.keys_log2, args.queries_log2, rank)
+    nq = len(q)
+    stream = torch.cuda.current_stream(device)
+    sp = P(stream.cuda_stream)
+    tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
+    rep = tree.learned_train(num_segments=1 << args.segments_log2)
+    dq = torch.from_numpy(q).to(device)
+    out = torch.empty(nq, dtype=torch.uint64, device=device)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    def search_learned():
+        bt._check(L.bt_point_search(tree.handle, 2, P(dq.data_ptr()), nq, P(out.data_ptr()), sp),
+                  "learned")
+
+    def search_plain():
+        bt._check(L.bt_point_search(tree.handle, 0, P(dq.data_ptr()), nq, P(out.data_ptr()), sp),
+                  "plain")
+
+    # clocks are sampled from here (GPU busy with tuning and warm-up) through
+    # the end of the timed region
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    at = importlib.import_module(PKG + ".autotune")
+    p_lanes, p_rounds, _ = at.tune(tree, dq, mode="basic", repeats=3)
+    for _ in range(max(args.warmup, 3)):
+        search_learned()
+    torch.cuda.synchronize(device)
+    learned_res = out.cpu().numpy()
+    hits = int(np.count_nonzero(learned_res != np.uint64(0xFFFFFFFFFFFFFFFF)))
+
+    # ---- timed region: K learned steps, device time per step ----------------
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    barrier(dist, device)
+    torch.cuda.synchronize(device)
+    launches0 = L.bt_kernel_launches()
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        search_learned()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(device)
+    launches = L.bt_kernel_launches() - launches0
+    barrier(dist, device)
+    clk = clocks.stop()
+    step_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    ms = max_over_ranks(statistics.mean(step_ms), dist, device)
+    value = world * nq / (ms / 1000.0)
+    extra, fallback = tree.learned_last_stats()
+
+    # ---- the plain tree search of the same batch ----------------------------
+    for _ in range(2):
+        search_plain()
+    pev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        pev[i][0].record(stream)
+        search_plain()
+        pev[i][1].record(stream)
+    torch.cuda.synchronize(device)
+    plain_ms = max_over_ranks(statistics.mean(e[0].elapsed_time(e[1]) for e in pev), dist, device)
+    plain_res = out.cpu().numpy()
+
+    # ---- end to end through the host-buffer C-ABI call ----------------------
+    hq = torch.from_numpy(q).pin_memory()
+    hout = torch.empty(nq, dtype=torch.uint64).pin_memory()
+    hq_p, hout_p = P(hq.data_ptr()), P(hout.data_ptr())
+    for _ in range(2):
+        bt._check(L.bt_point_search_host(tree.handle, 2, hq_p, nq, hout_p, sp), "e2e")
+    e2e_t = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        bt._check(L.bt_point_search_host(tree.handle, 2, hq_p, nq, hout_p, sp), "e2e")
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = max_over_ranks(statistics.mean(e2e_t), dist, device)
+    e2e_ok = bool(np.array_equal(hout.numpy(), learned_res))
+
+    # ---- roofline of the learned search kernel -----------------------------
+    kb = vb = 8
+    # per query: key in, value out, the key's 32-byte sector and, on a hit,
+    # its value's sector
+    alg_bytes = nq * (kb + vb + 32) + hits * 32
+    kernel_s = statistics.mean(step_ms) / 1e3  # this GPU's launches
+    achieved = alg_bytes / kernel_s / 1e9
+    peak, peak_kind = measured_peak()
+    leaf_bytes = -(-len(keys) // 4) * 64
+    chain = {f"{l}_line": bt.measure_chain(max(rep["index_bytes"], 1 << 20), leaf_bytes, 1 << 24,
+                                           128, l, 2) for l in (1, 2)}
+    tq = profiled_traffic("learned_kernel_lognormal_k28_q24")
+
+    sections = {}
+    if world == 1:
+        sections["serving"] = serving_section(args, bt, tree, keys, (p_lanes, p_rounds),
+                                              (p_lanes, p_rounds)) if not args.no_serving else None
+    tree.close()
+    del dq, out
+    if world == 1:
+        sections["small"] = small_section(args, device, bt, flush, stream)
+        if not args.no_grouped:
+            g, gtree, gkeys = grouped_section(args, device, bt, flush, stream)
+            sections["grouped"] = g
+            sections["ranges"] = range_section(args, device, bt, flush, gtree, gkeys)
+            gtree.close()
+            sections["build"] = build_section(device, bt, gkeys, np.arange(len(gkeys), dtype=np.uint32))
+        if not args.no_forest:
+            sections["forest"] = forest_section(args, device, bt, flush)
+        if not args.no_rect:
+            sections["rectangles"] = rect_section(args, device, bt, flush)
+        if not args.no_reference_gpu:
+            torch.cuda.synchronize(device)
+            torch.cuda.empty_cache()
+            sections["reference_gpu"] = reference_gpu_section(args)
 
     line = None
     if rank == 0:
         cpu = None
+        checked = None
         if world == 1 and not args.no_cpu_baseline:
-            qps_refc, qps_lb, sample, checked = cpu_refc_qps(keys, vals, q, args.cpu_sample_log2, res)
+            qps_refc, qps_lb, sample, checked = cpu_refc_qps(keys, vals, q, args.cpu_sample_log2,
+                                                             learned_res)
             cpu = {"value": qps_refc, "unit": "queries/s", "cores": os.cpu_count(),
                    "kind": "port",
                    "sample": f"{sample} queries of the batch, reference page tree (fanout 5000) "
@@ -745,44 +882,45 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
             "data": "synthetic (seeded)", "config": workload_desc(args),
             "e2e": {"value": world * nq / e2e_s, "unit": "queries/s",
                     "h2d_bytes_per_step": nq * kb, "d2h_bytes_per_step": nq * vb,
-                    "api": "bt_point_search_host (grouped), pinned host buffers",
+                    "api": "bt_point_search_host(BT_POINT_LEARNED), pinned host buffers",
                     "matches_device_result": e2e_ok},
+            "plain": {"value": world * nq / (plain_ms / 1e3), "unit": "queries/s",
+                      "ms_per_step": plain_ms, "lanes_per_query": p_lanes, "rounds": p_rounds,
+                      "api": "bt_point_search(BT_POINT_BASIC)"},
+            "learned_over_plain": plain_ms / ms,
+            "learned_equals_plain": bool(np.array_equal(learned_res, plain_res)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": None if tq is None else tq * nq,
-                         "kernel": "point_window_kernel (grouped batch)",
+                         "traffic_source": "ncu dram bytes per query of learned_kernel "
+                                           "(profiles/learned_kernel_lognormal_2e28.md) x queries",
+                         "kernel": "learned_kernel",
                          "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel_ms": statistics.mean(search_ms),
-                         "random_gather_ceiling": {
-                             "reads_per_s": gather_rps, "block_bytes": 64,
-                             "region_bytes": leaf_bytes,
-                             "search_queries_per_s": nq / search_s,
-                             "frac": nq / search_s / gather_rps}},
+                         "kernel_ms": statistics.mean(step_ms),
+                         "chain_ceiling": {
+                             "queries_per_s": chain,
+                             "what": "random 128-byte index line(s) from an L2-sized array of "
+                                     "the index's size, then one dependent random 128-byte leaf "
+                                     "read (btp_measure_chain)",
+                             "frac_1_line": nq / kernel_s / chain["1_line"]}},
+            "learned_index": {k: rep[k] for k in ("num_segments", "max_error", "eps_max", "eps_mean",
+                                                  "root_error", "root_error_initial",
+                                                  "root_loss_initial", "root_loss_final",
+                                                  "code_lines_mean", "index_bytes",
+                                                  "keys_per_unit", "train_ms")},
+            "learned_stats": {"extra_unit_reads": extra, "full_descents": fallback},
             "cpu_baseline": cpu,
+            "cpu_sample_matches_gpu": checked,
             "clocks": clk,
             "gpu_launches": int(launches),
-            "breakdown_ms": {"group": statistics.mean(group_ms),
-                             "search": statistics.mean(search_ms)},
-            "plain_basic": {"value": world * nq / (basic_ms / 1000.0), "unit": "queries/s",
-                            "ms_per_step": basic_ms},
             "hit_fraction": hits / nq,
-            "autotune": {"grouped": {"lanes_per_query": g_lanes, "queries_per_group": g_slots,
-                                     "ms": g_ms},
-                         "basic": {"lanes_per_query": b_lanes, "queries_per_group": b_slots,
-                                   "ms": b_ms}},
-            "cpu_sample_matches_gpu": checked,
-            "learned_index": learned,
-            "forest": forest,
-            "rectangles": rect,
-            "ranges": ranges,
-            "build": build,
+            **sections,
         }
         print(json.dumps(line), flush=True)
-    tree.close()
     if dist is not None:
         dist.destroy_process_group()
     return 0
@@ -793,9 +931,19 @@ def run_only(args):
     bt = importlib.import_module(PKG)
     device = torch.device("cuda:0")
     torch.cuda.set_device(device)
+    stream = torch.cuda.current_stream(device)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
-    fn = {"learned": learned_section, "forest": forest_section, "rect": rect_section}[args.only]
-    print(json.dumps(fn(args, device, bt, flush)), flush=True)
+    if args.only == "learned":
+        return run_ours(argparse.Namespace(**{**vars(args), "no_serving": True, "no_grouped": True,
+                                              "no_forest": True, "no_rect": True,
+                                              "no_reference_gpu": True, "no_cpu_baseline": True}))
+    if args.only == "grouped":
+        sec = grouped_section(args, device, bt, flush, stream)[0]
+    elif args.only == "small":
+        sec = small_section(args, device, bt, flush, stream)
+    else:
+        sec = {"forest": forest_section, "rect": rect_section}[args.only](args, device, bt, flush)
+    print(json.dumps(sec), flush=True)
     return 0
 
 

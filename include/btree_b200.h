@@ -55,7 +55,9 @@ typedef enum bt_status {
 
 typedef enum bt_point_mode {
     BT_POINT_BASIC = 0,  /* SearchingBTreeGPUOnlyOneState, BPTreeExactSearch.cu:409 */
-    BT_POINT_GROUPED = 1 /* SearchingBTreeGPUCombineStep, BPTreeExactSearch.cu:602 */
+    BT_POINT_GROUPED = 1, /* SearchingBTreeGPUCombineStep, BPTreeExactSearch.cu:602 */
+    BT_POINT_LEARNED = 2  /* through the tree's learned index (bt_learned_train); no
+                             counterpart in the reference */
 } bt_point_mode;
 
 typedef enum bt_range_mode {
@@ -202,7 +204,9 @@ BT_API bt_status bt_point_search_grouped_batch(const bt_tree *tree, const void *
  * to 262144 per call (larger batches: BT_ERR_INVALID_ARGUMENT).  All calls on
  * a device share that array: calls that overlap on the GPU race.  The first
  * call on each device looks up the array's address; make it before any
- * stream capture.
+ * stream capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset (which ends the context it belongs to) this entry point
+ * must not be called again on that device.
  */
 BT_API bt_status bt_point_search_grouped_noalloc(const bt_tree *tree, const void *d_queries,
                                                  uint64_t nq, void *d_out, void *stream);
@@ -315,8 +319,9 @@ typedef struct bt_learned_report {
 BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, void *stream,
                                   bt_learned_report *report);
 
-/* Point search through the learned index (same results as bt_point_search).
- * BT_ERR_INVALID_ARGUMENT if the tree has no trained index. */
+/* Point search through the learned index: bt_point_search(BT_POINT_LEARNED)
+ * (same results as the other modes).  BT_ERR_INVALID_ARGUMENT if the tree has
+ * no trained index. */
 BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
                                          void *d_out, void *stream);
 
@@ -431,6 +436,17 @@ BT_API bt_status bt_server_replay(bt_server *srv, uint64_t nreq, const uint64_t 
 /* Number of kernel launches this library has issued in this process (all
  * devices, all threads).  Lets a caller count the device work behind a call. */
 BT_API uint64_t bt_kernel_launches(void);
+
+/* Number of scratch allocations this library has made from its memory pool
+ * in this process (all devices, all threads).  Lets a caller check that a
+ * call allocated nothing. */
+BT_API uint64_t bt_workspace_allocations(void);
+
+/* Number of times a grouping or sorting pass on the current device gave up
+ * waiting for the digit counts of an earlier tile (its look-back is bounded;
+ * a correct launch never gives up, and a pass that did has wrong output).
+ * Synchronous; all-ones if it cannot be read. */
+BT_API uint64_t bt_partition_lookback_timeouts(void);
 
 #ifdef __cplusplus
 }

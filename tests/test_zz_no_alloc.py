@@ -46,7 +46,12 @@ def test_noalloc_matches_grouped_search_twice(bt, cuda, kt, vt):
             expected = t.point_search(dq, mode="grouped").cpu().numpy()
             out = torch.empty(nq, dtype={4: torch.uint32, 8: torch.uint64}[t.value_bytes],
                               device=cuda)
+            torch.cuda.synchronize()
+            allocs = bt.lib().bt_workspace_allocations()
             assert _noalloc(bt, t, dq, out) == 0, bt.lib().bt_last_error()
+            torch.cuda.synchronize()
+            # the call took no scratch from the library's pool
+            assert bt.lib().bt_workspace_allocations() == allocs
             assert np.array_equal(out.cpu().numpy(), expected), f"call {call}"
 
 
