@@ -58,11 +58,13 @@ def test_single_rank_needs_no_process_group():
 
 
 @pytest.mark.parametrize("rank", [0, 1, 3])
-def test_replica_batches_differ_per_rank(rank, monkeypatch, tmp_path):
+@pytest.mark.parametrize("which", ["lognormal_workload", "zipf_workload"])
+def test_replica_batches_differ_per_rank(rank, which, monkeypatch, tmp_path):
     """Weak scaling: each rank answers its own batch over the same keys."""
     import bench
     monkeypatch.setattr(bench.tempfile, "gettempdir", lambda: str(tmp_path))
-    k0, v0, q0 = bench.workload(12, 10, 0)
-    k, v, q = bench.workload(12, 10, rank)
+    make = getattr(bench, which)
+    k0, v0, q0 = make(12, 10, 0)
+    k, v, q = make(12, 10, rank)
     assert (k == k0).all() and (v == v0).all()
     assert (q == q0).all() == (rank == 0)
