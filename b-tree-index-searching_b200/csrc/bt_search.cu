@@ -317,6 +317,162 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
     }
 }
 
+// Range bounds with the upper bound taken from the lower bound's path.
+// A narrow range usually ends in the same bottom separator line as it
+// starts: while the group walks lo down, it counts that line's separators
+// <= hi as well (the line is already in its registers), which gives hi's
+// leaf block whenever the line's last separator is above hi; both leaf
+// blocks are then read together.  Only the queries whose range leaves that
+// line take a second descent, compacted per warp into as few rounds as they
+// need.  Same results as bounds_kernel.
+template <typename K, typename V, int G, int R, bool PERM>
+__global__ void __launch_bounds__(kThreads, 2)
+bounds_line_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
+                   const K *__restrict__ hi, const uint32_t *__restrict__ perm, uint64_t nq,
+                   uint64_t *__restrict__ counts, uint64_t *__restrict__ lb_out) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    K *s_lvl = reinterpret_cast<K *>(smem_raw);
+    stage_level<K>(s_lvl, t);
+    __syncthreads();
+
+    using LG = LeafGeom<K, V>;
+    constexpr int F = kLineBytes / (int)sizeof(K);
+    constexpr int KPL = F / G;
+    constexpr int NB = KPL * (int)sizeof(K);
+    constexpr int NG = 32 / G;
+    constexpr int I = G / R;
+    const int lane = threadIdx.x & 31;
+    const int grp = lane / G;
+    const int gl = lane % G;
+    uint64_t *res = reinterpret_cast<uint64_t *>(smem_raw + scratch_offset(t)) + (threadIdx.x >> 5) * 64;
+    const K tmax = (K)t.max_key;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    const K *gseps = static_cast<const K *>(t.seps);
+    const int bottom = t.nlevels - 1;
+    // the staged level is the bottom one for small trees: no line to share
+    const bool share = t.smem_level < bottom;
+    const uint64_t ntiles = (nq + 31) / 32;
+    const uint64_t per_cta = PERM ? (ntiles + gridDim.x - 1) / gridDim.x : 0;
+    const uint64_t t_begin = PERM ? blockIdx.x * per_cta + (threadIdx.x >> 5)
+                                  : (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t t_end = PERM ? min(ntiles, (blockIdx.x + 1) * per_cta) : ntiles;
+    const uint64_t t_step = PERM ? (blockDim.x >> 5) : ((uint64_t)gridDim.x * blockDim.x) >> 5;
+
+    for (uint64_t tile = t_begin; tile < t_end; tile += t_step) {
+        const uint64_t base = tile * 32;
+        const uint64_t my = base + lane;
+        const bool v = my < nq;
+        const K a = v ? lo[my] : (K)0;
+        const K b = v ? hi[my] : (K)0;
+        const K qa = a <= tmax ? a : tmax;
+        const K qb = b < tmax ? b : tmax;
+        const uint32_t na = smem_bound<K>(s_lvl, t.smem_entries, qa, false);
+        // hi >= the largest key: the upper bound is n, no walk
+        const bool hi_open = v && b < tmax;
+        // ---- lower bounds, and upper bounds that end in the same bottom line
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            K qe[2 * I];
+            bool up[2 * I];
+            uint32_t node[2 * I];
+            bool hin[I];
+#pragma unroll
+            for (int s = 0; s < I; s++) {
+                const int k = r * (NG * I) + s * NG + grp;
+                qe[s] = __shfl_sync(0xffffffffu, qa, k);
+                qe[I + s] = __shfl_sync(0xffffffffu, qb, k);
+                node[s] = __shfl_sync(0xffffffffu, na, k);
+                up[s] = false;
+                up[I + s] = true;
+                hin[s] = false;
+            }
+            for (int lvl = t.smem_level + 1; lvl < bottom; lvl++) {
+                K qs[I];
+                bool us[I];
+                uint32_t ns[I];
+#pragma unroll
+                for (int s = 0; s < I; s++) {
+                    qs[s] = qe[s];
+                    us[s] = false;
+                    ns[s] = node[s];
+                }
+                level_step<K, G, I>(gseps + t.lvl_off[lvl], qs, us, ns, grp, gl);
+#pragma unroll
+                for (int s = 0; s < I; s++) node[s] = ns[s];
+            }
+            if (share) {
+                // bottom line: separators < lo and <= hi from the same registers
+                uint32_t c[I][NB / 4];
+#pragma unroll
+                for (int s = 0; s < I; s++)
+                    load_bytes<NB>(gseps + t.lvl_off[bottom] + (size_t)node[s] * F + gl * KPL, c[s]);
+#pragma unroll
+                for (int s = 0; s < I; s++) {
+                    const int cl = group_count<G, G, KPL>(count_below<K, KPL>(c[s], qe[s], false), true, grp);
+                    const int ch = group_count<G, G, KPL>(count_below<K, KPL>(c[s], qe[I + s], true), true, grp);
+                    hin[s] = ch < F;  // the line's last separator is above hi
+                    // (otherwise read lo's block again: ch = F may be past the last block)
+                    node[I + s] = node[s] * F + (uint32_t)(hin[s] ? ch : cl);
+                    node[s] = node[s] * F + (uint32_t)cl;
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < I; s++) node[I + s] = node[s];
+            }
+            int pos[2 * I];
+            leaf_bound<K, V, G, 2 * I>(leaves, node, qe, up, grp, gl, pos);
+#pragma unroll
+            for (int s = 0; s < I; s++) {
+                const int k = r * (NG * I) + s * NG + grp;
+                if (gl == 0) {
+                    res[k] = (uint64_t)node[s] * LG::S + pos[s];
+                    res[32 + k] = hin[s] ? (uint64_t)node[I + s] * LG::S + pos[I + s] : ~0ull;
+                }
+            }
+        }
+        __syncwarp();
+        // ---- the remaining upper bounds: full descents, compacted
+        const bool need = hi_open && res[32 + lane] == ~0ull;
+        const unsigned needm = __ballot_sync(0xffffffffu, need);
+        if (needm) {
+            const uint32_t nb = need ? smem_bound<K>(s_lvl, t.smem_entries, qb, true) : 0u;
+            const int nneed = __popc(needm);
+            for (int r0 = 0; r0 < nneed; r0 += NG * I) {
+                K qe[I];
+                bool up[I];
+                uint32_t node[I];
+                int who[I];
+#pragma unroll
+                for (int s = 0; s < I; s++) {
+                    const int j = r0 + s * NG + grp;  // j-th query that needs a descent
+                    unsigned m = needm;               // its lane (the first one as filler)
+                    for (int z = 0; z < (j < nneed ? j : 0); z++) m &= m - 1;
+                    const int src = __ffs(m) - 1;
+                    who[s] = j < nneed ? src : -1;
+                    qe[s] = __shfl_sync(0xffffffffu, qb, src);
+                    node[s] = __shfl_sync(0xffffffffu, nb, src);
+                    up[s] = true;
+                }
+                walk_global<K, G, I>(t, qe, up, node, grp, gl);
+                int pos[I];
+                leaf_bound<K, V, G, I>(leaves, node, qe, up, grp, gl, pos);
+#pragma unroll
+                for (int s = 0; s < I; s++)
+                    if (gl == 0 && who[s] >= 0) res[32 + who[s]] = (uint64_t)node[s] * LG::S + pos[s];
+            }
+        }
+        __syncwarp();
+        if (v) {
+            const uint64_t lb = a <= tmax ? res[lane] : t.n;
+            const uint64_t ub = b < tmax ? res[32 + lane] : t.n;
+            const uint64_t dst = PERM ? (uint64_t)perm[my] : my;
+            counts[dst] = (a <= b && ub > lb) ? ub - lb : 0;
+            if (lb_out) lb_out[dst] = lb;
+        }
+        __syncwarp();
+    }
+}
+
 // Empty tree: every point query misses, every range is empty.
 template <typename V>
 __global__ void fill_kernel(V *out, uint64_t n, V v) {
@@ -422,7 +578,7 @@ template <typename K, typename V, int G, int R, bool PERM>
 bt_status bounds_launch(const bt_tree *t, const void *d_lo, const void *d_hi,
                         const uint32_t *d_perm, uint64_t nq, uint64_t *d_counts, uint64_t *d_lb,
                         cudaStream_t s) {
-    auto fn = bounds_kernel<K, V, G, R, PERM>;
+    auto fn = bounds_line_kernel<K, V, G, R, PERM>;
     const size_t smem = scratch_offset(t->dev) + (size_t)kWarps * 64 * sizeof(uint64_t);
     bt_status st = set_smem(fn, smem);
     if (st != BT_OK) return st;

@@ -67,7 +67,7 @@ def parse_args(argv=None):
     p.add_argument("--no-rect", action="store_true", help="skip the rectangle-search section")
     p.add_argument("--rect-boxes-log2", type=int, default=20, help="boxes in the rectangle section")
     p.add_argument("--forest-trees", type=int, default=4096, help="trees in the forest section")
-    p.add_argument("--only", choices=["learned", "grouped", "forest", "rect", "small"],
+    p.add_argument("--only", choices=["learned", "grouped", "ranges", "forest", "rect", "small"],
                    help="run one extension section alone on cuda:0 and print its JSON object "
                         "(for profiling; not the bench line)")
     return p.parse_args(argv)
@@ -937,8 +937,11 @@ def run_only(args):
         return run_ours(argparse.Namespace(**{**vars(args), "no_serving": True, "no_grouped": True,
                                               "no_forest": True, "no_rect": True,
                                               "no_reference_gpu": True, "no_cpu_baseline": True}))
-    if args.only == "grouped":
-        sec = grouped_section(args, device, bt, flush, stream)[0]
+    if args.only in ("grouped", "ranges"):
+        sec, gtree, gkeys = grouped_section(args, device, bt, flush, stream)
+        if args.only == "ranges":
+            sec = range_section(args, device, bt, flush, gtree, gkeys)
+        gtree.close()
     elif args.only == "small":
         sec = small_section(args, device, bt, flush, stream)
     else:
