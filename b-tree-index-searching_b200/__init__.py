@@ -125,6 +125,8 @@ _PROTOS = {
     "bt_learned_last_stats": (_I, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "bt_mlp_loss_grad": (_I, [_P, ctypes.c_uint32, _P, _P, _U64, _P, _P, _P]),
     "bt_rect_search": (_I, [_P, _P, _P, _P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64), _P]),
+    "bt_rect_search_mode": (_I, [_P, _I, _P, _P, _P, _P, _U64, _P, _P, _P, _U64,
+                                 ctypes.POINTER(_U64), _P]),
     "bt_forest_build": (_I, [_P, _P, _P, ctypes.c_uint32, _I, _I, _P, ctypes.POINTER(_P)]),
     "bt_forest_destroy": (_I, [_P]),
     "bt_forest_plan_create": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, ctypes.c_uint32,
@@ -574,24 +576,26 @@ class Server:
             pass
 
 
-def rect_search(tree, x0, y0, x1, y1, stream=None):
+def rect_search(tree, x0, y0, x1, y1, stream=None, mode="basic"):
     """Points of a Morton-keyed tree inside boxes [x0,x1] x [y0,y1] (u16 CUDA
-    tensors): (counts, offsets, ids sorted per box)."""
+    tensors): (counts, offsets, ids sorted per box).  mode "2d" / "zorder"
+    processes the boxes grouped by the cell of their corner (same output)."""
     import torch
     L = lib()
     n = len(x0)
+    m = RANGE_MODES[mode]
     x0, y0, x1, y1 = (t.contiguous() for t in (x0, y0, x1, y1))
     counts = torch.empty(n, dtype=torch.uint64, device=x0.device)
     offsets = torch.empty(n, dtype=torch.uint64, device=x0.device)
     total = ctypes.c_uint64(0)
-    args = (tree.handle, _P(x0.data_ptr()), _P(y0.data_ptr()), _P(x1.data_ptr()), _P(y1.data_ptr()),
-            n, _P(counts.data_ptr()), _P(offsets.data_ptr()))
-    st = L.bt_rect_search(*args, None, 0, ctypes.byref(total), _stream_ptr(stream))
+    args = (tree.handle, m, _P(x0.data_ptr()), _P(y0.data_ptr()), _P(x1.data_ptr()),
+            _P(y1.data_ptr()), n, _P(counts.data_ptr()), _P(offsets.data_ptr()))
+    st = L.bt_rect_search_mode(*args, None, 0, ctypes.byref(total), _stream_ptr(stream))
     if st not in (0, 5):
-        _check(st, "bt_rect_search")
+        _check(st, "bt_rect_search_mode")
     ids = torch.empty(max(1, total.value), dtype=_torch_dtype(tree.value_bytes), device=x0.device)
-    _check(L.bt_rect_search(*args, _P(ids.data_ptr()), total.value, ctypes.byref(total),
-                            _stream_ptr(stream)), "bt_rect_search")
+    _check(L.bt_rect_search_mode(*args, _P(ids.data_ptr()), total.value, ctypes.byref(total),
+                                 _stream_ptr(stream)), "bt_rect_search_mode")
     return counts, offsets, ids[: total.value]
 
 

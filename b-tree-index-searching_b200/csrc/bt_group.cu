@@ -740,6 +740,29 @@ bt_status sort_pairs_impl(const K *d_keys, const V *d_vals, uint64_t n, K *out_k
     return st;
 }
 
+bt_status order_u16_impl(const uint32_t *d_keys, uint64_t n, uint32_t *d_perm, cudaStream_t s) {
+    const uint64_t ntiles = (n + kPTile - 1) / kPTile;
+    const size_t sweep_bytes = (SweepWs::bytes(ntiles) + 255) / 256 * 256;
+    const size_t b = (n * sizeof(uint32_t) + 255) / 256 * 256;
+    unsigned char *ws = nullptr;
+    bt_status st = ws_alloc((void **)&ws, sweep_bytes + 3 * b, s);
+    if (st != BT_OK) return st;
+    SweepWs sw;
+    sw.carve(ws);
+    uint32_t *k0 = reinterpret_cast<uint32_t *>(ws + sweep_bytes);
+    uint32_t *k1 = reinterpret_cast<uint32_t *>(ws + sweep_bytes + b);
+    uint32_t *p0 = reinterpret_cast<uint32_t *>(ws + sweep_bytes + 2 * b);
+    uint32_t *ok[2] = {k0, k1};
+    uint32_t *op[2] = {p0, d_perm};
+    GroupKeyParams gp;
+    gp.kind = kPartRadix;
+    gp.cbits = 8;
+    gp.shift = 0;
+    st = sweep_passes<uint32_t, false>(d_keys, nullptr, n, gp, 2, ok, nullptr, op, sw, s);
+    ws_free(ws, s);
+    return st;
+}
+
 // Single-pass point partition into caller-provided memory (no allocation):
 // counts and scan scratch come from `ws` (partition_ws_bytes bytes).
 template <typename K>
@@ -947,6 +970,12 @@ bt_status launch_sort_pairs(int key_bytes, int value_bytes, const void *d_keys, 
                                                      (uint64_t *)out_keys, (uint32_t *)out_vals, s)
                : sort_pairs_impl<uint64_t, uint64_t>((const uint64_t *)d_keys, (const uint64_t *)d_vals, n,
                                                      (uint64_t *)out_keys, (uint64_t *)out_vals, s);
+}
+
+bt_status launch_order_u16(const uint32_t *d_keys, uint64_t n, uint32_t *d_perm, cudaStream_t s) {
+    if (n == 0) return BT_OK;
+    if (n >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "ordering needs n < 2^32");
+    return order_u16_impl(d_keys, n, d_perm, s);
 }
 
 size_t partition_point_ws_bytes(uint64_t nq) {

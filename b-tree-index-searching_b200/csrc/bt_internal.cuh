@@ -218,6 +218,9 @@ bt_status launch_range_fill(const bt_tree *t, const uint64_t *d_lb, const uint64
 // order.  n < 2^32; outputs must not alias inputs.
 bt_status launch_sort_pairs(int key_bytes, int value_bytes, const void *d_keys, const void *d_vals,
                             uint64_t n, void *out_keys, void *out_vals, cudaStream_t s);
+// Stable order of n 16-bit keys (the low halves of d_keys): d_perm[g] = the
+// index of the item in position g (two 8-bit passes of the partition).
+bt_status launch_order_u16(const uint32_t *d_keys, uint64_t n, uint32_t *d_perm, cudaStream_t s);
 // Sorts each segment ids[offsets[i] .. + counts[i]) ascending (value width
 // of t).  small_sorted: segments of up to 256 values are sorted already.
 bt_status launch_segment_sort(const bt_tree *t, const uint64_t *d_counts, const uint64_t *d_offsets,

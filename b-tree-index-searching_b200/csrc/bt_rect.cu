@@ -157,8 +157,8 @@ template <typename V>
 __global__ void __launch_bounds__(kRThreads, 2)
 rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
                   const uint16_t *__restrict__ y0s, const uint16_t *__restrict__ x1s,
-                  const uint16_t *__restrict__ y1s, uint64_t nr, uint64_t *__restrict__ counts,
-                  uint2 *__restrict__ runs) {
+                  const uint16_t *__restrict__ y1s, const uint32_t *__restrict__ order, uint64_t nr,
+                  uint64_t *__restrict__ counts, uint2 *__restrict__ runs) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t *s_lvl = reinterpret_cast<uint32_t *>(smem_raw);
     uint32_t *res = reinterpret_cast<uint32_t *>(smem_raw + (((size_t)t.smem_bytes + 15) / 16 * 16)) +
@@ -169,12 +169,14 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
     const int lane = threadIdx.x & 31;
     const int j = lane % kMaxCells;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nr;
-         i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+    for (uint64_t g = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; g < nr;
+         g += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        // box i in position g of the processing order; runs follow that order
+        const uint64_t i = order ? (uint64_t)order[g] : g;
         const uint32_t x0 = x0s[i], y0 = y0s[i], x1 = x1s[i], y1 = y1s[i];
         if (x0 > x1 || y0 > y1) {  // empty box (warp-uniform)
             if (lane == 0) counts[i] = 0;
-            if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2(0u, 0u);
+            if (lane < kMaxCells) runs[g * kMaxCells + lane] = make_uint2(0u, 0u);
             continue;
         }
         const ZBox box(x0, y0, x1, y1);
@@ -203,7 +205,7 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
             for (int h = 0; h < 2; h++) c += __popc(__ballot_sync(0xffffffffu, act[h] && box.holds(key[h])));
         }
         if (lane == 0) counts[i] = c;
-        if (lane < kMaxCells) runs[i * kMaxCells + lane] = make_uint2(b, len);
+        if (lane < kMaxCells) runs[g * kMaxCells + lane] = make_uint2(b, len);
     }
 }
 
@@ -215,7 +217,8 @@ template <typename V>
 __global__ void __launch_bounds__(kRThreads)
 rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__ x0s,
                  const uint16_t *__restrict__ y0s, const uint16_t *__restrict__ x1s,
-                 const uint16_t *__restrict__ y1s, uint64_t nr, const uint2 *__restrict__ runs,
+                 const uint16_t *__restrict__ y1s, const uint32_t *__restrict__ order, uint64_t nr,
+                 const uint2 *__restrict__ runs,
                  const uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                  V *__restrict__ ids) {
     __shared__ V s_buf[kRWarps][kWarpSortCap];
@@ -224,14 +227,15 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
     const unsigned lt = (1u << lane) - 1u;
     V *buf = s_buf[threadIdx.x >> 5];
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    for (uint64_t i = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; i < nr;
-         i += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+    for (uint64_t g = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; g < nr;
+         g += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
+        const uint64_t i = order ? (uint64_t)order[g] : g;
         const uint32_t x0 = x0s[i], y0 = y0s[i], x1 = x1s[i], y1 = y1s[i];
         const uint64_t cnt = counts[i];
         if (x0 > x1 || y0 > y1 || cnt == 0) continue;
         const ZBox box(x0, y0, x1, y1);
         const Cell cell = box_cell(x0, y0, x1, y1, lane % kMaxCells);
-        const uint2 run = lane < kMaxCells ? runs[i * kMaxCells + lane] : make_uint2(0u, 0u);
+        const uint2 run = lane < kMaxCells ? runs[g * kMaxCells + lane] : make_uint2(0u, 0u);
         const bool buffered = cnt <= (uint64_t)kWarpSortCap;
         V *dst = buffered ? buf : ids + offsets[i];
         uint32_t T;
@@ -268,10 +272,24 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
     }
 }
 
+// Group key of every box: the 256 x 256 cell of its corner (x0, y0), as a
+// row-major cell index (2-D grouping) or the Morton code of the cell (Z-order
+// grouping) -- the two reorderings the reference applies to its 1-D range
+// queries (grouping2d.cu, zOrder2d.cu:27-54), here on the boxes themselves.
+__global__ void rect_group_key_kernel(const uint16_t *__restrict__ x0s,
+                                      const uint16_t *__restrict__ y0s, uint64_t nr, int zorder,
+                                      uint32_t *__restrict__ key) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nr;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t cx = (uint32_t)x0s[i] >> 8, cy = (uint32_t)y0s[i] >> 8;
+        key[i] = zorder ? (spread16d(cx) | (spread16d(cy) << 1)) : ((cy << 8) | cx);
+    }
+}
+
 template <typename V>
-bt_status rect_impl(const bt_tree *t, const uint16_t *x0, const uint16_t *y0, const uint16_t *x1,
-                    const uint16_t *y1, uint64_t nr, uint64_t *counts, uint64_t *offsets,
-                    void *ids, uint64_t cap, uint64_t *h_total, cudaStream_t s) {
+bt_status rect_impl(const bt_tree *t, int mode, const uint16_t *x0, const uint16_t *y0,
+                    const uint16_t *x1, const uint16_t *y1, uint64_t nr, uint64_t *counts,
+                    uint64_t *offsets, void *ids, uint64_t cap, uint64_t *h_total, cudaStream_t s) {
     const size_t smem = ((size_t)t->dev.smem_bytes + 15) / 16 * 16 + (size_t)kRWarps * 32 * sizeof(uint32_t);
     auto kc = rect_count_kernel<V>;
     auto kf = rect_fill_kernel<V>;
@@ -281,17 +299,27 @@ bt_status rect_impl(const bt_tree *t, const uint16_t *x0, const uint16_t *y0, co
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kc, kRThreads, smem);
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((nr + kRWarps - 1) / kRWarps, (uint64_t)sm_count() * std::max(per_sm, 1)));
-    uint2 *runs = nullptr;
-    uint64_t *d_total = nullptr;
-    bt_status st = ws_alloc((void **)&runs, nr * kMaxCells * sizeof(uint2), s);
+    WsGuard g_runs(s), g_total(s), g_order(s), g_key(s);
+    bt_status st = g_runs.alloc(nr * kMaxCells * sizeof(uint2));
+    if (st == BT_OK) st = g_total.alloc(sizeof(uint64_t));
     if (st != BT_OK) return st;
-    st = ws_alloc((void **)&d_total, sizeof(uint64_t), s);
-    if (st != BT_OK) {
-        ws_free(runs, s);
-        return st;
+    uint2 *runs = g_runs.as<uint2>();
+    uint64_t *d_total = g_total.as<uint64_t>();
+    const uint32_t *order = nullptr;
+    if (mode != BT_RANGE_BASIC) {  // process the boxes in grouped order
+        st = g_order.alloc(nr * sizeof(uint32_t));
+        if (st == BT_OK) st = g_key.alloc(nr * sizeof(uint32_t));
+        if (st != BT_OK) return st;
+        count_launch();
+        rect_group_key_kernel<<<(unsigned)std::min<uint64_t>((nr + 255) / 256, (uint64_t)sm_count() * 8),
+                                256, 0, s>>>(x0, y0, nr, mode == BT_RANGE_ZORDER, g_key.as<uint32_t>());
+        BT_CUDA(cudaGetLastError());
+        st = launch_order_u16(g_key.as<uint32_t>(), nr, g_order.as<uint32_t>(), s);
+        if (st != BT_OK) return st;
+        order = g_order.as<uint32_t>();
     }
     count_launch();
-    kc<<<grid, kRThreads, smem, s>>>(t->dev, x0, y0, x1, y1, nr, counts, runs);
+    kc<<<grid, kRThreads, smem, s>>>(t->dev, x0, y0, x1, y1, order, nr, counts, runs);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) st = cuda_fail(e, "rectangle count pass");
     if (st == BT_OK) st = launch_scan_u64(counts, offsets, nr, d_total, s);
@@ -311,14 +339,13 @@ bt_status rect_impl(const bt_tree *t, const uint16_t *x0, const uint16_t *y0, co
             const unsigned fgrid = (unsigned)std::max<uint64_t>(
                 1, std::min<uint64_t>((nr + kRWarps - 1) / kRWarps, (uint64_t)sm_count() * 4));
             count_launch();
-            kf<<<fgrid, kRThreads, 0, s>>>(t->dev, x0, y0, x1, y1, nr, runs, counts, offsets, (V *)ids);
+            kf<<<fgrid, kRThreads, 0, s>>>(t->dev, x0, y0, x1, y1, order, nr, runs, counts, offsets,
+                                           (V *)ids);
             e = cudaGetLastError();
             if (e != cudaSuccess) st = cuda_fail(e, "rectangle fill pass");
             if (st == BT_OK) st = launch_segment_sort(t, counts, offsets, nr, ids, s, true);
         }
     }
-    ws_free(d_total, s);
-    ws_free(runs, s);
     return st;
 }
 
@@ -331,8 +358,19 @@ bt_status bt_rect_search(const bt_tree *t, const uint16_t *x0, const uint16_t *y
                          const uint16_t *x1, const uint16_t *y1, uint64_t nr, uint64_t *counts,
                          uint64_t *offsets, void *ids, uint64_t cap, uint64_t *h_total,
                          void *stream) {
+    return bt_rect_search_mode(t, BT_RANGE_BASIC, x0, y0, x1, y1, nr, counts, offsets, ids, cap,
+                               h_total, stream);
+}
+
+bt_status bt_rect_search_mode(const bt_tree *t, int mode, const uint16_t *x0, const uint16_t *y0,
+                              const uint16_t *x1, const uint16_t *y1, uint64_t nr,
+                              uint64_t *counts, uint64_t *offsets, void *ids, uint64_t cap,
+                              uint64_t *h_total, void *stream) {
     using namespace bt;
     if (!t) return fail(BT_ERR_INVALID_ARGUMENT, "tree is NULL");
+    if (mode != BT_RANGE_BASIC && mode != BT_RANGE_GROUPED_2D && mode != BT_RANGE_ZORDER)
+        return fail(BT_ERR_INVALID_ARGUMENT, "unknown rectangle mode");
+    if (nr >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "nr must be below 2^32");
     if (!h_total) return fail(BT_ERR_INVALID_ARGUMENT, "h_total is NULL");
     *h_total = 0;
     if (t->key_bytes != 4)
@@ -353,8 +391,9 @@ bt_status bt_rect_search(const bt_tree *t, const uint16_t *x0, const uint16_t *y
         return e == cudaSuccess ? BT_OK : cuda_fail(e, "rectangle search on an empty tree");
     }
     const bt_status st =
-        t->val_bytes == 4 ? rect_impl<uint32_t>(t, x0, y0, x1, y1, nr, counts, offsets, ids, cap, h_total, s)
-                          : rect_impl<uint64_t>(t, x0, y0, x1, y1, nr, counts, offsets, ids, cap, h_total, s);
+        t->val_bytes == 4
+            ? rect_impl<uint32_t>(t, mode, x0, y0, x1, y1, nr, counts, offsets, ids, cap, h_total, s)
+            : rect_impl<uint64_t>(t, mode, x0, y0, x1, y1, nr, counts, offsets, ids, cap, h_total, s);
     if (prev != t->device) cudaSetDevice(prev);
     return st;
 }

@@ -241,14 +241,29 @@ BT_API bt_status bt_range_search(const bt_tree *tree, int mode, const void *d_lo
  * bits, y in the odd bits), its values point IDs; rectangle i is
  * [x0,x1] x [y0,y1] inclusive.  Outputs as bt_range_search: counts, offsets
  * and, for each rectangle, the IDs of the points inside sorted ascending.
- * Scans the Z interval [Z(x0,y0), Z(x1,y1)] and jumps over runs of keys
- * outside the box with the BIGMIN computation of Tropf & Herzog (1981).
+ * Each box is covered by at most 16 aligned square cells (each cell is one
+ * contiguous run of Morton codes, found by a lower and an upper bound);
+ * cells inside the box count whole, the keys of cells on its edge are
+ * tested one by one.
  * BT_ERR_INVALID_ARGUMENT unless the tree has 4-byte keys.
  */
 BT_API bt_status bt_rect_search(const bt_tree *tree, const uint16_t *d_x0, const uint16_t *d_y0,
                                 const uint16_t *d_x1, const uint16_t *d_y1, uint64_t nr,
                                 uint64_t *d_counts, uint64_t *d_offsets, void *d_ids,
                                 uint64_t ids_capacity, uint64_t *h_total, void *stream);
+
+/* bt_rect_search with the boxes processed in a grouped order (no counterpart
+ * in the reference; its 2-D and Z-order groupings reorder 1-D range queries,
+ * grouping2d.cu:24-31, zOrder2d.cu:27-54): mode BT_RANGE_GROUPED_2D orders
+ * them by the 256 x 256 cell of their corner (x0, y0) row by row,
+ * BT_RANGE_ZORDER by the Morton code of that cell, BT_RANGE_BASIC keeps the
+ * input order.  Boxes of one cell then run together and share their keys in
+ * cache.  Outputs are the same in every mode, in the caller's order. */
+BT_API bt_status bt_rect_search_mode(const bt_tree *tree, int mode, const uint16_t *d_x0,
+                                     const uint16_t *d_y0, const uint16_t *d_x1,
+                                     const uint16_t *d_y1, uint64_t nr, uint64_t *d_counts,
+                                     uint64_t *d_offsets, void *d_ids, uint64_t ids_capacity,
+                                     uint64_t *h_total, void *stream);
 
 /* Range count with host buffers (pipelined like bt_point_search_host). */
 BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *h_lo,

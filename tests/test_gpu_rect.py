@@ -29,10 +29,26 @@ def test_rect_search_matches_oracle(bt, orc, wl, cuda, npts, grid, vt):
     x0[:4], y0[:4], x1[:4], y1[:4] = [0, 7, 9, 65000], [0, 7, 3, 65000], [65535, 7, 8, 65535], [65535, 7, 3, 65535]
     ec, eo, ei = orc.rect_search(zs, idss.astype(np.uint32), x0, y0, x1, y1)
     with bt.Tree.build(dev(zs, cuda), dev(idss, cuda)) as t:
-        c, off, got = bt.rect_search(t, dev(x0, cuda), dev(y0, cuda), dev(x1, cuda), dev(y1, cuda))
-    assert np.array_equal(c.cpu().numpy(), ec)
-    assert np.array_equal(off.cpu().numpy(), eo)
-    assert np.array_equal(got.cpu().numpy().astype(np.uint64), ei.astype(np.uint64))
+        for mode in ("basic", "2d", "zorder"):  # box orders: outputs identical
+            c, off, got = bt.rect_search(t, dev(x0, cuda), dev(y0, cuda), dev(x1, cuda),
+                                         dev(y1, cuda), mode=mode)
+            assert np.array_equal(c.cpu().numpy(), ec), mode
+            assert np.array_equal(off.cpu().numpy(), eo), mode
+            assert np.array_equal(got.cpu().numpy().astype(np.uint64), ei.astype(np.uint64)), mode
+
+
+def test_rect_search_rejects_unknown_mode(bt, cuda):
+    import ctypes
+    import torch
+    keys = np.arange(10, dtype=np.uint32)
+    with bt.Tree.build(dev(keys, cuda), dev(keys, cuda)) as t:
+        u = torch.zeros(1, dtype=torch.uint16, device=cuda)
+        c = torch.zeros(1, dtype=torch.uint64, device=cuda)
+        P = ctypes.c_void_p
+        tot = ctypes.c_uint64(0)
+        st = bt.lib().bt_rect_search_mode(t.handle, 7, *(P(u.data_ptr()),) * 4, 1, P(c.data_ptr()),
+                                          P(c.data_ptr()), None, 0, ctypes.byref(tot), None)
+        assert st == 1
 
 
 def test_rect_search_needs_32bit_keys(bt, cuda):
