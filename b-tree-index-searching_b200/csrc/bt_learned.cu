@@ -64,6 +64,7 @@ constexpr int kHullCap = 32;                 // points per convex hull
 constexpr int kLThreads = 512;               // search CTA (one per SM: the staged keys)
 constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
 constexpr int kMaxWalk = 8;                  // extra units read before the full descent
+constexpr int kLearnedNQ = 2;                // queries in flight per 4-lane group
 
 // ---------------------------------------------------------------- model ---
 
@@ -408,13 +409,13 @@ __device__ V tree_point(const DevTree &t, K q) {
 }
 
 // One warp tile = 32 queries; a group of 4 lanes owns queries grp, grp + 8,
-// grp + 16, grp + 24 of the tile and keeps all four in flight.
-template <typename K, typename V>
+// grp + 16, grp + 24 of the tile and keeps NQ of them in flight (4 / NQ
+// passes per tile).
+template <typename K, typename V, int NQ>
 __global__ void __launch_bounds__(kLThreads, 1)
 learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
                const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
     using LG = LeafGeom<K, V>;
-    constexpr int NQ = 4;                       // queries per group
     constexpr int KPU = unit_keys<K, V>();      // keys per unit
     constexpr int BPU = kUnitBytes / LG::BS;    // blocks per unit (1 or 2)
     extern __shared__ uint4 smem_l[];
@@ -452,12 +453,14 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             const uint32_t b = (uint32_t)min((int)m.nls - 1, pl + e);
             my_sl = stage_search<K>(s_stage, a, b, myq);
         }
+#pragma unroll 1
+        for (int hf = 0; hf < 4 / NQ; hf++) {
         K qv[NQ];
         bool live[NQ];
         uint32_t w[NQ][8];
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
-            const int k = s * 8 + grp;
+            const int k = (hf * NQ + s) * 8 + grp;
             qv[s] = __shfl_sync(0xffffffffu, myq, k);
             live[s] = base + k < nq;
             const uint32_t sl = __shfl_sync(0xffffffffu, my_sl, k);
@@ -614,7 +617,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                         vw = (byte % 32) / 4;
                     }
                     if (!found) {
-                        if (gl == 0) out[base + s * 8 + grp] = key_max<V>();
+                        if (gl == 0) out[base + (hf * NQ + s) * 8 + grp] = key_max<V>();
                     } else if (gl == vl) {
                         V val;
                         if constexpr (sizeof(V) == 4) {
@@ -628,7 +631,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                             for (int k = 2; k < 8; k += 2)
                                 if (k == vw) val = ((uint64_t)u[s][k + 1] << 32) | u[s][k];
                         }
-                        out[base + s * 8 + grp] = val;
+                        out[base + (hf * NQ + s) * 8 + grp] = val;
                     }
                     pend[s] = false;
                 } else if (walk) {
@@ -638,7 +641,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 if (lost || (walk && it == kMaxWalk)) {
                     // outside the window: the tree's full descent
                     if (gl == 0) {
-                        out[base + s * 8 + grp] = tree_point<K, V>(t, qv[s]);
+                        out[base + (hf * NQ + s) * 8 + grp] = tree_point<K, V>(t, qv[s]);
                         n_fallback++;
                     }
                     pend[s] = false;
@@ -649,6 +652,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             for (int s = 0; s < NQ; s++) any |= pend[s];
             if (!__any_sync(0xffffffffu, any)) break;
         }
+        }  // passes of the tile
     }
     if (m.stats && (n_extra | n_fallback)) {
         atomicAdd(&m.stats[0], n_extra);
@@ -660,7 +664,7 @@ template <typename K, typename V>
 bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
                          cudaStream_t s) {
     const LearnedDev &m = t->learned->dev;
-    auto fn = learned_kernel<K, V>;
+    auto fn = learned_kernel<K, V, kLearnedNQ>;
     const size_t smem = (size_t)m.stage_bytes + (3 * kMaxHidden + 1) * sizeof(float);
     static int set_for[64] = {0};
     int dev = t->device;

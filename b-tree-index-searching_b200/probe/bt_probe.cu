@@ -8,7 +8,8 @@
 //                       lanes, L1 bypassed) over a region: the ceiling of a
 //                       kernel that makes one random DRAM read per query.
 //   btp_measure_chain   per query, 1 or 2 random 128-byte line reads from an
-//                       L2-sized array (the L2-resident part of an index),
+//                       L2-sized array (the L2-resident part of an index;
+//                       sizes are rounded down to powers of two),
 //                       then one random block read from a large region whose
 //                       address depends on the loaded line (the leaf read).
 //                       Shows how the random DRAM rate holds up while a given
@@ -92,7 +93,7 @@ chain_kernel(const unsigned char *__restrict__ lines, uint64_t nlines,
             const uint64_t h = splitmix64(seed + i0 + s);
             w[s] = 0;
             if (CL > 0 && nlines) {
-                const uint64_t li = h % nlines;
+                const uint64_t li = h & (nlines - 1);
 #pragma unroll
                 for (int c = 0; c < CL; c++) {
                     const uint64_t l = li + c < nlines ? li + c : li;
@@ -104,7 +105,7 @@ chain_kernel(const unsigned char *__restrict__ lines, uint64_t nlines,
 #pragma unroll
         for (int s = 0; s < I; s++) {
             const uint64_t h2 = splitmix64(~(seed + i0 + s));
-            const uint64_t b = (h2 ^ (uint64_t)(w[s] & mask)) % nblocks;
+            const uint64_t b = (h2 ^ (uint64_t)(w[s] & mask)) & (nblocks - 1);
             if (LB == 128 || gl < LB / 16) {
                 const uint4 y = ld_evict_first(leaves + b * LB + gl * 16);
                 acc ^= y.x ^ y.y ^ y.z ^ y.w;
@@ -228,8 +229,11 @@ __attribute__((visibility("default"))) int btp_measure_chain(uint64_t line_bytes
     if (lines_per_query > 2 || (lines_per_query > 0 && line_bytes < 128))
         return fail("lines_per_query must be 0, 1 or 2 (with line_bytes >= 128)", cudaSuccess);
     if (in_flight != 1 && in_flight != 2) return fail("in_flight must be 1 or 2", cudaSuccess);
-    const uint64_t nlines = lines_per_query ? line_bytes / 128 : 0;
-    const uint64_t nblocks = leaf_bytes / leaf_read;
+    // power-of-two counts: the kernel indexes with masks (a 64-bit modulo
+    // per query would make the probe instruction bound)
+    auto pow2_floor = [](uint64_t v) { return v ? 1ull << (63 - __builtin_clzll(v)) : 0ull; };
+    const uint64_t nlines = lines_per_query ? pow2_floor(line_bytes / 128) : 0;
+    const uint64_t nblocks = pow2_floor(leaf_bytes / leaf_read);
     if (nblocks == 0 || n_queries == 0 || n_queries > (1ull << 30) || nlines > (1ull << 32))
         return fail("sizes out of range", cudaSuccess);
     Bufs b;

@@ -448,6 +448,8 @@ def range_section(args, device, bt, flush, tree, keys):
     stream = torch.cuda.current_stream(device)
     dlo, dhi = torch.from_numpy(lo).to(device), torch.from_numpy(hi).to(device)
     cnt = torch.empty(nr, dtype=torch.uint64, device=device)
+    at = importlib.import_module(PKG + ".autotune")
+    r_lanes, r_rounds, r_ms = at.tune(tree, dlo, mode="range", hi=dhi, repeats=3)
     res = {}
     counts_ref = None
     for mode in ("basic", "2d", "zorder"):
@@ -474,9 +476,10 @@ def range_section(args, device, bt, flush, tree, keys):
     return {
         "workload": "2^26 u32 keys (value = rank), 2^22 ranges of width uniform [1, 64] ranks",
         "counts": res, "counts_equal_rank_difference": counts_ok,
+        "autotune": {"lanes_per_query": r_lanes, "rounds": r_rounds, "ms": r_ms},
         "ids": {"ranges_per_s": nr / (ms_ids / 1e3), "ms": ms_ids, "hits": hits,
                 "api": "Tree.range_search (counts, scan, offsets, ID fill)"},
-        "roofline": {"bound": "hbm", "kernel": "bounds_kernel (basic counts)",
+        "roofline": {"bound": "hbm", "kernel": "bounds_line_kernel (basic counts)",
                      "achieved": alg / (base_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (base_ms / 1e3) / 1e9 / peak},
     }
