@@ -123,6 +123,7 @@ _PROTOS = {
                               ctypes.POINTER(bt_learned_report)]),
     "bt_point_search_learned": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_last_stats": (_I, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
+    "bt_learned_set_shape": (_I, [_P, ctypes.c_uint32]),
     "bt_mlp_loss_grad": (_I, [_P, ctypes.c_uint32, _P, _P, _U64, _P, _P, _P]),
     "bt_rect_search": (_I, [_P, _P, _P, _P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64), _P]),
     "bt_rect_search_mode": (_I, [_P, _I, _P, _P, _P, _P, _U64, _P, _P, _P, _U64,
@@ -324,7 +325,7 @@ class Tree:
 
     # -- learned position model -------------------------------------------
     def learned_train(self, num_segments=65536, max_error=0, hidden=16, iterations=400,
-                      learning_rate=0.01, stream=None):
+                      learning_rate=0.002, stream=None):
         """Build the learned index of this tree (segmentation, root training,
         unit thresholds); returns the report as a dict."""
         cfg = bt_learned_config(num_segments, max_error, hidden, iterations, learning_rate)
@@ -343,6 +344,10 @@ class Tree:
                                              _P(out.data_ptr()), _stream_ptr(stream)),
                "bt_point_search_learned")
         return out
+
+    def learned_set_shape(self, queries_in_flight):
+        """Learned search kernel shape: 1 or 2 queries in flight per lane group."""
+        _check(lib().bt_learned_set_shape(self._h, queries_in_flight), "bt_learned_set_shape")
 
     def learned_last_stats(self):
         """(leaf units read beyond the first, queries that took the full descent)."""

@@ -19,6 +19,8 @@ import os
 import statistics
 
 SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
+# learned search: (lanes per query, queries in flight per lane group)
+LEARNED_SHAPES = ((4, 1), (4, 2))
 
 
 def _key(tree, mode, nq):
@@ -45,16 +47,21 @@ def _time(fn, stream, repeats):
 def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, configs=SEARCH_CONFIGS):
     """Pick and set the fastest search configuration for `tree` on this batch.
 
-    mode: "basic" / "grouped" (point search; `queries` a CUDA tensor), or
-    "range" (`queries` = lo, `hi` = hi).  Returns (lanes, slots, {cfg: ms}).
+    mode: "basic" / "grouped" / "learned" (point search; `queries` a CUDA
+    tensor), or "range" (`queries` = lo, `hi` = hi).  Returns (lanes, slots,
+    {cfg: ms}); for "learned", slots is the learned kernel's queries in
+    flight per lane group.
     """
     import torch
+    set_cfg = tree.set_search_config
+    if mode == "learned":
+        set_cfg = lambda g, i: tree.learned_set_shape(i)  # noqa: E731
     key = _key(tree, mode, len(queries))
     if cache_path and os.path.exists(cache_path):
         with open(cache_path) as f:
             cached = json.load(f).get(key)
         if cached:
-            tree.set_search_config(*cached["best"])
+            set_cfg(*cached["best"])
             return cached["best"][0], cached["best"][1], cached["ms"]
     stream = torch.cuda.current_stream(queries.device)
     out = None
@@ -62,6 +69,11 @@ def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, confi
         out = torch.empty(len(queries), dtype={4: torch.uint32, 8: torch.uint64}[tree.value_bytes],
                           device=queries.device)
         fn = lambda: tree.point_search(queries, mode=mode, out=out, stream=stream)  # noqa: E731
+    elif mode == "learned":
+        out = torch.empty(len(queries), dtype={4: torch.uint32, 8: torch.uint64}[tree.value_bytes],
+                          device=queries.device)
+        fn = lambda: tree.point_search(queries, mode="learned", out=out, stream=stream)  # noqa: E731
+        configs = LEARNED_SHAPES
     elif mode == "range":
         out = torch.empty(len(queries), dtype=torch.uint64, device=queries.device)
         fn = lambda: tree.range_count(queries, hi, out=out, stream=stream)  # noqa: E731
@@ -69,11 +81,11 @@ def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, confi
         raise ValueError(mode)
     ms = {}
     for g, i in configs:
-        tree.set_search_config(g, i)
+        set_cfg(g, i)
         ms[f"{g}x{i}"] = _time(fn, stream, repeats)
     best = min(ms, key=ms.get)
     g, i = (int(x) for x in best.split("x"))
-    tree.set_search_config(g, i)
+    set_cfg(g, i)
     if cache_path:
         data = {}
         if os.path.exists(cache_path):

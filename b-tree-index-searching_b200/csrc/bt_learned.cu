@@ -8,7 +8,8 @@
 // is on chip (shared memory and L2):
 //
 //   1. root (shared memory): a monotone MLP y = b2 + sum_j w2[j] *
-//      relu(w1[j] * x + b1[j]) (w1, w2 >= 0) of the normalised key predicts
+//      ramp(w1[j] * x + b1[j]) (ramp = clamp to [0, 1]; w1, w2 >= 0) of the
+//      normalised key predicts
 //      the key's segment line among the nls lines; its worst error root_err
 //      over the lines' first keys bounds a binary search over those keys,
 //      staged in shared memory, to 2 * root_err + 3 entries.
@@ -44,6 +45,7 @@ struct LearnedState {
     void *d_stage = nullptr;
     unsigned long long *d_stats = nullptr;
     uint64_t bytes = 0;
+    int in_flight = 2;  // queries in flight per lane group (bt_learned_set_shape)
     LearnedDev dev;
 };
 
@@ -61,20 +63,29 @@ namespace {
 
 constexpr uint64_t kPlaChunk = 1ull << 14;  // keys per segmentation thread
 constexpr int kHullCap = 32;                 // points per convex hull
-constexpr int kLThreads = 512;               // search CTA (one per SM: the staged keys)
 constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
 constexpr int kMaxWalk = 8;                  // extra units read before the full descent
-constexpr int kLearnedNQ = 2;                // queries in flight per 4-lane group
+// Search CTA shapes (one CTA per SM: the staged keys): NQ queries in flight
+// per 4-lane group, 1024 / NQ threads -- the register budget of either shape
+// holds the kernel without spills.
+template <int NQ>
+struct LShape {
+    static constexpr int kThreads = NQ == 1 ? 1024 : 512;
+};
 
 // ---------------------------------------------------------------- model ---
 
 // Root model in FP32 with explicit round-to-nearest operations (the same
 // arithmetic at training-time error measurement and in the search).
+// Units are ramps, clamp(w1 x + b1, 0, 1): with w1, w2 >= 0 every term is
+// non-decreasing in x under round-to-nearest, so the network is monotone, and
+// (unlike ReLUs with non-negative weights, whose sum is convex) a sum of
+// ramps can follow a CDF that bends both ways.
 __device__ __forceinline__ float mlp_eval(const float *p, int H, float x) {
     float out = p[3 * H];
     for (int j = 0; j < H; j++) {
         const float h = __fadd_rn(__fmul_rn(p[j], x), p[H + j]);
-        out = __fadd_rn(out, __fmul_rn(p[2 * H + j], fmaxf(h, 0.f)));
+        out = __fadd_rn(out, __fmul_rn(p[2 * H + j], fminf(fmaxf(h, 0.f), 1.f)));
     }
     return out;
 }
@@ -412,7 +423,7 @@ __device__ V tree_point(const DevTree &t, K q) {
 // grp + 16, grp + 24 of the tile and keeps NQ of them in flight (4 / NQ
 // passes per tile).
 template <typename K, typename V, int NQ>
-__global__ void __launch_bounds__(kLThreads, 1)
+__global__ void __launch_bounds__(LShape<NQ>::kThreads, 1)
 learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
                const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
     using LG = LeafGeom<K, V>;
@@ -529,33 +540,41 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 const uint32_t b0 = __shfl_sync(0xffffffffu, act ? cw[s][0] : 0u, g0);
                 const uint32_t b1 = __shfl_sync(0xffffffffu, act ? cw[s][1] : 0u, g0);
                 const uint32_t shw = __shfl_sync(0xffffffffu, act ? cw[s][2] : 0u, g0);
-                if (!act) continue;
                 const uint64_t lbase = ((uint64_t)b1 << 32) | b0;
-                const uint32_t j0 = (ua[s] / kCodesPerLine + l) * kCodesPerLine;
                 const uint64_t key = (uint64_t)qv[s];
-                if (key < lbase) continue;  // every threshold of the line is above the key
-                const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
-                const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
-                // lane 0: codes 0..10 (half-words 5..15: after the base and the
-                // shift); lane g > 0: codes 16 g - 5 .. 16 g + 10
+                // A line's codes never decrease, so those at or below the
+                // key's bucket are a prefix of its 59 slots: count them two
+                // at a time (lane 0 holds slots 0-10 after the base and the
+                // shift, lane g > 0 slots 16 g - 5 .. 16 g + 10).
+                uint32_t c = 0;
+                if (act && key >= lbase) {
+                    const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
+                    const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
+                    const uint32_t qd2 = qd | (qd << 16);
 #pragma unroll
-                for (int h2 = 0; h2 < 16; h2++) {
-                    if (gl == 0 && h2 < 5) continue;
-                    const uint32_t j = j0 + (uint32_t)(16 * gl + h2 - 5);
-                    const uint32_t code = (cw[s][h2 >> 1] >> ((h2 & 1) * 16)) & 0xFFFFu;
-                    skip[s] += (j >= ua[s] && j < ub[s] && code <= qd) ? 1u : 0u;
+                    for (int w2 = 0; w2 < 8; w2++) {
+                        uint32_t le = __vcmpleu2(cw[s][w2], qd2);
+                        if (gl == 0) le = w2 < 2 ? 0u : (w2 == 2 ? (le & 0xFFFF0000u) : le);
+                        c += __popc(le);
+                    }
+                    c >>= 4;  // 16 set bits per slot
+                }
+                c += __shfl_xor_sync(0xffffffffu, c, 1);
+                c += __shfl_xor_sync(0xffffffffu, c, 2);
+                if (act) {
+                    // thresholds j0 .. j0 + c - 1 are at or below the key; keep
+                    // those of the window [ua, ub - 1]
+                    const uint32_t j0 = (ua[s] / kCodesPerLine + l) * kCodesPerLine;
+                    const uint32_t lo = max(ua[s], j0), hi = min(ub[s], j0 + kCodesPerLine);
+                    const uint32_t e = min(j0 + c, hi);
+                    skip[s] += e > lo ? e - lo : 0u;
                 }
             }
         }
         // ---- 4. the leaf unit (walking right past a threshold bucket)
         uint32_t unit[NQ];
 #pragma unroll
-        for (int s = 0; s < NQ; s++) {
-            uint32_t c = skip[s];
-            c += __shfl_xor_sync(0xffffffffu, c, 1);
-            c += __shfl_xor_sync(0xffffffffu, c, 2);
-            unit[s] = ua[s] + c;
-        }
+        for (int s = 0; s < NQ; s++) unit[s] = ua[s] + skip[s];
         bool pend[NQ];
 #pragma unroll
         for (int s = 0; s < NQ; s++) pend[s] = live[s];
@@ -660,11 +679,12 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     }
 }
 
-template <typename K, typename V>
-bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                         cudaStream_t s) {
+template <typename K, typename V, int NQ>
+bt_status learned_launch_nq(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
+                            cudaStream_t s) {
     const LearnedDev &m = t->learned->dev;
-    auto fn = learned_kernel<K, V, kLearnedNQ>;
+    constexpr int T = LShape<NQ>::kThreads;
+    auto fn = learned_kernel<K, V, NQ>;
     const size_t smem = (size_t)m.stage_bytes + (3 * kMaxHidden + 1) * sizeof(float);
     static int set_for[64] = {0};
     int dev = t->device;
@@ -673,12 +693,19 @@ bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d
         set_for[dev] = (int)smem;
     }
     const uint64_t ntiles = (nq + 31) / 32;
-    const uint64_t want = (ntiles + kLThreads / 32 - 1) / (kLThreads / 32);
+    const uint64_t want = (ntiles + T / 32 - 1) / (T / 32);
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, sm_count()));
     count_launch();
-    fn<<<grid, kLThreads, smem, s>>>(t->dev, m, (const K *)d_q, nq, (V *)d_out);
+    fn<<<grid, T, smem, s>>>(t->dev, m, (const K *)d_q, nq, (V *)d_out);
     BT_CUDA(cudaGetLastError());
     return BT_OK;
+}
+
+template <typename K, typename V>
+bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
+                         cudaStream_t s) {
+    return t->learned->in_flight == 1 ? learned_launch_nq<K, V, 1>(t, d_q, nq, d_out, s)
+                                      : learned_launch_nq<K, V, 2>(t, d_q, nq, d_out, s);
 }
 
 // ------------------------------------------------------------- training ---
@@ -716,15 +743,15 @@ mlp_loss_grad_kernel(const float *__restrict__ p, int H, const float *__restrict
          i += (uint64_t)gridDim.x * blockDim.x) {
         const float xi = x[i];
         float out = sp[3 * H];
-        for (int j = 0; j < H; j++) out += sp[2 * H + j] * fmaxf(sp[j] * xi + sp[H + j], 0.f);
+        for (int j = 0; j < H; j++) out += sp[2 * H + j] * fminf(fmaxf(sp[j] * xi + sp[H + j], 0.f), 1.f);
         const float err = out - y[i];
         l += err * err;
         const float dout = scale * err;
         for (int j = 0; j < H; j++) {
             const float h = sp[j] * xi + sp[H + j];
-            const float a = fmaxf(h, 0.f);
+            const float a = fminf(fmaxf(h, 0.f), 1.f);
             g[2 * H + j] += dout * a;
-            const float dh = h > 0.f ? dout * sp[2 * H + j] : 0.f;
+            const float dh = (h > 0.f && h < 1.f) ? dout * sp[2 * H + j] : 0.f;
             g[j] += dh * xi;
             g[H + j] += dh;
         }
@@ -877,11 +904,12 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     stage_kernel<K><<<grid_of(nls, 256), 256, 0, s>>>(st->d_seg, nls, kmin, xscale,
                                                      (K *)st->d_stage, x, y);
 
-    // ---- root: hinges spread over [0, 1), output weights 1/H, then Adam
+    // ---- root: ramps tiling [0, 1] in equal steps with output weights 1/H
+    // (the identity y = x: the untrained network), then Adam
     std::vector<float> p0(np);
     for (int j = 0; j < H; j++) {
-        p0[j] = 1.f;
-        p0[H + j] = -(float)j / (float)H;
+        p0[j] = (float)H;
+        p0[H + j] = -(float)j;
         p0[2 * H + j] = 1.f / (float)H;
     }
     p0[3 * H] = 0.f;
@@ -1003,7 +1031,7 @@ bt_status bt_learned_train(bt_tree *t, const bt_learned_config *cfg_in, void *st
     if (!t) return fail(BT_ERR_INVALID_ARGUMENT, "tree is NULL");
     if (t->n < 2) return fail(BT_ERR_INVALID_ARGUMENT, "a learned index needs at least 2 keys");
     if (t->n >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "learned index supports n < 2^32");
-    bt_learned_config cfg = {65536, 0, 16, 400, 0.01f};
+    bt_learned_config cfg = {65536, 0, 16, 400, 0.002f};
     if (cfg_in) {
         if (cfg_in->num_segments) cfg.num_segments = cfg_in->num_segments;
         cfg.max_error = cfg_in->max_error;
@@ -1031,6 +1059,15 @@ bt_status bt_learned_train(bt_tree *t, const bt_learned_config *cfg_in, void *st
 bt_status bt_point_search_learned(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
                                   void *stream) {
     return bt_point_search(t, BT_POINT_LEARNED, d_q, nq, d_out, stream);
+}
+
+bt_status bt_learned_set_shape(bt_tree *t, uint32_t queries_in_flight) {
+    using namespace bt;
+    if (!t || !t->learned) return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
+    if (queries_in_flight != 1 && queries_in_flight != 2)
+        return fail(BT_ERR_INVALID_ARGUMENT, "queries_in_flight must be 1 or 2");
+    t->learned->in_flight = (int)queries_in_flight;
+    return BT_OK;
 }
 
 bt_status bt_learned_last_stats(const bt_tree *t, uint64_t *extra, uint64_t *fallback) {

@@ -80,25 +80,78 @@ __device__ __forceinline__ Cell box_cell(uint32_t x0, uint32_t y0, uint32_t x1, 
     return cell;
 }
 
-// Lanes 0-15 receive the first key position of cell `lane`, lanes 16-31 the
-// position after the last key of cell `lane - 16`: lower bounds of the
-// cells' first codes and upper bounds of their last codes, 32 descents in
-// one round (G lanes per descent, G descents per group).  n < 2^32.
-template <typename V, int G>
-__device__ __forceinline__ uint32_t cell_bounds(const DevTree &t, const uint32_t *s_lvl,
-                                                uint32_t *res, const Cell &cell, int lane) {
+// The cover's cells merged into runs: cells taken in Z order, a cell joining
+// the run before it when its codes continue that run's (last code + 1 ==
+// first code) and it is of the same kind (inside the box, or on its edge).
+// A run is one contiguous stretch of codes, so its points are one stretch of
+// the sorted keys: two bounds per run instead of two per cell.  Lane r < 16
+// receives run r (valid for r < the returned count); lanes >= 16 receive
+// run r - 16 as well.  `ord` is 16 words of per-warp scratch.
+__device__ __forceinline__ int box_runs(uint32_t x0, uint32_t y0, uint32_t x1, uint32_t y1,
+                                        int lane, uint32_t *ord, Cell &run) {
+    const int j = lane % kMaxCells;
+    const Cell c = box_cell(x0, y0, x1, y1, j);
+    // Z rank of this cell among the valid ones (codes of distinct cells differ)
+    int rank = 0;
+#pragma unroll
+    for (int k = 0; k < kMaxCells; k++) {
+        const uint32_t zk = __shfl_sync(0xffffffffu, c.zs, k);
+        const bool vk = __shfl_sync(0xffffffffu, (int)c.valid, k) != 0;
+        rank += (vk && zk < c.zs) ? 1 : 0;
+    }
+    if (lane < kMaxCells && c.valid) ord[rank] = (uint32_t)j;
+    __syncwarp();
+    const int nvalid = __popc(__ballot_sync(0xffffffffu, lane < kMaxCells && c.valid));
+    // the cell of rank r (lane r), and of rank r - 1
+    const int r = j;
+    const int src = r < nvalid ? (int)ord[r] : 0;
+    const int prv = (r > 0 && r <= nvalid) ? (int)ord[r - 1] : 0;
+    __syncwarp();
+    const uint32_t zs = __shfl_sync(0xffffffffu, c.zs, src);
+    const uint32_t ze = __shfl_sync(0xffffffffu, c.ze, src);
+    const bool full = __shfl_sync(0xffffffffu, (int)c.full, src) != 0;
+    const uint32_t pze = __shfl_sync(0xffffffffu, c.ze, prv);
+    const bool pfull = __shfl_sync(0xffffffffu, (int)c.full, prv) != 0;
+    const bool in = r < nvalid;
+    const bool starts = in && (r == 0 || pze + 1u != zs || pfull != full);
+    const unsigned sm = __ballot_sync(0xffffffffu, lane < kMaxCells && starts);
+    const int nruns = __popc(sm);
+    // run k: from the k-th start to the cell before the (k+1)-th start
+    const int k = j;
+    unsigned m = sm;
+    for (int z = 0; z < k && m; z++) m &= m - 1;
+    const int first = m ? __ffs(m) - 1 : 0;
+    const unsigned after = m ? (m & (m - 1)) : 0u;
+    const int last = after ? __ffs(after) - 2 : nvalid - 1;
+    run.zs = __shfl_sync(0xffffffffu, zs, first);
+    run.ze = __shfl_sync(0xffffffffu, ze, last < 0 ? 0 : last);
+    run.full = __shfl_sync(0xffffffffu, (int)full, first) != 0;
+    run.valid = k < nruns;
+    return nruns;
+}
+
+// Bounds of up to NR runs (NR = 8 or 16), 2 NR descents in one round with
+// 4 lanes per descent: descent d < NR is the lower bound of run d's first
+// code, d >= NR the upper bound of run d - NR's last code.  Lane r < 16
+// receives the first key position of run r, lane 16 + r the position after
+// its last key (as cell_bounds does for cells).
+template <typename V, int NR>
+__device__ __forceinline__ uint32_t run_bounds(const DevTree &t, const uint32_t *s_lvl,
+                                               uint32_t *res, const Cell &run, int lane) {
     using LG = LeafGeom<uint32_t, V>;
-    constexpr int NG = 32 / G;
-    constexpr int I = G;
+    constexpr int G = 4, NG = 32 / G, I = 2 * NR / NG;
     const int grp = lane / G, gl = lane % G;
     const uint32_t tmax = (uint32_t)t.max_key;
-    const bool upper_lane = lane >= kMaxCells;
-    // lower bound of a: a > max gives n; upper bound of b: b >= max gives n
-    const uint32_t a = upper_lane ? cell.ze : cell.zs;
-    const bool beyond = upper_lane ? a >= tmax : a > tmax;
-    const bool up = upper_lane && a < tmax;
+    // the query of descent d = lane (lanes >= 2 NR idle in the search)
+    const int d = lane;
+    const int ri = d % NR;
+    const bool upper = d >= NR;
+    const uint32_t zs = __shfl_sync(0xffffffffu, run.zs, ri);
+    const uint32_t ze = __shfl_sync(0xffffffffu, run.ze, ri);
+    const uint32_t a = upper ? ze : zs;
+    const bool up = upper && a < tmax;
     const uint32_t qa = a < tmax ? a : tmax;
-    const uint32_t nd = smem_bound<uint32_t>(s_lvl, t.smem_entries, qa, up);
+    const uint32_t nd = d < 2 * NR ? smem_bound<uint32_t>(s_lvl, t.smem_entries, qa, up) : 0u;
     uint32_t qe[I], node[I];
     bool ups[I];
 #pragma unroll
@@ -116,9 +169,15 @@ __device__ __forceinline__ uint32_t cell_bounds(const DevTree &t, const uint32_t
     for (int s = 0; s < I; s++)
         if (gl == 0) res[s * NG + grp] = node[s] * (uint32_t)LG::S + (uint32_t)pos[s];
     __syncwarp();
-    const uint32_t r = beyond ? (uint32_t)t.n : res[lane];
+    const int r = lane % kMaxCells;
+    const bool want_upper = lane >= kMaxCells;
+    // beyond the keys: a lower bound of a code above the largest key, or an
+    // upper bound of one at or above it, is n
+    const uint32_t mine = want_upper ? run.ze : run.zs;
+    const bool beyond = want_upper ? mine >= tmax : mine > tmax;
+    const uint32_t v = r < NR ? res[(want_upper ? NR : 0) + r] : 0u;
     __syncwarp();
-    return r;
+    return beyond ? (uint32_t)t.n : v;
 }
 
 // Exclusive prefix sum over the warp.
@@ -167,7 +226,6 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
     __syncthreads();
     using LG = LeafGeom<uint32_t, V>;
     const int lane = threadIdx.x & 31;
-    const int j = lane % kMaxCells;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
     for (uint64_t g = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; g < nr;
          g += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
@@ -180,8 +238,10 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
             continue;
         }
         const ZBox box(x0, y0, x1, y1);
-        const Cell cell = box_cell(x0, y0, x1, y1, j);
-        const uint32_t b = cell_bounds<V, 4>(t, s_lvl, res, cell, lane);
+        Cell cell;
+        const int nruns = box_runs(x0, y0, x1, y1, lane, res, cell);
+        const uint32_t b = nruns <= 8 ? run_bounds<V, 8>(t, s_lvl, res, cell, lane)
+                                      : run_bounds<V, 16>(t, s_lvl, res, cell, lane);
         const uint32_t ub = __shfl_sync(0xffffffffu, b, (lane + kMaxCells) & 31);
         const uint32_t len = (lane < kMaxCells && cell.valid && ub > b) ? ub - b : 0u;
         uint32_t total;
@@ -222,6 +282,7 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
                  const uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                  V *__restrict__ ids) {
     __shared__ V s_buf[kRWarps][kWarpSortCap];
+    __shared__ uint32_t ord[kRWarps][kMaxCells];
     using LG = LeafGeom<uint32_t, V>;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -234,7 +295,8 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
         const uint64_t cnt = counts[i];
         if (x0 > x1 || y0 > y1 || cnt == 0) continue;
         const ZBox box(x0, y0, x1, y1);
-        const Cell cell = box_cell(x0, y0, x1, y1, lane % kMaxCells);
+        Cell cell;
+        box_runs(x0, y0, x1, y1, lane, ord[threadIdx.x >> 5], cell);
         const uint2 run = lane < kMaxCells ? runs[g * kMaxCells + lane] : make_uint2(0u, 0u);
         const bool buffered = cnt <= (uint64_t)kWarpSortCap;
         V *dst = buffered ? buf : ids + offsets[i];

@@ -319,11 +319,12 @@ def serving_section(args, bt, tree, keys, plain_cfg, learned_cfg):
     for mode in ("basic", "learned"):
         tree.set_search_config(*(learned_cfg if mode == "learned" else plain_cfg))
         with bt.Server(tree, mode=mode, slots=8, memory_budget_bytes=512 << 20) as srv:
-            srv.replay(reqs[:200], arrivals[:200] - arrivals[0], outs[:200])  # warm-up
+            srv.replay(reqs, arrivals - arrivals[0], outs)  # warm-up: the whole loop once
             lat, wall, _ = srv.replay(reqs, arrivals - arrivals[0], outs)
             st = srv.stats()
         res["plain" if mode == "basic" else "learned"] = {
             "p50_us": float(np.percentile(lat, 50)), "p99_us": float(np.percentile(lat, 99)),
+            "max_us": float(lat.max()), "over_1ms": int(np.count_nonzero(lat > 1000.0)),
             "mean_us": float(lat.mean()), "queries_per_s": float(sizes.sum() / (wall / 1e6)),
             "max_in_flight": st["max_in_flight"], "slots": st["slots"]}
     return res
@@ -795,6 +796,7 @@ def run_ours(args):
     clocks.start()
     at = importlib.import_module(PKG + ".autotune")
     p_lanes, p_rounds, _ = at.tune(tree, dq, mode="basic", repeats=3)
+    _, l_in_flight, l_tune_ms = at.tune(tree, dq, mode="learned", repeats=3)
     for _ in range(max(args.warmup, 3)):
         search_learned()
     torch.cuda.synchronize(device)
@@ -931,6 +933,7 @@ def run_ours(args):
                                                   "code_lines_mean", "index_bytes",
                                                   "keys_per_unit", "train_ms")},
             "learned_stats": {"extra_unit_reads": extra, "full_descents": fallback},
+            "learned_shape": {"queries_in_flight_per_group": l_in_flight, "autotune_ms": l_tune_ms},
             "cpu_baseline": cpu,
             "cpu_sample_matches_gpu": checked,
             "clocks": clk,

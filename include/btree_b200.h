@@ -285,12 +285,13 @@ BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *
  *    O'Rourke 1981, the segmentation of the PGM-index, Ferragina &
  *    Vinciguerra 2020), computed on the GPU; a segment's bound eps is then
  *    re-measured with the exact FP32 arithmetic of the search;
- *  - root: a monotone MLP (1 input, `hidden` ReLU units, 1 output; input and
- *    output weights kept >= 0) from the normalised key to the position of
- *    the key's segment among the segment lines (4 segments per 128-byte
- *    line), trained on the GPU by full-batch Adam with this library's own
- *    forward/backward kernels; its worst error over the lines' first keys
- *    bounds a shared-memory search over those keys;
+ *  - root: a monotone MLP (1 input, `hidden` ramp units clamp(w1 x + b1, 0,
+ *    1), 1 output; input and output weights kept >= 0) from the normalised
+ *    key to the position of the key's segment among the segment lines (4
+ *    segments per 128-byte line), started as the identity and trained on the
+ *    GPU by full-batch Adam with this library's own forward/backward kernels;
+ *    its worst error over the lines' first keys bounds a shared-memory search
+ *    over those keys;
  *  - unit thresholds: one 16-bit code per leaf-unit boundary (59 per
  *    128-byte line with a 64-bit base and a shift), an exact separator
  *    between the units' key ranges.
@@ -308,7 +309,7 @@ typedef struct bt_learned_config {
                                When set, num_segments is ignored */
     uint32_t hidden;        /* root hidden units, 1..32 (default 16) */
     uint32_t iterations;    /* root training steps (default 400) */
-    float learning_rate;    /* Adam step size (default 0.01) */
+    float learning_rate;    /* Adam step size (default 0.002) */
 } bt_learned_config;
 
 typedef struct bt_learned_report {
@@ -339,6 +340,11 @@ BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, v
  * no trained index. */
 BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
                                          void *d_out, void *stream);
+
+/* Shape of the learned search kernel: queries in flight per 4-lane group,
+ * 1 (1024-thread CTAs) or 2 (512-thread CTAs; the default).  Results do not
+ * depend on it; the autotuner picks the faster one. */
+BT_API bt_status bt_learned_set_shape(bt_tree *tree, uint32_t queries_in_flight);
 
 /* Counters of the last learned search on this tree: leaf units read beyond
  * the first one (keys just past a unit's threshold) and queries that took

@@ -1,9 +1,9 @@
 """CPU reference of the learned index's root network -- TEST INFRASTRUCTURE.
 
 Float64 forward pass, mean-squared-error loss and its analytic gradient for
-the one-hidden-layer ReLU network the engine trains on the GPU
-(y = b2 + sum_j w2[j] * relu(w1[j] * x + b1[j]); parameter vector
-[w1, b1, w2, b2]).  The tests check the GPU gradient kernel against it and it
+the one-hidden-layer network of ramp units the engine trains on the GPU
+(y = b2 + sum_j w2[j] * ramp(w1[j] * x + b1[j]), ramp = clamp to [0, 1];
+parameter vector [w1, b1, w2, b2]).  The tests check the GPU gradient kernel against it and it
 against central finite differences.  The engine never imports this file.
 """
 import numpy as np
@@ -17,7 +17,7 @@ def unpack(p, H):
 def forward(p, H, x):
     w1, b1, w2, b2 = unpack(p, H)
     h = np.outer(np.asarray(x, dtype=np.float64), w1) + b1
-    return b2 + np.maximum(h, 0.0) @ w2
+    return b2 + np.clip(h, 0.0, 1.0) @ w2
 
 
 def loss(p, H, x, y):
@@ -29,12 +29,12 @@ def loss_grad(p, H, x, y):
     w1, b1, w2, b2 = unpack(p, H)
     x = np.asarray(x, dtype=np.float64)
     h = np.outer(x, w1) + b1
-    a = np.maximum(h, 0.0)
+    a = np.clip(h, 0.0, 1.0)
     e = b2 + a @ w2 - np.asarray(y, dtype=np.float64)
     n = len(x)
     dout = 2.0 * e / n
     g_w2 = a.T @ dout
-    dh = (h > 0) * np.outer(dout, w2)
+    dh = ((h > 0) & (h < 1)) * np.outer(dout, w2)
     g_w1 = dh.T @ x
     g_b1 = dh.sum(axis=0)
     g_b2 = dout.sum()
