@@ -346,7 +346,7 @@ class Tree:
         return out
 
     def learned_set_shape(self, queries_in_flight):
-        """Learned search kernel shape: 1 or 2 queries in flight per lane group."""
+        """Learned search kernel shape: 1 or 2 queries in flight per lane pair."""
         _check(lib().bt_learned_set_shape(self._h, queries_in_flight), "bt_learned_set_shape")
 
     def learned_last_stats(self):

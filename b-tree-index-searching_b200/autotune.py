@@ -19,8 +19,8 @@ import os
 import statistics
 
 SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
-# learned search: (lanes per query, queries in flight per lane group)
-LEARNED_SHAPES = ((4, 1), (4, 2))
+# learned search: (lanes per query, queries in flight per lane pair)
+LEARNED_SHAPES = ((2, 1), (2, 2))
 
 
 def _key(tree, mode, nq):

@@ -45,7 +45,7 @@ struct LearnedState {
     void *d_stage = nullptr;
     unsigned long long *d_stats = nullptr;
     uint64_t bytes = 0;
-    int in_flight = 2;  // queries in flight per lane group (bt_learned_set_shape)
+    int in_flight = 2;  // queries in flight per lane pair (bt_learned_set_shape)
     LearnedDev dev;
 };
 
@@ -66,8 +66,7 @@ constexpr int kHullCap = 32;                 // points per convex hull
 constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
 constexpr int kMaxWalk = 8;                  // extra units read before the full descent
 // Search CTA shapes (one CTA per SM: the staged keys): NQ queries in flight
-// per 4-lane group, 1024 / NQ threads -- the register budget of either shape
-// holds the kernel without spills.
+// per lane pair, 1024 / NQ threads.
 template <int NQ>
 struct LShape {
     static constexpr int kThreads = NQ == 1 ? 1024 : 512;
@@ -384,9 +383,6 @@ __device__ __forceinline__ void load_unit32(const void *p, uint32_t (&w)[8]) {
         : "l"(p), "l"(l2_evict_first()));
 }
 
-__device__ __forceinline__ uint32_t sel4(const uint32_t *w, int i) {
-    return i == 0 ? w[0] : i == 1 ? w[1] : i == 2 ? w[2] : w[3];
-}
 
 // Last staged index in [a, b] whose key is below q (a when none: then a == 0
 // by the root's bound).  Routing by "first key < q" sends a key equal to a
@@ -419,9 +415,44 @@ __device__ V tree_point(const DevTree &t, K q) {
     return key_max<V>();
 }
 
-// One warp tile = 32 queries; a group of 4 lanes owns queries grp, grp + 8,
-// grp + 16, grp + 24 of the tile and keeps NQ of them in flight (4 / NQ
-// passes per tile).
+// 64-byte half of an index line: two 32-byte loads, evict-last in L2.
+__device__ __forceinline__ void load_half_line(const unsigned char *p, uint32_t (&w)[16]) {
+    uint32_t a[8], b[8];
+    load_line32(p, a);
+    load_line32(p + 32, b);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        w[i] = a[i];
+        w[8 + i] = b[i];
+    }
+}
+
+// 64-byte half of a leaf unit (touched once per query): evict-first.
+__device__ __forceinline__ void load_half_unit(const unsigned char *p, uint32_t (&w)[16]) {
+    uint32_t a[8], b[8];
+    load_unit32(p, a);
+    load_unit32(p + 32, b);
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        w[i] = a[i];
+        w[8 + i] = b[i];
+    }
+}
+
+template <int N>
+__device__ __forceinline__ uint32_t pick(const uint32_t (&w)[N], int i) {
+    uint32_t v = w[0];
+#pragma unroll
+    for (int k = 1; k < N; k++) v = i == k ? w[k] : v;
+    return v;
+}
+
+// One warp tile = 32 queries.  Phase 1 takes one lane per query; phase 2 a
+// pair of lanes per query, each lane reading one 64-byte half of every
+// 128-byte line (segment line, code lines, leaf unit): lane pair p owns
+// queries p and p + 16 of the tile and keeps NQ of them in flight (2 / NQ
+// passes per tile).  With a leaf unit of two blocks each lane holds a whole
+// block -- its keys and their values -- and answers its own matches.
 template <typename K, typename V, int NQ>
 __global__ void __launch_bounds__(LShape<NQ>::kThreads, 1)
 learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
@@ -429,6 +460,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     using LG = LeafGeom<K, V>;
     constexpr int KPU = unit_keys<K, V>();      // keys per unit
     constexpr int BPU = kUnitBytes / LG::BS;    // blocks per unit (1 or 2)
+    constexpr int VW = (int)sizeof(V) / 4;      // words per value
     extern __shared__ uint4 smem_l[];
     K *s_stage = reinterpret_cast<K *>(smem_l);
     float *s_mlp = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem_l) + m.stage_bytes);
@@ -442,11 +474,11 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
-    const int grp = lane >> 2, gl = lane & 3, g0 = grp * 4;
+    const int pr = lane >> 1, hl = lane & 1, p0 = pr * 2;
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
     const uint64_t leaf_bytes = t.n_sectors * (uint64_t)LG::BS;
     const uint64_t n = t.n;
-    const uint64_t U = m.units;
+    const uint32_t U = (uint32_t)m.units;
     const uint64_t ntiles = (nq + 31) / 32;
     unsigned long long n_extra = 0, n_fallback = 0;
 
@@ -465,57 +497,52 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             my_sl = stage_search<K>(s_stage, a, b, myq);
         }
 #pragma unroll 1
-        for (int hf = 0; hf < 4 / NQ; hf++) {
+        for (int hf = 0; hf < 2 / NQ; hf++) {
         K qv[NQ];
         bool live[NQ];
-        uint32_t w[NQ][8];
+        uint32_t w[NQ][16];
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
-            const int k = (hf * NQ + s) * 8 + grp;
+            const int k = (hf * NQ + s) * 16 + pr;
             qv[s] = __shfl_sync(0xffffffffu, myq, k);
             live[s] = base + k < nq;
             const uint32_t sl = __shfl_sync(0xffffffffu, my_sl, k);
-            if (live[s]) load_line32(reinterpret_cast<const unsigned char *>(m.seg + sl) + gl * 32, w[s]);
+            if (live[s]) load_half_line(reinterpret_cast<const unsigned char *>(m.seg + sl) + hl * 64, w[s]);
         }
         // ---- 2. segment -> rank window -> unit window [ua, ub]
+        // lane 0 of a pair: key[0..3] (words 0-7), r_lo[4] (8-11), cnt[4] (12-15);
+        // lane 1: slope[4] (0-3), icpt[4] (4-7), eps[4] (8-11)
         uint32_t ua[NQ], ub[NQ];
         int nlines[NQ];
         int maxl = 0;
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
+            const uint64_t key = (uint64_t)qv[s];
             int c = 0;
-            if (gl == 0) {
 #pragma unroll
-                for (int i = 1; i < kSegPerLine; i++) {
-                    const uint64_t k = ((uint64_t)w[s][2 * i + 1] << 32) | w[s][2 * i];
-                    c += k < (uint64_t)qv[s] ? 1 : 0;
-                }
-            }
-            c = __shfl_sync(0xffffffffu, c, g0);
-            uint32_t a = 0, b = 0;
-            if (gl == 0) {
-                a = c == 0 ? w[s][0] : c == 1 ? w[s][2] : c == 2 ? w[s][4] : w[s][6];
-                b = c == 0 ? w[s][1] : c == 1 ? w[s][3] : c == 2 ? w[s][5] : w[s][7];
-            } else if (gl == 3) {
-                a = sel4(w[s], c);  // eps
-            } else {
-                a = sel4(w[s], c);      // r_lo (lane 1) or slope (lane 2)
-                b = sel4(w[s] + 4, c);  // cnt (lane 1) or icpt (lane 2)
-            }
-            const uint64_t fk = ((uint64_t)__shfl_sync(0xffffffffu, b, g0) << 32) |
-                                __shfl_sync(0xffffffffu, a, g0);
-            const uint32_t r_lo = __shfl_sync(0xffffffffu, a, g0 + 1);
-            const uint32_t cnt = __shfl_sync(0xffffffffu, b, g0 + 1);
-            const float slope = __uint_as_float(__shfl_sync(0xffffffffu, a, g0 + 2));
-            const float icpt = __uint_as_float(__shfl_sync(0xffffffffu, b, g0 + 2));
-            const uint32_t eps = __shfl_sync(0xffffffffu, a, g0 + 3);
-            const float p = seg_pred(slope, icpt, cnt, fk, (uint64_t)qv[s]);
+            for (int i = 1; i < kSegPerLine; i++)
+                c += (((uint64_t)w[s][2 * i + 1] << 32) | w[s][2 * i]) < key ? 1 : 0;
+            c = __shfl_sync(0xffffffffu, c, p0);
+            // this lane's fields of segment c, then the partner's
+            const uint32_t f0 = hl ? pick(w[s], c) : pick(w[s], 2 * c);          // slope | key lo
+            const uint32_t f1 = hl ? pick(w[s], 4 + c) : pick(w[s], 2 * c + 1);  // icpt | key hi
+            const uint32_t f2 = pick(w[s], 8 + c);                                // eps | r_lo
+            const uint32_t f3 = hl ? 0u : pick(w[s], 12 + c);                     // - | cnt
+            const uint32_t g0 = __shfl_xor_sync(0xffffffffu, f0, 1);
+            const uint32_t g1 = __shfl_xor_sync(0xffffffffu, f1, 1);
+            const uint32_t g2 = __shfl_xor_sync(0xffffffffu, f2, 1);
+            const uint32_t g3 = __shfl_xor_sync(0xffffffffu, f3, 1);
+            const uint64_t fk = hl ? (((uint64_t)g1 << 32) | g0) : (((uint64_t)f1 << 32) | f0);
+            const uint32_t r_lo = hl ? g2 : f2, cnt = hl ? g3 : f3;
+            const float slope = __uint_as_float(hl ? f0 : g0), icpt = __uint_as_float(hl ? f1 : g1);
+            const uint32_t eps = hl ? f2 : g2;
+            const float p = seg_pred(slope, icpt, cnt, fk, key);
             const int64_t ra = (int64_t)r_lo + (int64_t)floorf(p) - (int64_t)eps - 1;
             const int64_t rb = (int64_t)r_lo + (int64_t)ceilf(p) + (int64_t)eps + 1;
-            const uint64_t a_u = ra <= 0 ? 0 : min((uint64_t)ra / KPU, U - 1);
-            const uint64_t b_u = rb <= 0 ? 0 : min((uint64_t)rb / KPU, U - 1);
-            ua[s] = (uint32_t)a_u;
-            ub[s] = (uint32_t)(b_u < a_u ? a_u : b_u);
+            const uint32_t a_u = ra <= 0 ? 0u : (uint32_t)min((uint64_t)ra / KPU, (uint64_t)U - 1);
+            const uint32_t b_u = rb <= 0 ? 0u : (uint32_t)min((uint64_t)rb / KPU, (uint64_t)U - 1);
+            ua[s] = a_u;
+            ub[s] = b_u < a_u ? a_u : b_u;
             nlines[s] = (live[s] && ub[s] > ua[s])
                             ? (int)((ub[s] - 1) / kCodesPerLine - ua[s] / kCodesPerLine) + 1
                             : 0;
@@ -527,40 +554,39 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
 #pragma unroll
         for (int s = 0; s < NQ; s++) skip[s] = 0;
         for (int l = 0; l < maxl; l++) {
-            uint32_t cw[NQ][8];
+            uint32_t cw[NQ][16];
 #pragma unroll
             for (int s = 0; s < NQ; s++)
                 if (l < nlines[s])
-                    load_line32(reinterpret_cast<const unsigned char *>(m.codes + ua[s] / kCodesPerLine + l) +
-                                    gl * 32,
-                                cw[s]);
+                    load_half_line(reinterpret_cast<const unsigned char *>(m.codes + ua[s] / kCodesPerLine + l) +
+                                       hl * 64,
+                                   cw[s]);
 #pragma unroll
             for (int s = 0; s < NQ; s++) {
                 const bool act = l < nlines[s];
-                const uint32_t b0 = __shfl_sync(0xffffffffu, act ? cw[s][0] : 0u, g0);
-                const uint32_t b1 = __shfl_sync(0xffffffffu, act ? cw[s][1] : 0u, g0);
-                const uint32_t shw = __shfl_sync(0xffffffffu, act ? cw[s][2] : 0u, g0);
+                const uint32_t b0 = __shfl_sync(0xffffffffu, act ? cw[s][0] : 0u, p0);
+                const uint32_t b1 = __shfl_sync(0xffffffffu, act ? cw[s][1] : 0u, p0);
+                const uint32_t shw = __shfl_sync(0xffffffffu, act ? cw[s][2] : 0u, p0);
                 const uint64_t lbase = ((uint64_t)b1 << 32) | b0;
                 const uint64_t key = (uint64_t)qv[s];
                 // A line's codes never decrease, so those at or below the
                 // key's bucket are a prefix of its 59 slots: count them two
-                // at a time (lane 0 holds slots 0-10 after the base and the
-                // shift, lane g > 0 slots 16 g - 5 .. 16 g + 10).
+                // at a time (lane 0 of the pair holds slots 0-26 after the
+                // base and the shift, lane 1 slots 27-58).
                 uint32_t c = 0;
                 if (act && key >= lbase) {
                     const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
                     const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
                     const uint32_t qd2 = qd | (qd << 16);
 #pragma unroll
-                    for (int w2 = 0; w2 < 8; w2++) {
+                    for (int w2 = 0; w2 < 16; w2++) {
                         uint32_t le = __vcmpleu2(cw[s][w2], qd2);
-                        if (gl == 0) le = w2 < 2 ? 0u : (w2 == 2 ? (le & 0xFFFF0000u) : le);
+                        if (hl == 0) le = w2 < 2 ? 0u : (w2 == 2 ? (le & 0xFFFF0000u) : le);
                         c += __popc(le);
                     }
                     c >>= 4;  // 16 set bits per slot
                 }
                 c += __shfl_xor_sync(0xffffffffu, c, 1);
-                c += __shfl_xor_sync(0xffffffffu, c, 2);
                 if (act) {
                     // thresholds j0 .. j0 + c - 1 are at or below the key; keep
                     // those of the window [ua, ub - 1]
@@ -573,94 +599,89 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         }
         // ---- 4. the leaf unit (walking right past a threshold bucket)
         uint32_t unit[NQ];
-#pragma unroll
-        for (int s = 0; s < NQ; s++) unit[s] = ua[s] + skip[s];
         bool pend[NQ];
 #pragma unroll
-        for (int s = 0; s < NQ; s++) pend[s] = live[s];
+        for (int s = 0; s < NQ; s++) {
+            unit[s] = ua[s] + skip[s];
+            pend[s] = live[s];
+        }
         for (int it = 0; it <= kMaxWalk; it++) {
-            uint32_t u[NQ][8];
+            uint32_t u[NQ][16];
 #pragma unroll
             for (int s = 0; s < NQ; s++) {
-                const uint64_t off = (uint64_t)unit[s] * kUnitBytes + gl * 32;
+                const uint64_t off = (uint64_t)unit[s] * kUnitBytes + hl * 64;
                 if (pend[s] && off < leaf_bytes) {
-                    load_unit32(leaves + off, u[s]);
+                    load_half_unit(leaves + off, u[s]);
                 } else {
 #pragma unroll
-                    for (int k = 0; k < 8; k++) u[s][k] = 0xFFFFFFFFu;  // padding keys
+                    for (int k = 0; k < 16; k++) u[s][k] = 0xFFFFFFFFu;  // padding keys
                 }
             }
 #pragma unroll
             for (int s = 0; s < NQ; s++) {
-                // key pieces: lanes 0 and 2 (two blocks) or lane 0 (one block)
-                const bool key_lane = BPU == 2 ? (gl == 0 || gl == 2) : gl == 0;
-                const int blk = BPU == 2 ? gl / 2 : 0;
-                int below = 0;
-                bool eq = false;
-                K last = 0;
+                // this lane's keys: its block (two blocks per unit), or the
+                // unit's one block in lane 0
+                const bool key_lane = BPU == 2 || hl == 0;
+                const uint64_t r0 = (uint64_t)unit[s] * KPU + (BPU == 2 ? (uint64_t)hl * LG::S : 0);
+                const bool last_unit = unit[s] + 1 >= U;
+                int pos = -1;
+                K lastk = 0;
                 if (key_lane) {
 #pragma unroll
-                    for (int i = 0; i < LG::S; i++) {
+                    for (int i = LG::S - 1; i >= 0; i--) {
                         const K k = key_at<K>(u[s], i);
-                        const uint64_t rank = (uint64_t)unit[s] * KPU + (uint64_t)blk * LG::S + i;
-                        const bool real = rank < n;
-                        below += (real && k < qv[s]) ? 1 : 0;
-                        eq |= real && k == qv[s];
-                        if (real) last = k;
+                        if (k == qv[s] && (!last_unit || r0 + i < n)) pos = i;
                     }
+                    lastk = key_at<K>(u[s], LG::S - 1);
                 }
-                const unsigned gm = 0xFu << g0;
-                const bool found = (__ballot_sync(0xffffffffu, pend[s] && eq) & gm) != 0;
-                int pos = __shfl_sync(0xffffffffu, below, g0);
-                if (BPU == 2) pos += __shfl_sync(0xffffffffu, below, g0 + 2);
-                // the unit's largest key (only read for units before the last,
-                // whose blocks are all full): the last key of its last block
-                const int ll = BPU == 2 ? g0 + 2 : g0;
-                K lastk = (K)__shfl_sync(0xffffffffu, (uint32_t)last, ll);
+                // the unit's largest key (read only for units before the last,
+                // whose blocks are full): the last key of its last block
+                const int ll = BPU == 2 ? p0 + 1 : p0;
+                K ulast = (K)__shfl_sync(0xffffffffu, (uint32_t)lastk, ll);
                 if constexpr (sizeof(K) == 8)
-                    lastk |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)last >> 32), ll) << 32;
-                const bool walk = pend[s] && !found && qv[s] > lastk && unit[s] + 1 < U &&
-                                  unit[s] + 1 <= ub[s];
-                const bool lost = pend[s] && !found && qv[s] > lastk && unit[s] + 1 < U &&
-                                  unit[s] + 1 > ub[s];
+                    ulast |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)lastk >> 32), ll) << 32;
+                const unsigned pm = 0x3u << p0;
+                const unsigned mb = __ballot_sync(0xffffffffu, pend[s] && pos >= 0) & pm;
+                const bool found = mb != 0;
+                // duplicates across the two blocks: the first occurrence (lane 0's) answers
+                const bool my_match = BPU == 2 && pos >= 0 && lane == __ffs(mb) - 1;
+                // with one block per unit the match is in lane 0 and its value
+                // may be in lane 1 (value bytes 32 + 8 pos)
+                const int mpos = BPU == 1 ? __shfl_sync(0xffffffffu, pos, p0) : pos;
+                const bool walk = pend[s] && !found && qv[s] > ulast && !last_unit && unit[s] + 1 <= ub[s];
+                const bool lost = pend[s] && !found && qv[s] > ulast && !last_unit && unit[s] + 1 > ub[s];
+                const uint64_t qi = base + (hf * NQ + s) * 16 + pr;
                 if (pend[s] && !walk && !lost) {
-                    // the lane holding the value writes the result
-                    int vl, vw;
-                    if (BPU == 2) {
-                        const int b = pos / LG::S, i = pos % LG::S;
-                        vl = 2 * b + 1;
-                        vw = i * (int)(sizeof(V) / 4);
-                    } else {
-                        const int byte = kSectorBytes + pos * (int)sizeof(V);
-                        vl = byte / 32;
-                        vw = (byte % 32) / 4;
-                    }
                     if (!found) {
-                        if (gl == 0) out[base + (hf * NQ + s) * 8 + grp] = key_max<V>();
-                    } else if (gl == vl) {
-                        V val;
-                        if constexpr (sizeof(V) == 4) {
-                            val = u[s][0];
-#pragma unroll
-                            for (int k = 1; k < 8; k++)
-                                if (k == vw) val = u[s][k];
+                        if (hl == 0) out[qi] = key_max<V>();
+                    } else {
+                        // words of the value at slot mpos, in the lane holding it
+                        int vw = -1;
+                        if (BPU == 2) {
+                            if (my_match) vw = (kSectorBytes / 4) + pos * VW;
                         } else {
-                            val = ((uint64_t)u[s][1] << 32) | u[s][0];
-#pragma unroll
-                            for (int k = 2; k < 8; k += 2)
-                                if (k == vw) val = ((uint64_t)u[s][k + 1] << 32) | u[s][k];
+                            const int byte = kSectorBytes + mpos * (int)sizeof(V);
+                            if (byte / 64 == hl) vw = (byte % 64) / 4;
                         }
-                        out[base + (hf * NQ + s) * 8 + grp] = val;
+                        if (vw >= 0) {
+                            V val;
+                            if constexpr (sizeof(V) == 4) {
+                                val = pick(u[s], vw);
+                            } else {
+                                val = ((uint64_t)pick(u[s], vw + 1) << 32) | pick(u[s], vw);
+                            }
+                            out[qi] = val;
+                        }
                     }
                     pend[s] = false;
                 } else if (walk) {
                     unit[s]++;
-                    if (gl == 0 && it < kMaxWalk) n_extra++;
+                    if (hl == 0 && it < kMaxWalk) n_extra++;
                 }
                 if (lost || (walk && it == kMaxWalk)) {
                     // outside the window: the tree's full descent
-                    if (gl == 0) {
-                        out[base + (hf * NQ + s) * 8 + grp] = tree_point<K, V>(t, qv[s]);
+                    if (hl == 0) {
+                        out[qi] = tree_point<K, V>(t, qv[s]);
                         n_fallback++;
                     }
                     pend[s] = false;

@@ -341,9 +341,10 @@ BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, v
 BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
                                          void *d_out, void *stream);
 
-/* Shape of the learned search kernel: queries in flight per 4-lane group,
- * 1 (1024-thread CTAs) or 2 (512-thread CTAs; the default).  Results do not
- * depend on it; the autotuner picks the faster one. */
+/* Shape of the learned search kernel: queries in flight per lane pair (two
+ * lanes share a query), 1 (1024-thread CTAs) or 2 (512-thread CTAs; the
+ * default).  Results do not depend on it; the autotuner picks the faster
+ * one. */
 BT_API bt_status bt_learned_set_shape(bt_tree *tree, uint32_t queries_in_flight);
 
 /* Counters of the last learned search on this tree: leaf units read beyond
