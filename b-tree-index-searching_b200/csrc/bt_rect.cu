@@ -118,11 +118,9 @@ __device__ __forceinline__ int box_runs(uint32_t x0, uint32_t y0, uint32_t x1, u
     const int nruns = __popc(sm);
     // run k: from the k-th start to the cell before the (k+1)-th start
     const int k = j;
-    unsigned m = sm;
-    for (int z = 0; z < k && m; z++) m &= m - 1;
-    const int first = m ? __ffs(m) - 1 : 0;
-    const unsigned after = m ? (m & (m - 1)) : 0u;
-    const int last = after ? __ffs(after) - 2 : nvalid - 1;
+    const unsigned fa = __fns(sm, 0, k + 1), fb = __fns(sm, 0, k + 2);  // ~0u: none
+    const int first = fa == ~0u ? 0 : (int)fa;
+    const int last = fa == ~0u ? 0 : (fb == ~0u ? nvalid - 1 : (int)fb - 1);
     run.zs = __shfl_sync(0xffffffffu, zs, first);
     run.ze = __shfl_sync(0xffffffffu, ze, last < 0 ? 0 : last);
     run.full = __shfl_sync(0xffffffffu, (int)full, first) != 0;
@@ -265,7 +263,8 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
             for (int h = 0; h < 2; h++) c += __popc(__ballot_sync(0xffffffffu, act[h] && box.holds(key[h])));
         }
         if (lane == 0) counts[i] = c;
-        if (lane < kMaxCells) runs[g * kMaxCells + lane] = make_uint2(b, len);
+        // the fill pass reads each run's kind from its length's top bit
+        if (lane < kMaxCells) runs[g * kMaxCells + lane] = make_uint2(b, len | (cell.full ? 0x80000000u : 0u));
     }
 }
 
@@ -282,7 +281,6 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
                  const uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
                  V *__restrict__ ids) {
     __shared__ V s_buf[kRWarps][kWarpSortCap];
-    __shared__ uint32_t ord[kRWarps][kMaxCells];
     using LG = LeafGeom<uint32_t, V>;
     const int lane = threadIdx.x & 31;
     const unsigned lt = (1u << lane) - 1u;
@@ -295,9 +293,9 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
         const uint64_t cnt = counts[i];
         if (x0 > x1 || y0 > y1 || cnt == 0) continue;
         const ZBox box(x0, y0, x1, y1);
-        Cell cell;
-        box_runs(x0, y0, x1, y1, lane, ord[threadIdx.x >> 5], cell);
-        const uint2 run = lane < kMaxCells ? runs[g * kMaxCells + lane] : make_uint2(0u, 0u);
+        const uint2 rr = lane < kMaxCells ? runs[g * kMaxCells + lane] : make_uint2(0u, 0u);
+        const bool run_full = (rr.y & 0x80000000u) != 0;
+        const uint2 run = make_uint2(rr.x, rr.y & 0x7FFFFFFFu);
         const bool buffered = cnt <= (uint64_t)kWarpSortCap;
         V *dst = buffered ? buf : ids + offsets[i];
         uint32_t T;
@@ -312,7 +310,7 @@ rect_fill_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict__
                 const uint32_t k = base + 32 * h + lane;
                 const int jc = find_cell(off, k);
                 const uint32_t p = __shfl_sync(0xffffffffu, run.x, jc) + (k - __shfl_sync(0xffffffffu, off, jc));
-                full[h] = __shfl_sync(0xffffffffu, (int)cell.full, jc) != 0;
+                full[h] = __shfl_sync(0xffffffffu, (int)run_full, jc) != 0;
                 act[h] = k < T;
                 const unsigned char *blk = block_of<V>(leaves, p);
                 key[h] = act[h] && !full[h] ? reinterpret_cast<const uint32_t *>(blk)[p % LG::S] : 0u;
@@ -437,8 +435,8 @@ bt_status bt_rect_search_mode(const bt_tree *t, int mode, const uint16_t *x0, co
     *h_total = 0;
     if (t->key_bytes != 4)
         return fail(BT_ERR_INVALID_ARGUMENT, "rectangle search needs 32-bit Morton-code keys");
-    if (t->n >= (1ull << 32))
-        return fail(BT_ERR_NOT_SUPPORTED, "rectangle search needs fewer than 2^32 points");
+    if (t->n >= (1ull << 31))
+        return fail(BT_ERR_NOT_SUPPORTED, "rectangle search needs fewer than 2^31 points");
     if (nr == 0) return BT_OK;
     if (!x0 || !y0 || !x1 || !y1 || !counts || !offsets)
         return fail(BT_ERR_INVALID_ARGUMENT, "a rectangle or output array is NULL");

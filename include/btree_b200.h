@@ -245,7 +245,8 @@ BT_API bt_status bt_range_search(const bt_tree *tree, int mode, const void *d_lo
  * contiguous run of Morton codes, found by a lower and an upper bound);
  * cells inside the box count whole, the keys of cells on its edge are
  * tested one by one.
- * BT_ERR_INVALID_ARGUMENT unless the tree has 4-byte keys.
+ * BT_ERR_INVALID_ARGUMENT unless the tree has 4-byte keys;
+ * BT_ERR_NOT_SUPPORTED from 2^31 points on.
  */
 BT_API bt_status bt_rect_search(const bt_tree *tree, const uint16_t *d_x0, const uint16_t *d_y0,
                                 const uint16_t *d_x1, const uint16_t *d_y1, uint64_t nr,
