@@ -439,12 +439,20 @@ __device__ __forceinline__ void load_half_unit(const unsigned char *p, uint32_t 
     }
 }
 
-template <int N>
-__device__ __forceinline__ uint32_t pick(const uint32_t (&w)[N], int i) {
-    uint32_t v = w[0];
-#pragma unroll
-    for (int k = 1; k < N; k++) v = i == k ? w[k] : v;
-    return v;
+// w[B + i] for i in 0..3 (B fixed): three selects.
+template <int B, int N>
+__device__ __forceinline__ uint32_t pick4(const uint32_t (&w)[N], int i) {
+    const uint32_t lo = (i & 1) ? w[B + 1] : w[B];
+    const uint32_t hi = (i & 1) ? w[B + 3] : w[B + 2];
+    return (i & 2) ? hi : lo;
+}
+
+// w[B + 2 i] for i in 0..3 (B fixed).
+template <int B, int N>
+__device__ __forceinline__ uint32_t pick4s2(const uint32_t (&w)[N], int i) {
+    const uint32_t lo = (i & 1) ? w[B + 2] : w[B];
+    const uint32_t hi = (i & 1) ? w[B + 6] : w[B + 4];
+    return (i & 2) ? hi : lo;
 }
 
 // One warp tile = 32 queries.  Phase 1 takes one lane per query; phase 2 a
@@ -524,10 +532,10 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 c += (((uint64_t)w[s][2 * i + 1] << 32) | w[s][2 * i]) < key ? 1 : 0;
             c = __shfl_sync(0xffffffffu, c, p0);
             // this lane's fields of segment c, then the partner's
-            const uint32_t f0 = hl ? pick(w[s], c) : pick(w[s], 2 * c);          // slope | key lo
-            const uint32_t f1 = hl ? pick(w[s], 4 + c) : pick(w[s], 2 * c + 1);  // icpt | key hi
-            const uint32_t f2 = pick(w[s], 8 + c);                                // eps | r_lo
-            const uint32_t f3 = hl ? 0u : pick(w[s], 12 + c);                     // - | cnt
+            const uint32_t f0 = hl ? pick4<0>(w[s], c) : pick4s2<0>(w[s], c);  // slope | key lo
+            const uint32_t f1 = hl ? pick4<4>(w[s], c) : pick4s2<1>(w[s], c);  // icpt | key hi
+            const uint32_t f2 = pick4<8>(w[s], c);                             // eps | r_lo
+            const uint32_t f3 = pick4<12>(w[s], c);                            // pad | cnt
             const uint32_t g0 = __shfl_xor_sync(0xffffffffu, f0, 1);
             const uint32_t g1 = __shfl_xor_sync(0xffffffffu, f1, 1);
             const uint32_t g2 = __shfl_xor_sync(0xffffffffu, f2, 1);
@@ -578,13 +586,19 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                     const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
                     const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
                     const uint32_t qd2 = qd | (qd << 16);
+                    // two packed counters: subtracting a compare's all-ones
+                    // half adds one to that half
+                    uint32_t acc = 0;
 #pragma unroll
-                    for (int w2 = 0; w2 < 16; w2++) {
-                        uint32_t le = __vcmpleu2(cw[s][w2], qd2);
-                        if (hl == 0) le = w2 < 2 ? 0u : (w2 == 2 ? (le & 0xFFFF0000u) : le);
-                        c += __popc(le);
+                    for (int w2 = 3; w2 < 16; w2++) acc = __vsub2(acc, __vcmpleu2(cw[s][w2], qd2));
+                    uint32_t head = __vcmpleu2(cw[s][2], qd2);  // lane 0: shift | slot 0
+                    if (hl == 0) head &= 0xFFFF0000u;
+                    acc = __vsub2(acc, head);
+                    if (hl) {
+                        acc = __vsub2(acc, __vcmpleu2(cw[s][0], qd2));
+                        acc = __vsub2(acc, __vcmpleu2(cw[s][1], qd2));
                     }
-                    c >>= 4;  // 16 set bits per slot
+                    c = (acc & 0xFFFFu) + (acc >> 16);
                 }
                 c += __shfl_xor_sync(0xffffffffu, c, 1);
                 if (act) {
@@ -628,10 +642,11 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 K lastk = 0;
                 if (key_lane) {
 #pragma unroll
-                    for (int i = LG::S - 1; i >= 0; i--) {
-                        const K k = key_at<K>(u[s], i);
-                        if (k == qv[s] && (!last_unit || r0 + i < n)) pos = i;
-                    }
+                    for (int i = LG::S - 1; i >= 0; i--)
+                        if (key_at<K>(u[s], i) == qv[s]) pos = i;
+                    // the last unit's padding slots hold all-ones keys, which a
+                    // query may equal: a match there is no key
+                    if (last_unit && pos >= 0 && r0 + (uint64_t)pos >= n) pos = -1;
                     lastk = key_at<K>(u[s], LG::S - 1);
                 }
                 // the unit's largest key (read only for units before the last,
@@ -664,11 +679,19 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                             if (byte / 64 == hl) vw = (byte % 64) / 4;
                         }
                         if (vw >= 0) {
+                            // vw is 8 + (slot) * VW in a block lane, or any
+                            // even word of the half in the one-block layout
                             V val;
                             if constexpr (sizeof(V) == 4) {
-                                val = pick(u[s], vw);
+                                const int i = vw & 7;
+                                const uint32_t a = pick4<8>(u[s], i & 3), b = pick4<12>(u[s], i & 3);
+                                val = (i & 4) ? b : a;
                             } else {
-                                val = ((uint64_t)pick(u[s], vw + 1) << 32) | pick(u[s], vw);
+                                const int i = (vw >> 1) & 3;
+                                const bool high = vw >= 8;
+                                const uint32_t lo = high ? pick4s2<8>(u[s], i) : pick4s2<0>(u[s], i);
+                                const uint32_t hi = high ? pick4s2<9>(u[s], i) : pick4s2<1>(u[s], i);
+                                val = ((uint64_t)hi << 32) | lo;
                             }
                             out[qi] = val;
                         }
