@@ -299,14 +299,21 @@ __global__ void seg_eps_kernel(const unsigned char *__restrict__ leaves, uint32_
 }
 
 // Staged keys (first key of every segment line) and the root's training
-// pairs (x = normalised key, y = the line's centre in [0, 1)).
+// pairs (x = normalised key, y = the line's centre in [0, 1)).  The staged
+// array is stored already swizzled (entry l at slot swz(l), all-ones keys in
+// the padding up to ns entries), so the search copies it to shared memory
+// verbatim.
 template <typename K>
-__global__ void stage_kernel(const SegLine *__restrict__ seg, uint32_t nls, uint64_t kmin,
-                             float xscale, K *__restrict__ stage, float *__restrict__ x,
-                             float *__restrict__ y) {
-    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nls; l += gridDim.x * blockDim.x) {
+__global__ void stage_kernel(const SegLine *__restrict__ seg, uint32_t nls, uint32_t ns,
+                             uint64_t kmin, float xscale, K *__restrict__ stage,
+                             float *__restrict__ x, float *__restrict__ y) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < ns; l += gridDim.x * blockDim.x) {
+        if (l >= nls) {
+            stage[swz<K>(l)] = key_max<K>();
+            continue;
+        }
         const uint64_t k = seg[l].key[0];
-        stage[l] = (K)k;
+        stage[swz<K>(l)] = (K)k;
         x[l] = norm_key(k, kmin, xscale);
         y[l] = (float)(((double)l + 0.5) / (double)nls);
     }
@@ -364,9 +371,14 @@ __global__ void code_kernel(const unsigned char *__restrict__ leaves, uint64_t n
 
 // 32-byte load of an index line piece: read-only path, no L1 allocation,
 // kept in L2 ahead of the streaming leaf reads (evict-last).
-__device__ __forceinline__ void load_line32(const void *p, uint32_t (&w)[8]) {
+__device__ __forceinline__ uint64_t l2_evict_last() {
     uint64_t pol;
     asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ void load_line32(const void *p, uint32_t (&w)[8],
+                                            uint64_t pol = l2_evict_last()) {
     asm volatile(
         "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
         : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]),
@@ -375,12 +387,13 @@ __device__ __forceinline__ void load_line32(const void *p, uint32_t (&w)[8]) {
 }
 
 // 32-byte load of a leaf-unit piece (touched once per query): evict-first.
-__device__ __forceinline__ void load_unit32(const void *p, uint32_t (&w)[8]) {
+__device__ __forceinline__ void load_unit32(const void *p, uint32_t (&w)[8],
+                                            uint64_t pol = l2_evict_first()) {
     asm volatile(
         "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
         : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]),
           "=r"(w[7])
-        : "l"(p), "l"(l2_evict_first()));
+        : "l"(p), "l"(pol));
 }
 
 
@@ -416,10 +429,11 @@ __device__ V tree_point(const DevTree &t, K q) {
 }
 
 // 64-byte half of an index line: two 32-byte loads, evict-last in L2.
-__device__ __forceinline__ void load_half_line(const unsigned char *p, uint32_t (&w)[16]) {
+__device__ __forceinline__ void load_half_line(const unsigned char *p, uint32_t (&w)[16],
+                                               uint64_t pol) {
     uint32_t a[8], b[8];
-    load_line32(p, a);
-    load_line32(p + 32, b);
+    load_line32(p, a, pol);
+    load_line32(p + 32, b, pol);
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         w[i] = a[i];
@@ -428,10 +442,11 @@ __device__ __forceinline__ void load_half_line(const unsigned char *p, uint32_t 
 }
 
 // 64-byte half of a leaf unit (touched once per query): evict-first.
-__device__ __forceinline__ void load_half_unit(const unsigned char *p, uint32_t (&w)[16]) {
+__device__ __forceinline__ void load_half_unit(const unsigned char *p, uint32_t (&w)[16],
+                                               uint64_t pol) {
     uint32_t a[8], b[8];
-    load_unit32(p, a);
-    load_unit32(p + 32, b);
+    load_unit32(p, a, pol);
+    load_unit32(p + 32, b, pol);
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         w[i] = a[i];
@@ -440,6 +455,54 @@ __device__ __forceinline__ void load_half_unit(const unsigned char *p, uint32_t 
 }
 
 // w[B + i] for i in 0..3 (B fixed): three selects.
+// Copies `bytes` (a multiple of 128) from global `src` into shared `dst` with
+// bulk copies (cp.async.bulk, no multicast) completing on the mbarrier
+// `bar`; every thread of the CTA calls it.  The wait is bounded: if the copy
+// has not landed after kStageWaits polls, the CTA waits as long again (so
+// no copy is left in flight when it moves on) and returns false -- the
+// caller then answers its queries without the staged keys.
+constexpr uint32_t kStageWaits = 1u << 22;
+
+__device__ __forceinline__ bool stage_bulk(void *dst, const void *src, uint32_t bytes,
+                                           unsigned long long *bar) {
+    const uint32_t b = (uint32_t)__cvta_generic_to_shared(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes)
+                     : "memory");
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+        for (uint32_t off = 0; off < bytes; off += 32768u) {
+            const uint32_t nb = min(32768u, bytes - off);
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    d + off),
+                "l"(static_cast<const unsigned char *>(src) + off), "r"(nb), "r"(b)
+                : "memory");
+        }
+    }
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kStageWaits && !done; it++)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b)
+            : "memory");
+    if (!done) {  // wait once more for the copy in flight, then give up on it
+        uint32_t late = 0;
+        for (uint32_t it = 0; it < kStageWaits && !late; it++)
+            asm volatile(
+                "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+                : "=r"(late)
+                : "r"(b)
+                : "memory");
+    }
+    return __syncthreads_and(done != 0) != 0;
+}
+
 template <int B, int N>
 __device__ __forceinline__ uint32_t pick4(const uint32_t (&w)[N], int i) {
     const uint32_t lo = (i & 1) ? w[B + 1] : w[B];
@@ -470,19 +533,18 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     constexpr int BPU = kUnitBytes / LG::BS;    // blocks per unit (1 or 2)
     constexpr int VW = (int)sizeof(V) / 4;      // words per value
     extern __shared__ uint4 smem_l[];
+    __shared__ __align__(8) unsigned long long s_bar;
     K *s_stage = reinterpret_cast<K *>(smem_l);
     float *s_mlp = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem_l) + m.stage_bytes);
-    {
-        const K *src = static_cast<const K *>(m.stage);
-        const uint32_t ns = m.stage_bytes / sizeof(K);
-        for (uint32_t i = threadIdx.x; i < ns; i += blockDim.x)
-            s_stage[swz<K>(i)] = i < m.nls ? src[i] : key_max<K>();
-        for (int k = threadIdx.x; k < 3 * m.hidden + 1; k += blockDim.x) s_mlp[k] = m.mlp[k];
-    }
+    // the staged keys: one bulk copy of the (pre-swizzled) array, completing
+    // on an mbarrier; the MLP parameters meanwhile by plain loads
+    const bool staged = stage_bulk(s_stage, m.stage, m.stage_bytes, &s_bar);
+    for (int k = threadIdx.x; k < 3 * m.hidden + 1; k += blockDim.x) s_mlp[k] = m.mlp[k];
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
     const int pr = lane >> 1, hl = lane & 1, p0 = pr * 2;
+    const uint64_t pol_idx = l2_evict_last(), pol_leaf = l2_evict_first();
     const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
     const uint64_t leaf_bytes = t.n_sectors * (uint64_t)LG::BS;
     const uint64_t n = t.n;
@@ -496,6 +558,13 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         // ---- 1. root + staged keys: the query's segment line (one lane per query)
         const uint64_t my = base + lane;
         const K myq = my < nq ? q[my] : (K)0;
+        if (!staged) {  // the staged keys never arrived: the tree's full descent
+            if (my < nq) {
+                out[my] = tree_point<K, V>(t, myq);
+                n_fallback++;
+            }
+            continue;
+        }
         uint32_t my_sl;
         {
             const int pl = root_line(s_mlp, m.hidden, m.nls, norm_key((uint64_t)myq, m.kmin, m.xscale));
@@ -515,7 +584,8 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             qv[s] = __shfl_sync(0xffffffffu, myq, k);
             live[s] = base + k < nq;
             const uint32_t sl = __shfl_sync(0xffffffffu, my_sl, k);
-            if (live[s]) load_half_line(reinterpret_cast<const unsigned char *>(m.seg + sl) + hl * 64, w[s]);
+            if (live[s])
+                load_half_line(reinterpret_cast<const unsigned char *>(m.seg + sl) + hl * 64, w[s], pol_idx);
         }
         // ---- 2. segment -> rank window -> unit window [ua, ub]
         // lane 0 of a pair: key[0..3] (words 0-7), r_lo[4] (8-11), cnt[4] (12-15);
@@ -544,11 +614,13 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             const uint32_t r_lo = hl ? g2 : f2, cnt = hl ? g3 : f3;
             const float slope = __uint_as_float(hl ? f0 : g0), icpt = __uint_as_float(hl ? f1 : g1);
             const uint32_t eps = hl ? f2 : g2;
-            const float p = seg_pred(slope, icpt, cnt, fk, key);
-            const int64_t ra = (int64_t)r_lo + (int64_t)floorf(p) - (int64_t)eps - 1;
-            const int64_t rb = (int64_t)r_lo + (int64_t)ceilf(p) + (int64_t)eps + 1;
-            const uint32_t a_u = ra <= 0 ? 0u : (uint32_t)min((uint64_t)ra / KPU, (uint64_t)U - 1);
-            const uint32_t b_u = rb <= 0 ? 0u : (uint32_t)min((uint64_t)rb / KPU, (uint64_t)U - 1);
+            const float p = seg_pred(slope, icpt, cnt, fk, key);  // in [0, cnt]
+            // ranks [r_lo + floor(p) - eps - 1, r_lo + ceil(p) + eps + 1], clamped
+            const uint32_t lo_r = r_lo + (uint32_t)floorf(p), hi_r = r_lo + (uint32_t)ceilf(p);
+            const uint32_t ra = eps >= lo_r ? 0u : lo_r - eps - 1u;
+            const uint32_t rb = hi_r + eps + 1u < hi_r ? 0xFFFFFFFFu : hi_r + eps + 1u;
+            const uint32_t a_u = min(ra / (uint32_t)KPU, U - 1);
+            const uint32_t b_u = min(rb / (uint32_t)KPU, U - 1);
             ua[s] = a_u;
             ub[s] = b_u < a_u ? a_u : b_u;
             nlines[s] = (live[s] && ub[s] > ua[s])
@@ -568,7 +640,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 if (l < nlines[s])
                     load_half_line(reinterpret_cast<const unsigned char *>(m.codes + ua[s] / kCodesPerLine + l) +
                                        hl * 64,
-                                   cw[s]);
+                                   cw[s], pol_idx);
 #pragma unroll
             for (int s = 0; s < NQ; s++) {
                 const bool act = l < nlines[s];
@@ -585,20 +657,22 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 if (act && key >= lbase) {
                     const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
                     const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
-                    const uint32_t qd2 = qd | (qd << 16);
-                    // two packed counters: subtracting a compare's all-ones
-                    // half adds one to that half
-                    uint32_t acc = 0;
+                    // a word holds two slots (low half first); the high half
+                    // is <= qd iff the word is <= (qd << 16) | 0xFFFF, the
+                    // low half iff the word shifted up is
+                    const uint32_t lim = (qd << 16) | 0xFFFFu;
 #pragma unroll
-                    for (int w2 = 3; w2 < 16; w2++) acc = __vsub2(acc, __vcmpleu2(cw[s][w2], qd2));
-                    uint32_t head = __vcmpleu2(cw[s][2], qd2);  // lane 0: shift | slot 0
-                    if (hl == 0) head &= 0xFFFF0000u;
-                    acc = __vsub2(acc, head);
+                    for (int w2 = 3; w2 < 16; w2++)
+                        c += (cw[s][w2] <= lim ? 1u : 0u) + ((cw[s][w2] << 16) <= lim ? 1u : 0u);
+                    // lane 0: word 2 holds the shift (low) and slot 0 (high);
+                    // words 0-1 the base
+                    c += cw[s][2] <= lim ? 1u : 0u;
                     if (hl) {
-                        acc = __vsub2(acc, __vcmpleu2(cw[s][0], qd2));
-                        acc = __vsub2(acc, __vcmpleu2(cw[s][1], qd2));
+                        c += ((cw[s][2] << 16) <= lim ? 1u : 0u);
+#pragma unroll
+                        for (int w2 = 0; w2 < 2; w2++)
+                            c += (cw[s][w2] <= lim ? 1u : 0u) + ((cw[s][w2] << 16) <= lim ? 1u : 0u);
                     }
-                    c = (acc & 0xFFFFu) + (acc >> 16);
                 }
                 c += __shfl_xor_sync(0xffffffffu, c, 1);
                 if (act) {
@@ -625,7 +699,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             for (int s = 0; s < NQ; s++) {
                 const uint64_t off = (uint64_t)unit[s] * kUnitBytes + hl * 64;
                 if (pend[s] && off < leaf_bytes) {
-                    load_half_unit(leaves + off, u[s]);
+                    load_half_unit(leaves + off, u[s], pol_leaf);
                 } else {
 #pragma unroll
                     for (int k = 0; k < 16; k++) u[s][k] = 0xFFFFFFFFu;  // padding keys
@@ -945,8 +1019,8 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     float *x = (float *)bx.p, *y = (float *)by.p, *grad = (float *)bg.p, *loss = grad + np;
     unsigned int *err = (unsigned int *)berr.p;
     count_launch();
-    stage_kernel<K><<<grid_of(nls, 256), 256, 0, s>>>(st->d_seg, nls, kmin, xscale,
-                                                     (K *)st->d_stage, x, y);
+    stage_kernel<K><<<grid_of(stage_bytes / sizeof(K), 256), 256, 0, s>>>(
+        st->d_seg, nls, (uint32_t)(stage_bytes / sizeof(K)), kmin, xscale, (K *)st->d_stage, x, y);
 
     // ---- root: ramps tiling [0, 1] in equal steps with output weights 1/H
     // (the identity y = x: the untrained network), then Adam
