@@ -188,3 +188,43 @@ def test_reference_query_families(wl):
     mg = wl.reference_queries("multi_gaussian", n, mx)
     assert len(np.unique(mg)) <= 10  # five clusters of nearly one value each
     assert np.array_equal(wl.reference_queries("zipf", 1000, mx), wl.reference_queries("zipf", 1000, mx))
+
+
+def _line_fits(xs, ys, eps):
+    """Is there a line within eps of every point?  (LP feasibility)"""
+    from scipy.optimize import linprog
+    x = (xs - xs[0]).astype(np.float64)
+    y = ys.astype(np.float64)
+    a = np.vstack([np.c_[x, np.ones_like(x)], np.c_[-x, -np.ones_like(x)]])
+    b = np.r_[y + eps, eps - y]
+    r = linprog([0, 0], A_ub=a, b_ub=b, bounds=[(None, None), (None, None)], method="highs")
+    return r.status == 0
+
+
+@pytest.mark.parametrize("eps", [1, 4, 16])
+def test_pla_segments_are_feasible_and_maximal(orc, eps):
+    """Every segment of the oracle's error-bounded segmentation admits a line
+    within eps of its points, and none could take one more point."""
+    g = np.random.default_rng(eps)
+    keys = np.cumsum(np.floor(g.lognormal(4.0, 2.0, size=2500)).astype(np.uint64) + 1)
+    st, sl, ic = orc.pla_segments(keys, eps)
+    bounds = list(st.astype(np.int64)) + [len(keys)]
+    for s, e, slope, icpt in zip(bounds[:-1], bounds[1:], sl, ic):
+        r = np.arange(e - s, dtype=np.float64)
+        assert _line_fits(keys[s:e], r, eps)
+        # the line the oracle reports is itself within eps (float64 rounding aside)
+        pred = icpt + slope * (keys[s:e] - keys[s]).astype(np.float64)
+        assert np.max(np.abs(pred - r)) <= eps + 1e-6
+        if e < len(keys):
+            assert not _line_fits(keys[s:e + 1], np.arange(e + 1 - s, dtype=np.float64), eps)
+
+
+def test_pla_segment_counts_shrink_with_eps(orc):
+    keys = np.cumsum(np.floor(np.random.default_rng(2).lognormal(4.0, 2.0, size=1 << 18))
+                     .astype(np.uint64) + 1)
+    counts = [orc.pla_segments(keys, e, lines=False) for e in (8, 16, 64, 256)]
+    assert counts == sorted(counts, reverse=True) and counts[-1] < counts[0]
+    # chunking adds at most one segment per chunk boundary
+    full = orc.pla_segments(keys, 64, lines=False)
+    chunked = orc.pla_segments(keys, 64, chunk=1 << 14, lines=False)
+    assert full <= chunked <= full + (len(keys) >> 14)
