@@ -345,9 +345,11 @@ class Tree:
                "bt_point_search_learned")
         return out
 
-    def learned_set_shape(self, queries_in_flight):
-        """Learned search kernel shape: 1 or 2 queries in flight per lane pair."""
-        _check(lib().bt_learned_set_shape(self._h, queries_in_flight), "bt_learned_set_shape")
+    def learned_set_shape(self, shape):
+        """Learned search kernel shape (bt_learned_set_shape): 1 = one query in
+        flight per lane pair, 1024 threads; 2 = two, 512; 3 = one, 640;
+        4 = two, 384."""
+        _check(lib().bt_learned_set_shape(self._h, shape), "bt_learned_set_shape")
 
     def learned_last_stats(self):
         """(leaf units read beyond the first, queries that took the full descent)."""
@@ -643,6 +645,9 @@ def probe_lib():
         h.btp_measure_chain.restype = _I
         h.btp_measure_chain.argtypes = [_U64, _U64, _U64, ctypes.c_uint32, ctypes.c_uint32,
                                         ctypes.c_uint32, _I, ctypes.POINTER(ctypes.c_double)]
+        h.btp_measure_hops.restype = _I
+        h.btp_measure_hops.argtypes = [_U64, _U64, _U64, ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.POINTER(ctypes.c_double)]
         _probe = h
     return _probe
 
@@ -668,4 +673,20 @@ def measure_chain(line_bytes, leaf_bytes, n_queries=1 << 24, leaf_read=128, line
     _probe_check(probe_lib().btp_measure_chain(line_bytes, leaf_bytes, n_queries, leaf_read,
                                                lines_per_query, in_flight, int(warm),
                                                ctypes.byref(r)), "btp_measure_chain")
+    return r.value
+
+
+HOP_FORMS = {"lane": 0, "pair": 1, "bulk": 2, "quad": 3, "pair_quad": 4}
+
+
+def measure_hops(line_bytes, leaf_bytes, n_queries=1 << 24, hops=2, form="bulk"):
+    """Queries per second of "`hops` dependent random 128-byte lines from an
+    L2-sized array, then one dependent random 128-byte read from a large
+    region", read by a lane per query ("lane"), a lane pair ("pair"), a lane
+    whose lines arrive in shared memory by bulk copies ("bulk"), a lane quad
+    ("quad"), or pairs for the lines and quads for the last read ("pair_quad")
+    (btp_measure_hops)."""
+    r = ctypes.c_double(0)
+    _probe_check(probe_lib().btp_measure_hops(line_bytes, leaf_bytes, n_queries, hops,
+                                              HOP_FORMS[form], ctypes.byref(r)), "btp_measure_hops")
     return r.value

@@ -19,8 +19,10 @@ import os
 import statistics
 
 SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
-# learned search: (lanes per query, queries in flight per lane pair)
-LEARNED_SHAPES = ((2, 1), (2, 2))
+# learned search: (lanes per query in the index-line steps, kernel shape of
+# bt_learned_set_shape: 1 = one query in flight per lane pair with 1024
+# threads, 2 = two with 512, 3 = one with 640, 4 = two with 384)
+LEARNED_SHAPES = ((2, 1), (2, 2), (2, 3), (2, 4))
 
 
 def _key(tree, mode, nq):
@@ -49,8 +51,8 @@ def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, confi
 
     mode: "basic" / "grouped" / "learned" (point search; `queries` a CUDA
     tensor), or "range" (`queries` = lo, `hi` = hi).  Returns (lanes, slots,
-    {cfg: ms}); for "learned", slots is the learned kernel's queries in
-    flight per lane group.
+    {cfg: ms}); for "learned", slots is the learned kernel's shape
+    (LEARNED_SHAPES).
     """
     import torch
     set_cfg = tree.set_search_config

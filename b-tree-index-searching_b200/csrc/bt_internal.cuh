@@ -89,7 +89,12 @@ struct SegLine {
 // Thresholds between consecutive leaf units, 59 per 128-byte line.
 // Threshold j separates unit j from unit j + 1: T_j = base + (code << shift)
 // is the smallest such value above the largest key of unit j, so q >= T_j
-// iff q >= base and ((q - base) >> shift) >= code.
+// iff q >= base and ((q - base) >> shift) >= code.  Codes are 15-bit values
+// (at most kCodeMax; kCodePad marks a slot past the last threshold), so that
+// two of them in a 32-bit word compare against the key in one subtraction.
+constexpr uint32_t kCodeMax = 0x7FFEu;
+constexpr uint32_t kCodePad = 0x7FFFu;
+
 struct CodeLine {
     uint64_t base;
     uint16_t shift;

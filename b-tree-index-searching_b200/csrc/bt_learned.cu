@@ -45,7 +45,7 @@ struct LearnedState {
     void *d_stage = nullptr;
     unsigned long long *d_stats = nullptr;
     uint64_t bytes = 0;
-    int in_flight = 2;  // queries in flight per lane pair (bt_learned_set_shape)
+    int shape = 2;  // search kernel shape (bt_learned_set_shape)
     LearnedDev dev;
 };
 
@@ -65,26 +65,46 @@ constexpr uint64_t kPlaChunk = 1ull << 14;  // keys per segmentation thread
 constexpr int kHullCap = 32;                 // points per convex hull
 constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
 constexpr int kMaxWalk = 8;                  // extra units read before the full descent
-// Search CTA shapes (one CTA per SM: the staged keys): NQ queries in flight
-// per lane pair, 1024 / NQ threads.
-template <int NQ>
-struct LShape {
-    static constexpr int kThreads = NQ == 1 ? 1024 : 512;
-};
+// Search CTA shapes (one CTA per SM: the staged keys), bt_learned_set_shape:
+// 1 = one query in flight per lane pair, 1024 threads; 2 = two, 512 threads;
+// 3 = one, 640 threads; 4 = two, 384 threads (fewer threads, more registers
+// per thread).
+constexpr int kLearnedShapes = 4;
 
 // ---------------------------------------------------------------- model ---
 
 // Root model in FP32 with explicit round-to-nearest operations (the same
 // arithmetic at training-time error measurement and in the search).
 // Units are ramps, clamp(w1 x + b1, 0, 1): with w1, w2 >= 0 every term is
-// non-decreasing in x under round-to-nearest, so the network is monotone, and
+// non-decreasing in x under round-to-nearest (each fused multiply-add rounds
+// a non-decreasing exact value once), so the network is monotone, and
 // (unlike ReLUs with non-negative weights, whose sum is convex) a sum of
 // ramps can follow a CDF that bends both ways.
-__device__ __forceinline__ float mlp_eval(const float *p, int H, float x) {
-    float out = p[3 * H];
-    for (int j = 0; j < H; j++) {
-        const float h = __fadd_rn(__fmul_rn(p[j], x), p[H + j]);
-        out = __fadd_rn(out, __fmul_rn(p[2 * H + j], fminf(fmaxf(h, 0.f), 1.f)));
+//
+// Evaluated from the parameters packed one float4 per unit, (w1, b1, w2, 0),
+// with the units padded to a multiple of 4 by zero units (a zero unit adds
+// exactly 0): one shared-memory load and two fused multiply-adds per unit.
+constexpr int kMlpPack = 4;
+
+__host__ __device__ constexpr int mlp_units4(int H) { return (H + kMlpPack - 1) / kMlpPack * kMlpPack; }
+
+// Packs the flat parameters p = [w1[H], b1[H], w2[H], b2] into u[mlp_units4(H)]
+// (+ b2 in *b2); called by every thread of the block with its own index.
+__device__ __forceinline__ void pack_mlp(const float *p, int H, float4 *u, float *b2, int tid,
+                                         int nth) {
+    for (int k = tid; k < mlp_units4(H); k += nth)
+        u[k] = k < H ? make_float4(p[k], p[H + k], p[2 * H + k], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (tid == 0) *b2 = p[3 * H];
+}
+
+__device__ __forceinline__ float mlp_eval4(const float4 *u, int H4, float b2, float x) {
+    float out = b2;
+    for (int j = 0; j < H4; j += kMlpPack) {
+#pragma unroll
+        for (int k = 0; k < kMlpPack; k++) {
+            const float4 w = u[j + k];
+            out = __fmaf_rn(w.z, __saturatef(__fmaf_rn(w.x, x, w.y)), out);
+        }
     }
     return out;
 }
@@ -94,8 +114,8 @@ __device__ __forceinline__ float norm_key(uint64_t key, uint64_t kmin, float xsc
 }
 
 // Segment line predicted by the root for normalised key x.
-__device__ __forceinline__ int root_line(const float *p, int H, uint32_t nls, float x) {
-    const float y = __fmul_rn(mlp_eval(p, H, x), (float)nls);
+__device__ __forceinline__ int root_line(const float4 *u, int H4, float b2, uint32_t nls, float x) {
+    const float y = __fmul_rn(mlp_eval4(u, H4, b2, x), (float)nls);
     if (!(y > 0.f)) return 0;  // also NaN
     const float f = floorf(y);
     return f >= (float)nls ? (int)nls - 1 : (int)f;
@@ -322,12 +342,13 @@ __global__ void stage_kernel(const SegLine *__restrict__ seg, uint32_t nls, uint
 // Worst |root_line(x_l) - l| over the staged keys.
 __global__ void root_err_kernel(const float *__restrict__ p, int H, const float *__restrict__ x,
                                 uint32_t nls, unsigned int *__restrict__ err) {
-    __shared__ float sp[3 * kMaxHidden + 1];
-    for (int k = threadIdx.x; k < 3 * H + 1; k += blockDim.x) sp[k] = p[k];
+    __shared__ float4 su[mlp_units4(kMaxHidden)];
+    __shared__ float sb2;
+    pack_mlp(p, H, su, &sb2, threadIdx.x, blockDim.x);
     __syncthreads();
     unsigned int e = 0;
     for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nls; l += gridDim.x * blockDim.x) {
-        const int pl = root_line(sp, H, nls, x[l]);
+        const int pl = root_line(su, mlp_units4(H), sb2, nls, x[l]);
         const int d = pl - (int)l;
         e = max(e, (unsigned int)(d < 0 ? -d : d));
     }
@@ -337,8 +358,8 @@ __global__ void root_err_kernel(const float *__restrict__ p, int H, const float 
 
 // Code lines, one thread per line: thresholds j = 59 l .. 59 l + 58 (j <
 // units - 1) between unit j and unit j + 1.  base = first key of the line's
-// first unit; shift = the least that fits the line's span in 16 bits; code
-// = ((last key of unit j - base) >> shift) + 1, so T_j = base + (code <<
+// first unit; shift = the least for which every code fits kCodeMax; code =
+// ((last key of unit j - base) >> shift) + 1, so T_j = base + (code <<
 // shift) is the least multiple above unit j's keys.
 template <typename K, typename V>
 __global__ void code_kernel(const unsigned char *__restrict__ leaves, uint64_t n, uint64_t units,
@@ -353,10 +374,10 @@ __global__ void code_kernel(const unsigned char *__restrict__ leaves, uint64_t n
         const uint64_t top = (uint64_t)leaf_key<K, V>(leaves, min(j1 * KPU, n) - 1);
         const uint64_t span = top - cl.base;
         int sh = 0;
-        while ((span >> sh) >= 0xFFFFull) sh++;
+        while ((span >> sh) + 1 > kCodeMax) sh++;
         cl.shift = (uint16_t)sh;
         for (uint64_t j = j0; j < j0 + kCodesPerLine; j++) {
-            uint16_t c = 0xFFFF;
+            uint16_t c = (uint16_t)kCodePad;
             if (j < j1) {
                 const uint64_t last = (uint64_t)leaf_key<K, V>(leaves, (j + 1) * KPU - 1);
                 c = (uint16_t)(((last - cl.base) >> sh) + 1);
@@ -415,7 +436,7 @@ __device__ __forceinline__ uint32_t stage_search(const K *__restrict__ s, uint32
 
 // Scalar full descent of the tree for one query (the fallback).
 template <typename K, typename V>
-__device__ V tree_point(const DevTree &t, K q) {
+__device__ __noinline__ V tree_point(const DevTree &t, K q) {
     using LG = LeafGeom<K, V>;
     const K tmax = (K)t.max_key;
     if (q > tmax) return key_max<V>();
@@ -441,20 +462,6 @@ __device__ __forceinline__ void load_half_line(const unsigned char *p, uint32_t 
     }
 }
 
-// 64-byte half of a leaf unit (touched once per query): evict-first.
-__device__ __forceinline__ void load_half_unit(const unsigned char *p, uint32_t (&w)[16],
-                                               uint64_t pol) {
-    uint32_t a[8], b[8];
-    load_unit32(p, a, pol);
-    load_unit32(p + 32, b, pol);
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-        w[i] = a[i];
-        w[8 + i] = b[i];
-    }
-}
-
-// w[B + i] for i in 0..3 (B fixed): three selects.
 // Copies `bytes` (a multiple of 128) from global `src` into shared `dst` with
 // bulk copies (cp.async.bulk, no multicast) completing on the mbarrier
 // `bar`; every thread of the CTA calls it.  The wait is bounded: if the copy
@@ -503,6 +510,7 @@ __device__ __forceinline__ bool stage_bulk(void *dst, const void *src, uint32_t 
     return __syncthreads_and(done != 0) != 0;
 }
 
+// w[B + i] for i in 0..3 (B fixed): three selects.
 template <int B, int N>
 __device__ __forceinline__ uint32_t pick4(const uint32_t (&w)[N], int i) {
     const uint32_t lo = (i & 1) ? w[B + 1] : w[B];
@@ -524,23 +532,25 @@ __device__ __forceinline__ uint32_t pick4s2(const uint32_t (&w)[N], int i) {
 // queries p and p + 16 of the tile and keeps NQ of them in flight (2 / NQ
 // passes per tile).  With a leaf unit of two blocks each lane holds a whole
 // block -- its keys and their values -- and answers its own matches.
-template <typename K, typename V, int NQ>
-__global__ void __launch_bounds__(LShape<NQ>::kThreads, 1)
+template <typename K, typename V, int NQ, int T>
+__global__ void __launch_bounds__(T, 1)
 learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
                const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
     using LG = LeafGeom<K, V>;
     constexpr int KPU = unit_keys<K, V>();      // keys per unit
     constexpr int BPU = kUnitBytes / LG::BS;    // blocks per unit (1 or 2)
-    constexpr int VW = (int)sizeof(V) / 4;      // words per value
     extern __shared__ uint4 smem_l[];
     __shared__ __align__(8) unsigned long long s_bar;
+    __shared__ float4 s_mlp[mlp_units4(kMaxHidden)];
+    __shared__ float s_b2;
     K *s_stage = reinterpret_cast<K *>(smem_l);
-    float *s_mlp = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(smem_l) + m.stage_bytes);
     // the staged keys: one bulk copy of the (pre-swizzled) array, completing
     // on an mbarrier; the MLP parameters meanwhile by plain loads
     const bool staged = stage_bulk(s_stage, m.stage, m.stage_bytes, &s_bar);
-    for (int k = threadIdx.x; k < 3 * m.hidden + 1; k += blockDim.x) s_mlp[k] = m.mlp[k];
+    pack_mlp(m.mlp, (int)m.hidden, s_mlp, &s_b2, threadIdx.x, blockDim.x);
     __syncthreads();
+    const int H4 = mlp_units4((int)m.hidden);
+    const float b2 = s_b2;
 
     const int lane = threadIdx.x & 31;
     const int pr = lane >> 1, hl = lane & 1, p0 = pr * 2;
@@ -567,7 +577,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         }
         uint32_t my_sl;
         {
-            const int pl = root_line(s_mlp, m.hidden, m.nls, norm_key((uint64_t)myq, m.kmin, m.xscale));
+            const int pl = root_line(s_mlp, H4, b2, m.nls, norm_key((uint64_t)myq, m.kmin, m.xscale));
             const int e = (int)m.root_err + 1;
             const uint32_t a = (uint32_t)max(0, pl - e);
             const uint32_t b = (uint32_t)min((int)m.nls - 1, pl + e);
@@ -656,23 +666,20 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 uint32_t c = 0;
                 if (act && key >= lbase) {
                     const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
-                    const uint32_t qd = d >= 0xFFFFull ? 0xFFFFu : (uint32_t)d;
-                    // a word holds two slots (low half first); the high half
-                    // is <= qd iff the word is <= (qd << 16) | 0xFFFF, the
-                    // low half iff the word shifted up is
-                    const uint32_t lim = (qd << 16) | 0xFFFFu;
+                    const uint32_t qd = d >= kCodeMax ? kCodeMax : (uint32_t)d;
+                    // a word holds two 15-bit codes; in (0x8000 + qd) - code
+                    // per half no borrow crosses the halves, and bit 15 of a
+                    // half is set iff code <= qd
+                    const uint32_t qq2 = (qd | (qd << 16)) | 0x80008000u;
+                    // lane 0: words 0-1 hold the base and the low half of
+                    // word 2 the shift -- made codes that never count
+                    const uint32_t w0 = hl ? cw[s][0] : 0x7FFF7FFFu;
+                    const uint32_t w1 = hl ? cw[s][1] : 0x7FFF7FFFu;
+                    const uint32_t w2x = hl ? cw[s][2] : (cw[s][2] | 0x7FFFu);
+                    c = __popc((qq2 - w0) & 0x80008000u) + __popc((qq2 - w1) & 0x80008000u) +
+                        __popc((qq2 - w2x) & 0x80008000u);
 #pragma unroll
-                    for (int w2 = 3; w2 < 16; w2++)
-                        c += (cw[s][w2] <= lim ? 1u : 0u) + ((cw[s][w2] << 16) <= lim ? 1u : 0u);
-                    // lane 0: word 2 holds the shift (low) and slot 0 (high);
-                    // words 0-1 the base
-                    c += cw[s][2] <= lim ? 1u : 0u;
-                    if (hl) {
-                        c += ((cw[s][2] << 16) <= lim ? 1u : 0u);
-#pragma unroll
-                        for (int w2 = 0; w2 < 2; w2++)
-                            c += (cw[s][w2] <= lim ? 1u : 0u) + ((cw[s][w2] << 16) <= lim ? 1u : 0u);
-                    }
+                    for (int w2 = 3; w2 < 16; w2++) c += __popc((qq2 - cw[s][w2]) & 0x80008000u);
                 }
                 c += __shfl_xor_sync(0xffffffffu, c, 1);
                 if (act) {
@@ -685,109 +692,119 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 }
             }
         }
-        // ---- 4. the leaf unit (walking right past a threshold bucket)
-        uint32_t unit[NQ];
-        bool pend[NQ];
+        // ---- 4. the leaf unit (walking right past a threshold bucket), read
+        // by lane quads: quad g takes the queries of pairs g and 8 + g, lane
+        // part p of the quad bytes 32 p .. 32 p + 31 of each unit, so that a
+        // unit is one request of one load instruction
+        {
+        constexpr int M = 2 * NQ;                 // queries per quad
+        const int g = lane >> 2, part = lane & 3;
+        // a key part holds the keys of block `blk` of the unit
+        const bool key_part = (part * 32) % LG::BS == 0;
+        const int blk = part * 32 / LG::BS;
+        uint32_t un[M], ubq[M];
+        K qq[M];
+        bool pend[M], lost_q[M];
 #pragma unroll
         for (int s = 0; s < NQ; s++) {
-            unit[s] = ua[s] + skip[s];
-            pend[s] = live[s];
-        }
-        for (int it = 0; it <= kMaxWalk; it++) {
-            uint32_t u[NQ][16];
 #pragma unroll
-            for (int s = 0; s < NQ; s++) {
-                const uint64_t off = (uint64_t)unit[s] * kUnitBytes + hl * 64;
-                if (pend[s] && off < leaf_bytes) {
-                    load_half_unit(leaves + off, u[s], pol_leaf);
+            for (int h = 0; h < 2; h++) {
+                const int m2 = s * 2 + h, src = 2 * (8 * h + g);
+                un[m2] = __shfl_sync(0xffffffffu, ua[s] + skip[s], src);
+                ubq[m2] = __shfl_sync(0xffffffffu, ub[s], src);
+                pend[m2] = __shfl_sync(0xffffffffu, live[s] ? 1u : 0u, src) != 0;
+                lost_q[m2] = false;
+                if constexpr (sizeof(K) == 8)
+                    qq[m2] = ((K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)qv[s] >> 32), src) << 32) |
+                             __shfl_sync(0xffffffffu, (uint32_t)qv[s], src);
+                else
+                    qq[m2] = (K)__shfl_sync(0xffffffffu, (uint32_t)qv[s], src);
+            }
+        }
+#pragma unroll 1
+        for (int it = 0; it <= kMaxWalk; it++) {
+            uint32_t u[M][8];
+#pragma unroll
+            for (int m2 = 0; m2 < M; m2++) {
+                const uint64_t off = (uint64_t)un[m2] * kUnitBytes + part * 32;
+                if (pend[m2] && off < leaf_bytes) {
+                    load_unit32(leaves + off, u[m2], pol_leaf);
                 } else {
 #pragma unroll
-                    for (int k = 0; k < 16; k++) u[s][k] = 0xFFFFFFFFu;  // padding keys
-                }
-            }
-#pragma unroll
-            for (int s = 0; s < NQ; s++) {
-                // this lane's keys: its block (two blocks per unit), or the
-                // unit's one block in lane 0
-                const bool key_lane = BPU == 2 || hl == 0;
-                const uint64_t r0 = (uint64_t)unit[s] * KPU + (BPU == 2 ? (uint64_t)hl * LG::S : 0);
-                const bool last_unit = unit[s] + 1 >= U;
-                int pos = -1;
-                K lastk = 0;
-                if (key_lane) {
-#pragma unroll
-                    for (int i = LG::S - 1; i >= 0; i--)
-                        if (key_at<K>(u[s], i) == qv[s]) pos = i;
-                    // the last unit's padding slots hold all-ones keys, which a
-                    // query may equal: a match there is no key
-                    if (last_unit && pos >= 0 && r0 + (uint64_t)pos >= n) pos = -1;
-                    lastk = key_at<K>(u[s], LG::S - 1);
-                }
-                // the unit's largest key (read only for units before the last,
-                // whose blocks are full): the last key of its last block
-                const int ll = BPU == 2 ? p0 + 1 : p0;
-                K ulast = (K)__shfl_sync(0xffffffffu, (uint32_t)lastk, ll);
-                if constexpr (sizeof(K) == 8)
-                    ulast |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)lastk >> 32), ll) << 32;
-                const unsigned pm = 0x3u << p0;
-                const unsigned mb = __ballot_sync(0xffffffffu, pend[s] && pos >= 0) & pm;
-                const bool found = mb != 0;
-                // duplicates across the two blocks: the first occurrence (lane 0's) answers
-                const bool my_match = BPU == 2 && pos >= 0 && lane == __ffs(mb) - 1;
-                // with one block per unit the match is in lane 0 and its value
-                // may be in lane 1 (value bytes 32 + 8 pos)
-                const int mpos = BPU == 1 ? __shfl_sync(0xffffffffu, pos, p0) : pos;
-                const bool walk = pend[s] && !found && qv[s] > ulast && !last_unit && unit[s] + 1 <= ub[s];
-                const bool lost = pend[s] && !found && qv[s] > ulast && !last_unit && unit[s] + 1 > ub[s];
-                const uint64_t qi = base + (hf * NQ + s) * 16 + pr;
-                if (pend[s] && !walk && !lost) {
-                    if (!found) {
-                        if (hl == 0) out[qi] = key_max<V>();
-                    } else {
-                        // words of the value at slot mpos, in the lane holding it
-                        int vw = -1;
-                        if (BPU == 2) {
-                            if (my_match) vw = (kSectorBytes / 4) + pos * VW;
-                        } else {
-                            const int byte = kSectorBytes + mpos * (int)sizeof(V);
-                            if (byte / 64 == hl) vw = (byte % 64) / 4;
-                        }
-                        if (vw >= 0) {
-                            // vw is 8 + (slot) * VW in a block lane, or any
-                            // even word of the half in the one-block layout
-                            V val;
-                            if constexpr (sizeof(V) == 4) {
-                                const int i = vw & 7;
-                                const uint32_t a = pick4<8>(u[s], i & 3), b = pick4<12>(u[s], i & 3);
-                                val = (i & 4) ? b : a;
-                            } else {
-                                const int i = (vw >> 1) & 3;
-                                const bool high = vw >= 8;
-                                const uint32_t lo = high ? pick4s2<8>(u[s], i) : pick4s2<0>(u[s], i);
-                                const uint32_t hi = high ? pick4s2<9>(u[s], i) : pick4s2<1>(u[s], i);
-                                val = ((uint64_t)hi << 32) | lo;
-                            }
-                            out[qi] = val;
-                        }
-                    }
-                    pend[s] = false;
-                } else if (walk) {
-                    unit[s]++;
-                    if (hl == 0 && it < kMaxWalk) n_extra++;
-                }
-                if (lost || (walk && it == kMaxWalk)) {
-                    // outside the window: the tree's full descent
-                    if (hl == 0) {
-                        out[qi] = tree_point<K, V>(t, qv[s]);
-                        n_fallback++;
-                    }
-                    pend[s] = false;
+                    for (int k = 0; k < 8; k++) u[m2][k] = 0xFFFFFFFFu;  // padding keys
                 }
             }
             bool any = false;
 #pragma unroll
-            for (int s = 0; s < NQ; s++) any |= pend[s];
+            for (int m2 = 0; m2 < M; m2++) {
+                const uint64_t r0 = (uint64_t)un[m2] * KPU + (uint64_t)blk * LG::S;
+                const bool last_unit = un[m2] + 1 >= U;
+                int pos = -1;
+                K lastk = 0;
+                if (key_part) {
+#pragma unroll
+                    for (int i = LG::S - 1; i >= 0; i--)
+                        if (key_at<K>(u[m2], i) == qq[m2]) pos = i;
+                    // the last unit's padding slots hold all-ones keys, which a
+                    // query may equal: a match there is no key
+                    if (last_unit && pos >= 0 && r0 + (uint64_t)pos >= n) pos = -1;
+                    lastk = key_at<K>(u[m2], LG::S - 1);
+                }
+                // matches of the quad: the first key part with one answers
+                // (block 0 before block 1: the first of equal keys)
+                const unsigned mb = (__ballot_sync(0xffffffffu, pend[m2] && pos >= 0) >> (4 * g)) & 0xFu;
+                const bool found = mb != 0;
+                const int kl = found ? __ffs(mb) - 1 : 0;
+                const int mpos = __shfl_sync(0xffffffffu, pos, 4 * g + kl);
+                // the unit's largest key (read only for units before the last,
+                // whose blocks are full): the last key of its last block
+                const int ll = 4 * g + (BPU == 2 ? 2 : 0);
+                K ulast = (K)__shfl_sync(0xffffffffu, (uint32_t)lastk, ll);
+                if constexpr (sizeof(K) == 8)
+                    ulast |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)lastk >> 32), ll) << 32;
+                const bool beyond = pend[m2] && !found && qq[m2] > ulast && !last_unit;
+                const bool walk = beyond && un[m2] + 1 <= ubq[m2];
+                const bool lost = beyond && un[m2] + 1 > ubq[m2];
+                const uint64_t qi = base + (hf * NQ + m2 / 2) * 16 + 8 * (m2 & 1) + g;
+                if (pend[m2] && !walk && !lost) {
+                    if (!found) {
+                        if (part == 0) out[qi] = key_max<V>();
+                    } else {
+                        // byte of the value within the unit: block kl / 2 (two
+                        // blocks) or 0, after its key sector
+                        const int byte = (kl * 32 / LG::BS) * LG::BS + kSectorBytes + mpos * (int)sizeof(V);
+                        if (byte / 32 == part) {
+                            const int wi = (byte % 32) / 4;
+                            V val;
+                            if constexpr (sizeof(V) == 4) {
+                                val = (wi & 4) ? pick4<4>(u[m2], wi & 3) : pick4<0>(u[m2], wi & 3);
+                            } else {
+                                const int i = wi >> 1;
+                                val = ((uint64_t)pick4s2<1>(u[m2], i) << 32) | pick4s2<0>(u[m2], i);
+                            }
+                            out[qi] = val;
+                        }
+                    }
+                    pend[m2] = false;
+                } else if (walk) {
+                    un[m2]++;
+                    if (part == 0 && it < kMaxWalk) n_extra++;
+                }
+                if (lost || (walk && it == kMaxWalk)) {
+                    lost_q[m2] = true;  // outside the window: answered below
+                    pend[m2] = false;
+                }
+                any |= pend[m2];
+            }
             if (!__any_sync(0xffffffffu, any)) break;
+        }
+#pragma unroll
+        for (int m2 = 0; m2 < M; m2++) {
+            if (lost_q[m2] && part == 0) {  // the tree's full descent
+                out[base + (hf * NQ + m2 / 2) * 16 + 8 * (m2 & 1) + g] = tree_point<K, V>(t, qq[m2]);
+                n_fallback++;
+            }
+        }
         }
         }  // passes of the tile
     }
@@ -797,13 +814,12 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     }
 }
 
-template <typename K, typename V, int NQ>
+template <typename K, typename V, int NQ, int T>
 bt_status learned_launch_nq(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
                             cudaStream_t s) {
     const LearnedDev &m = t->learned->dev;
-    constexpr int T = LShape<NQ>::kThreads;
-    auto fn = learned_kernel<K, V, NQ>;
-    const size_t smem = (size_t)m.stage_bytes + (3 * kMaxHidden + 1) * sizeof(float);
+    auto fn = learned_kernel<K, V, NQ, T>;
+    const size_t smem = (size_t)m.stage_bytes;
     static int set_for[64] = {0};
     int dev = t->device;
     if (dev >= 0 && dev < 64 && set_for[dev] < (int)smem) {
@@ -822,8 +838,12 @@ bt_status learned_launch_nq(const bt_tree *t, const void *d_q, uint64_t nq, void
 template <typename K, typename V>
 bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
                          cudaStream_t s) {
-    return t->learned->in_flight == 1 ? learned_launch_nq<K, V, 1>(t, d_q, nq, d_out, s)
-                                      : learned_launch_nq<K, V, 2>(t, d_q, nq, d_out, s);
+    switch (t->learned->shape) {
+        case 1: return learned_launch_nq<K, V, 1, 1024>(t, d_q, nq, d_out, s);
+        case 3: return learned_launch_nq<K, V, 1, 640>(t, d_q, nq, d_out, s);
+        case 4: return learned_launch_nq<K, V, 2, 384>(t, d_q, nq, d_out, s);
+        default: return learned_launch_nq<K, V, 2, 512>(t, d_q, nq, d_out, s);
+    }
 }
 
 // ------------------------------------------------------------- training ---
@@ -1179,12 +1199,12 @@ bt_status bt_point_search_learned(const bt_tree *t, const void *d_q, uint64_t nq
     return bt_point_search(t, BT_POINT_LEARNED, d_q, nq, d_out, stream);
 }
 
-bt_status bt_learned_set_shape(bt_tree *t, uint32_t queries_in_flight) {
+bt_status bt_learned_set_shape(bt_tree *t, uint32_t shape) {
     using namespace bt;
     if (!t || !t->learned) return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
-    if (queries_in_flight != 1 && queries_in_flight != 2)
-        return fail(BT_ERR_INVALID_ARGUMENT, "queries_in_flight must be 1 or 2");
-    t->learned->in_flight = (int)queries_in_flight;
+    if (shape < 1 || shape > (uint32_t)kLearnedShapes)
+        return fail(BT_ERR_INVALID_ARGUMENT, "shape must be 1..4");
+    t->learned->shape = (int)shape;
     return BT_OK;
 }
 

@@ -14,8 +14,18 @@
 //                       address depends on the loaded line (the leaf read).
 //                       Shows how the random DRAM rate holds up while a given
 //                       footprint of index lines is read from L2 beside it.
+//   btp_measure_hops    per query, `hops` DEPENDENT random 128-byte line reads
+//                       from an L2-sized array (each address depends on the
+//                       line before), then one dependent random 128-byte read
+//                       from a large region, in one of three forms: a lane
+//                       per query with 32-byte register loads, a lane pair
+//                       per query (64 bytes per lane), or a lane per query
+//                       whose lines arrive in its own shared-memory slot by
+//                       bulk copies (cp.async.bulk, completing on a per-lane
+//                       mbarrier; no multicast), a lane quad per query, or
+//                       lane pairs for the lines and quads for the last read.
 //
-// Both functions allocate their own buffers, flush L2 with a 512 MiB write
+// All functions allocate their own buffers, flush L2 with a 512 MiB write
 // between passes and return the best of three timed passes.  The extern "C"
 // declarations are below; they are not part of the engine's C ABI.
 #include <cuda_runtime.h>
@@ -110,6 +120,159 @@ chain_kernel(const unsigned char *__restrict__ lines, uint64_t nlines,
                 const uint4 y = ld_evict_first(leaves + b * LB + gl * 16);
                 acc ^= y.x ^ y.y ^ y.z ^ y.w;
             }
+        }
+    }
+    if (acc == 0x9E3779B9u) sink[0] = acc;
+}
+
+__device__ __forceinline__ void ld_line32(const void *p, uint32_t (&w)[8], uint64_t pol) {
+    asm volatile(
+        "ld.global.nc.L1::no_allocate.L2::cache_hint.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8], %9;"
+        : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]),
+          "=r"(w[7])
+        : "l"(p), "l"(pol));
+}
+
+__device__ __forceinline__ uint32_t xor8(const uint32_t (&w)[8]) {
+    return w[0] ^ w[1] ^ w[2] ^ w[3] ^ w[4] ^ w[5] ^ w[6] ^ w[7];
+}
+
+// XOR of `words` 32-byte pieces at p (registers, one lane).
+__device__ __forceinline__ uint32_t load_xor(const unsigned char *p, int pieces, uint64_t pol) {
+    uint32_t acc = 0;
+    for (int c = 0; c < pieces; c++) {
+        uint32_t w[8];
+        ld_line32(p + 32 * c, w, pol);
+        acc ^= xor8(w);
+    }
+    return acc;
+}
+
+constexpr uint32_t kHopWaits = 1u << 20;
+
+// Bounded wait for phase `par` of the mbarrier at shared address b; false if
+// it did not complete within kHopWaits polls.
+__device__ __forceinline__ bool bar_wait(uint32_t b, uint32_t par) {
+    uint32_t done = 0;
+    for (uint32_t it = 0; it < kHopWaits && !done; it++)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(b), "r"(par)
+            : "memory");
+    return done != 0;
+}
+
+// One 128-byte bulk copy global -> this lane's slot, completing on its mbarrier.
+__device__ __forceinline__ void bulk128(uint32_t slot, const void *src, uint32_t b) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], 128;" ::"r"(b) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], 128, [%2];" ::"r"(slot),
+        "l"(src), "r"(b)
+        : "memory");
+}
+
+// MODE 0: a lane per query, register loads (4 x 32 bytes per line).
+// MODE 1: a lane pair per query, 64 bytes per lane.
+// MODE 2: a lane per query, bulk copies into a 128-byte shared slot per lane.
+// MODE 3: a lane quad per query, 32 bytes per lane.
+// MODE 4: lane pairs for the line hops, lane quads for the final read.
+// Line addresses depend on the previous line's words (masked by `mask`, zero
+// at run time), so the reads of a query form a chain of hops + 1.
+template <int MODE, int HOPS>
+__global__ void __launch_bounds__(256)
+hop_kernel(const unsigned char *__restrict__ lines, uint64_t nlines,
+           const unsigned char *__restrict__ leaves, uint64_t nunits, uint64_t n, uint32_t mask,
+           uint64_t seed, uint32_t *__restrict__ sink) {
+    uint64_t pol_l, pol_f;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol_l));
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol_f));
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t nth = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t acc = 0;
+    if constexpr (MODE == 2) {
+        extern __shared__ __align__(128) unsigned char slots[];
+        __shared__ __align__(8) unsigned long long bars[256];
+        const uint32_t b = (uint32_t)__cvta_generic_to_shared(&bars[threadIdx.x]);
+        const uint32_t slot = (uint32_t)__cvta_generic_to_shared(slots + threadIdx.x * 128);
+        const uint4 *sp = reinterpret_cast<const uint4 *>(slots + threadIdx.x * 128);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        __syncwarp();
+        uint32_t par = 0;
+        for (uint64_t i = tid; i < n; i += nth) {
+            const uint64_t h = splitmix64(seed + i);
+            uint64_t li = h & (nlines - 1);
+            uint32_t w = 0;
+            for (int hop = 0; hop <= HOPS; hop++) {
+                const unsigned char *src =
+                    hop < HOPS ? lines + li * 128
+                               : leaves + ((splitmix64(~(seed + i)) ^ (w & mask)) & (nunits - 1)) * 128;
+                bulk128(slot, src, b);
+                if (!bar_wait(b, par)) {  // record, wait out the copy, stop
+                    atomicOr(sink + 1, 1u);
+                    bar_wait(b, par);
+                    return;
+                }
+                par ^= 1;
+                const uint4 x = sp[threadIdx.x & 7];
+                w = x.x ^ x.y ^ x.z ^ x.w;
+                if (hop < HOPS) li = (splitmix64(h + hop + 1) ^ (w & mask)) & (nlines - 1);
+            }
+            acc ^= w;
+        }
+    } else if constexpr (MODE == 4) {
+        // lane pairs for the hops; the final read by lane quads (a quad per
+        // query, 32 bytes per lane), the pair's address moved by shuffles
+        const int part = (int)(threadIdx.x & 1);
+        const int lane = (int)(threadIdx.x & 31);
+        const uint64_t warp = tid >> 5, nwarps = nth >> 5;
+        for (uint64_t base = warp * 16; base < n; base += nwarps * 16) {
+            const uint64_t i0 = base + (lane >> 1);
+            const bool live = i0 < n;
+            const uint64_t h = splitmix64(seed + i0);
+            uint64_t li = h & (nlines - 1);
+            uint32_t w = 0;
+            for (int hop = 0; hop < HOPS; hop++) {
+                if (live) w = load_xor(lines + li * 128 + part * 64, 2, pol_l);
+                w ^= __shfl_xor_sync(0xffffffffu, w, 1);
+                li = (splitmix64(h + hop + 1) ^ (w & mask)) & (nlines - 1);
+            }
+            const uint64_t leaf = (splitmix64(~(seed + i0)) ^ (w & mask)) & (nunits - 1);
+            for (int sub = 0; sub < 2; sub++) {
+                const int src = 2 * (8 * sub + (lane >> 2));
+                const uint64_t lf = ((uint64_t)__shfl_sync(0xffffffffu, (uint32_t)(leaf >> 32), src) << 32) |
+                                    __shfl_sync(0xffffffffu, (uint32_t)leaf, src);
+                if (base + 8 * sub + (lane >> 2) < n) {
+                    uint32_t y[8];
+                    ld_line32(leaves + lf * 128 + (lane & 3) * 32, y, pol_f);
+                    acc ^= xor8(y);
+                }
+            }
+        }
+    } else {
+        const int per = MODE == 0 ? 1 : MODE == 1 ? 2 : 4;  // lanes per query
+        const int part = (int)(threadIdx.x & (per - 1));
+        const int pieces = MODE == 0 ? 4 : MODE == 1 ? 2 : 1;
+        for (uint64_t i0 = tid / per; i0 < n; i0 += nth / per) {
+            const uint64_t h = splitmix64(seed + i0);
+            uint64_t li = h & (nlines - 1);
+            uint32_t w = 0;
+            for (int hop = 0; hop <= HOPS; hop++) {
+                const unsigned char *src =
+                    hop < HOPS ? lines + li * 128
+                               : leaves + ((splitmix64(~(seed + i0)) ^ (w & mask)) & (nunits - 1)) * 128;
+                w = load_xor(src + part * (128 / per), pieces, hop < HOPS ? pol_l : pol_f);
+                if (MODE == 1) w ^= __shfl_xor_sync(0x3u << (threadIdx.x & 30), w, 1);  // the group loops alike
+                if (MODE == 3) {
+                    const unsigned qm = 0xFu << (threadIdx.x & 28);
+                    w ^= __shfl_xor_sync(qm, w, 1);
+                    w ^= __shfl_xor_sync(qm, w, 2);
+                }
+                if (hop < HOPS) li = (splitmix64(h + hop + 1) ^ (w & mask)) & (nlines - 1);
+            }
+            acc ^= w;
         }
     }
     if (acc == 0x9E3779B9u) sink[0] = acc;
@@ -268,6 +431,74 @@ __attribute__((visibility("default"))) int btp_measure_chain(uint64_t line_bytes
         }
     }, warm != 0, &best);
     if (e != cudaSuccess) return fail("chain probe", e);
+    *queries_per_s = best > 0 ? (double)n_queries / (best * 1e-3) : 0.0;
+    return 0;
+}
+
+// Queries per second of the chain "hops dependent random 128-byte lines
+// from an array of line_bytes, then one dependent random 128-byte read from
+// a region of leaf_bytes" (both rounded down to powers of two), read in form
+// `mode`: 0 = a lane per query with register loads, 1 = a lane pair per
+// query, 2 = a lane per query with bulk copies into shared memory, 3 = a
+// lane quad per query, 4 = lane pairs for the lines and quads for the last
+// read.  The line
+// array starts each timed pass resident in L2.  Returns 0 on success; a bulk
+// wait that gives up is reported as a failure.
+__attribute__((visibility("default"))) int btp_measure_hops(uint64_t line_bytes, uint64_t leaf_bytes,
+                                                            uint64_t n_queries, uint32_t hops,
+                                                            uint32_t mode, double *queries_per_s) {
+    if (!queries_per_s) return fail("queries_per_s is NULL", cudaSuccess);
+    *queries_per_s = 0;
+    if (hops > 3 || mode > 4) return fail("hops must be 0..3 and mode 0..4", cudaSuccess);
+    auto pow2_floor = [](uint64_t v) { return v ? 1ull << (63 - __builtin_clzll(v)) : 0ull; };
+    const uint64_t nlines = pow2_floor(line_bytes / 128);
+    const uint64_t nunits = pow2_floor(leaf_bytes / 128);
+    if (nlines == 0 || nunits == 0 || n_queries == 0 || n_queries > (1ull << 30))
+        return fail("sizes out of range", cudaSuccess);
+    Bufs b;
+    cudaError_t e = cudaMalloc(&b.b, nunits * 128);
+    if (e == cudaSuccess) e = cudaMalloc(&b.a, nlines * 128);
+    if (e == cudaSuccess) e = cudaMalloc(&b.sink, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b.flush, kFlushBytes);
+    if (e == cudaSuccess) e = cudaMemset(b.b, 1, nunits * 128);
+    if (e == cudaSuccess) e = cudaMemset(b.a, 3, nlines * 128);
+    if (e == cudaSuccess) e = cudaMemset(b.sink, 0, 2 * sizeof(uint32_t));
+    if (e != cudaSuccess) return fail("allocation", e);
+    const unsigned grid = (unsigned)sm_count() * 8;
+    const size_t smem = mode == 2 ? 256 * 128 : 0;
+    auto run = [&](auto kern) {
+        kern<<<grid, 256, smem>>>(b.a, nlines, b.b, nunits, n_queries, 0u, 777, b.sink);
+    };
+    float best = 0;
+    e = time_best(b, [&] {
+        switch (mode * 10 + hops) {
+            case 0: run(hop_kernel<0, 0>); break;
+            case 1: run(hop_kernel<0, 1>); break;
+            case 2: run(hop_kernel<0, 2>); break;
+            case 3: run(hop_kernel<0, 3>); break;
+            case 10: run(hop_kernel<1, 0>); break;
+            case 11: run(hop_kernel<1, 1>); break;
+            case 12: run(hop_kernel<1, 2>); break;
+            case 13: run(hop_kernel<1, 3>); break;
+            case 20: run(hop_kernel<2, 0>); break;
+            case 21: run(hop_kernel<2, 1>); break;
+            case 22: run(hop_kernel<2, 2>); break;
+            case 23: run(hop_kernel<2, 3>); break;
+            case 30: run(hop_kernel<3, 0>); break;
+            case 31: run(hop_kernel<3, 1>); break;
+            case 32: run(hop_kernel<3, 2>); break;
+            case 33: run(hop_kernel<3, 3>); break;
+            case 40: run(hop_kernel<4, 0>); break;
+            case 41: run(hop_kernel<4, 1>); break;
+            case 42: run(hop_kernel<4, 2>); break;
+            default: run(hop_kernel<4, 3>); break;
+        }
+    }, true, &best);
+    if (e != cudaSuccess) return fail("hop probe", e);
+    uint32_t flags[2] = {0, 0};
+    e = cudaMemcpy(flags, b.sink, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail("hop probe", e);
+    if (flags[1]) return fail("hop probe: a bulk-copy wait gave up", cudaSuccess);
     *queries_per_s = best > 0 ? (double)n_queries / (best * 1e-3) : 0.0;
     return 0;
 }

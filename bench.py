@@ -809,7 +809,7 @@ def run_ours(args):
     clocks.start()
     at = importlib.import_module(PKG + ".autotune")
     p_lanes, p_rounds, _ = at.tune(tree, dq, mode="basic", repeats=3)
-    _, l_in_flight, l_tune_ms = at.tune(tree, dq, mode="learned", repeats=3)
+    _, l_shape, l_tune_ms = at.tune(tree, dq, mode="learned", repeats=3)
     for _ in range(max(args.warmup, 3)):
         search_learned()
     torch.cuda.synchronize(device)
@@ -946,7 +946,7 @@ def run_ours(args):
                                                   "code_lines_mean", "index_bytes",
                                                   "keys_per_unit", "train_ms")},
             "learned_stats": {"extra_unit_reads": extra, "full_descents": fallback},
-            "learned_shape": {"queries_in_flight_per_group": l_in_flight, "autotune_ms": l_tune_ms},
+            "learned_shape": {"shape": l_shape, "autotune_ms": l_tune_ms},
             "cpu_baseline": cpu,
             "cpu_sample_matches_gpu": checked,
             "clocks": clk,

@@ -342,11 +342,12 @@ BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, v
 BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
                                          void *d_out, void *stream);
 
-/* Shape of the learned search kernel: queries in flight per lane pair (two
- * lanes share a query), 1 (1024-thread CTAs) or 2 (512-thread CTAs; the
- * default).  Results do not depend on it; the autotuner picks the faster
- * one. */
-BT_API bt_status bt_learned_set_shape(bt_tree *tree, uint32_t queries_in_flight);
+/* Shape of the learned search kernel (one CTA per SM): 1 = one query in
+ * flight per lane pair (two lanes share a query), 1024-thread CTAs; 2 = two
+ * queries, 512 threads (the default); 3 = one query, 640 threads; 4 = two
+ * queries, 384 threads.  Fewer threads leave more registers to each.
+ * Results do not depend on it; the autotuner picks the fastest. */
+BT_API bt_status bt_learned_set_shape(bt_tree *tree, uint32_t shape);
 
 /* Counters of the last learned search on this tree: leaf units read beyond
  * the first one (keys just past a unit's threshold) and queries that took

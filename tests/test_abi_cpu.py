@@ -81,7 +81,8 @@ def test_probe_library_is_separate(bt, lib):
     assert not hasattr(lib, "bt_measure_gather")
     if os.path.exists(bt.PROBE_LIB_PATH):
         p = bt.probe_lib()
-        assert hasattr(p, "btp_measure_gather") and hasattr(p, "btp_measure_chain")
+        for name in ("btp_measure_gather", "btp_measure_chain", "btp_measure_hops"):
+            assert hasattr(p, name)
 
 
 def test_version_and_status_strings(lib):

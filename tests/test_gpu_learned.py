@@ -83,15 +83,16 @@ def test_learned_search_is_exact(bt, orc, cuda, kind, n, kt, vt, target):
             assert rep["max_error"] == target["max_error"]
         else:
             assert rep["num_segments"] <= target["num_segments"]
-        for shape in (1, 2):  # queries in flight per lane group
+        for shape in (1, 2, 3, 4):  # kernel shapes
             t.learned_set_shape(shape)
             got = t.point_search_learned(dev(q, cuda)).cpu().numpy()
             assert np.array_equal(got, exp), shape
             extra, fallback = t.learned_last_stats()
             assert fallback == 0  # the measured bounds always hold
             assert extra <= len(q) // 20
-        with pytest.raises(bt.BTreeError):
-            t.learned_set_shape(3)
+        for bad in (0, 5):
+            with pytest.raises(bt.BTreeError):
+                t.learned_set_shape(bad)
 
 
 def test_learned_with_duplicate_keys(bt, orc, cuda):

@@ -22,3 +22,12 @@ def test_chain_probe_measures_and_checks_arguments(bt, cuda):
         bt.measure_chain(8 << 20, 256 << 20, 1 << 20, 96, 1, 2)
     with pytest.raises(bt.BTreeError):
         bt.measure_chain(8 << 20, 256 << 20, 1 << 20, 128, 3, 2)
+
+
+@pytest.mark.parametrize("form", ["lane", "pair", "bulk", "quad", "pair_quad"])
+def test_hop_probe_measures_and_checks_arguments(bt, cuda, form):
+    for hops in (0, 1, 2, 3):
+        r = bt.measure_hops(8 << 20, 256 << 20, 1 << 20, hops, form)
+        assert 1e8 < r < 1e12
+    with pytest.raises(bt.BTreeError):
+        bt.measure_hops(8 << 20, 256 << 20, 1 << 20, 4, form)
