@@ -346,9 +346,8 @@ class Tree:
         return out
 
     def learned_set_shape(self, shape):
-        """Learned search kernel shape (bt_learned_set_shape): 1 = one query in
-        flight per lane pair, 1024 threads; 2 = two, 512; 3 = one, 640;
-        4 = two, 384."""
+        """Learned search kernel shape (bt_learned_set_shape): CTAs of 1024
+        (1), 768 (2), 640 (3) or 512 (4) threads."""
         _check(lib().bt_learned_set_shape(self._h, shape), "bt_learned_set_shape")
 
     def learned_last_stats(self):

@@ -20,8 +20,7 @@ import statistics
 
 SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
 # learned search: (lanes per query in the index-line steps, kernel shape of
-# bt_learned_set_shape: 1 = one query in flight per lane pair with 1024
-# threads, 2 = two with 512, 3 = one with 640, 4 = two with 384)
+# bt_learned_set_shape: CTAs of 1024, 768, 640 or 512 threads)
 LEARNED_SHAPES = ((2, 1), (2, 2), (2, 3), (2, 4))
 
 

@@ -45,7 +45,7 @@ struct LearnedState {
     void *d_stage = nullptr;
     unsigned long long *d_stats = nullptr;
     uint64_t bytes = 0;
-    int shape = 2;  // search kernel shape (bt_learned_set_shape)
+    int shape = 1;  // search kernel shape (bt_learned_set_shape)
     LearnedDev dev;
 };
 
@@ -66,9 +66,8 @@ constexpr int kHullCap = 32;                 // points per convex hull
 constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
 constexpr int kMaxWalk = 8;                  // extra units read before the full descent
 // Search CTA shapes (one CTA per SM: the staged keys), bt_learned_set_shape:
-// 1 = one query in flight per lane pair, 1024 threads; 2 = two, 512 threads;
-// 3 = one, 640 threads; 4 = two, 384 threads (fewer threads, more registers
-// per thread).
+// 1 = 1024 threads, 2 = 768, 3 = 640, 4 = 512 (fewer threads, more
+// registers per thread).
 constexpr int kLearnedShapes = 4;
 
 // ---------------------------------------------------------------- model ---
@@ -526,23 +525,206 @@ __device__ __forceinline__ uint32_t pick4s2(const uint32_t (&w)[N], int i) {
     return (i & 2) ? hi : lo;
 }
 
-// One warp tile = 32 queries.  Phase 1 takes one lane per query; phase 2 a
-// pair of lanes per query, each lane reading one 64-byte half of every
-// 128-byte line (segment line, code lines, leaf unit): lane pair p owns
-// queries p and p + 16 of the tile and keeps NQ of them in flight (2 / NQ
-// passes per tile).  With a leaf unit of two blocks each lane holds a whole
-// block -- its keys and their values -- and answers its own matches.
-template <typename K, typename V, int NQ, int T>
+// Count of the thresholds of code line `line` at or below `key`, for the
+// query of a lane pair (lane hl reads the 64-byte half hl; both lanes get
+// the count).  Called by the whole warp; `act` false gives 0 and no load.
+__device__ __forceinline__ uint32_t code_count(const CodeLine *__restrict__ codes, uint32_t line,
+                                               bool act, uint64_t key, int hl, int p0, uint64_t pol) {
+    uint32_t cw[16];
+    if (act) {
+        load_half_line(reinterpret_cast<const unsigned char *>(codes + line) + hl * 64, cw, pol);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 16; k++) cw[k] = 0;
+    }
+    const uint32_t b0 = __shfl_sync(0xffffffffu, cw[0], p0);
+    const uint32_t b1 = __shfl_sync(0xffffffffu, cw[1], p0);
+    const uint32_t shw = __shfl_sync(0xffffffffu, cw[2], p0);
+    const uint64_t lbase = ((uint64_t)b1 << 32) | b0;
+    // A line's codes never decrease, so those at or below the key's bucket
+    // are a prefix of its 59 slots (lane 0 of the pair holds slots 0-26
+    // after the base and the shift, lane 1 slots 27-58).
+    uint32_t c = 0;
+    if (act && key >= lbase) {
+        const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
+        const uint32_t qd = d >= kCodeMax ? kCodeMax : (uint32_t)d;
+        // a word holds two 15-bit codes; in (0x8000 + qd) - code per half
+        // no borrow crosses the halves, and bit 15 of a half is set iff
+        // code <= qd
+        const uint32_t qq2 = (qd | (qd << 16)) | 0x80008000u;
+        // lane 0: words 0-1 hold the base and the low half of word 2 the
+        // shift -- made codes that never count
+        const uint32_t w0 = hl ? cw[0] : 0x7FFF7FFFu;
+        const uint32_t w1 = hl ? cw[1] : 0x7FFF7FFFu;
+        const uint32_t w2 = hl ? cw[2] : (cw[2] | 0x7FFFu);
+        c = __popc((qq2 - w0) & 0x80008000u) + __popc((qq2 - w1) & 0x80008000u) +
+            __popc((qq2 - w2) & 0x80008000u);
+#pragma unroll
+        for (int k = 3; k < 16; k++) c += __popc((qq2 - cw[k]) & 0x80008000u);
+    }
+    return c + __shfl_xor_sync(0xffffffffu, c, 1);
+}
+
+// Thresholds of the unit window [ua, ub) among the first c of line j0 / 59.
+__device__ __forceinline__ uint32_t window_part(uint32_t ua, uint32_t ub, uint32_t j0, uint32_t c) {
+    const uint32_t lo = max(ua, j0), hi = min(ub, j0 + c);
+    return hi > lo ? hi - lo : 0u;
+}
+
+// A query whose unit window continues into the neighbouring code line, kept
+// in its warp's shared-memory queue until 16 of them fill a pass.
+struct Retry {
+    uint64_t key;   // the query key (zero-extended)
+    uint64_t qi;    // its index in the batch
+    uint32_t ua, ub;
+    uint32_t line;  // the code line still to count
+    uint32_t skip;  // thresholds of the window at or below the key so far
+};
+constexpr int kRetryCap = 32;  // entries per warp (at most 15 + 16 at once)
+
+// The leaf step of one pass: the query of every lane pair (live / unit / ub /
+// key / qi, as held by the pair) is answered from its leaf unit, walking
+// right past a threshold bucket.  Units are read by lane quads: quad g takes
+// the queries of pairs g and 8 + g, lane part p of the quad bytes 32 p ..
+// 32 p + 31 of the unit, so a unit is one request of one load instruction.
+// Queries whose answer lies outside their window are answered by the tree's
+// full descent.  Called by the whole warp.
+template <typename K, typename V>
+__device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_t pol, bool live,
+                                           uint32_t unit, uint32_t ub, K key, uint64_t qi,
+                                           V *__restrict__ out, unsigned long long &n_extra,
+                                           unsigned long long &n_fallback) {
+    using LG = LeafGeom<K, V>;
+    constexpr int KPU = unit_keys<K, V>();
+    constexpr int BPU = kUnitBytes / LG::BS;
+    const int lane = threadIdx.x & 31, g = lane >> 2, part = lane & 3;
+    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
+    const uint64_t leaf_bytes = t.n_sectors * (uint64_t)LG::BS;
+    // a key part holds the keys of block `blk` of the unit
+    const bool key_part = (part * 32) % LG::BS == 0;
+    const int blk = part * 32 / LG::BS;
+    uint32_t un[2], ubq[2];
+    K qq[2];
+    uint64_t qx[2];
+    bool pend[2], lost_q[2];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int src = 2 * (8 * h + g);  // lane 0 of the pair
+        un[h] = __shfl_sync(0xffffffffu, unit, src);
+        ubq[h] = __shfl_sync(0xffffffffu, ub, src);
+        pend[h] = __shfl_sync(0xffffffffu, live ? 1u : 0u, src) != 0;
+        lost_q[h] = false;
+        qx[h] = ((uint64_t)__shfl_sync(0xffffffffu, (uint32_t)(qi >> 32), src) << 32) |
+                __shfl_sync(0xffffffffu, (uint32_t)qi, src);
+        if constexpr (sizeof(K) == 8)
+            qq[h] = ((K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)key >> 32), src) << 32) |
+                    __shfl_sync(0xffffffffu, (uint32_t)key, src);
+        else
+            qq[h] = (K)__shfl_sync(0xffffffffu, (uint32_t)key, src);
+    }
+#pragma unroll 1
+    for (int it = 0; it <= kMaxWalk; it++) {
+        uint32_t u[2][8];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint64_t off = (uint64_t)un[h] * kUnitBytes + part * 32;
+            if (pend[h] && off < leaf_bytes) {
+                load_unit32(leaves + off, u[h], pol);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; k++) u[h][k] = 0xFFFFFFFFu;  // padding keys
+            }
+        }
+        bool any = false;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint64_t r0 = (uint64_t)un[h] * KPU + (uint64_t)blk * LG::S;
+            const bool last_unit = un[h] + 1 >= U;
+            int pos = -1;
+            K lastk = 0;
+            if (key_part) {
+#pragma unroll
+                for (int i = LG::S - 1; i >= 0; i--)
+                    if (key_at<K>(u[h], i) == qq[h]) pos = i;
+                // the last unit's padding slots hold all-ones keys, which a
+                // query may equal: a match there is no key
+                if (last_unit && pos >= 0 && r0 + (uint64_t)pos >= t.n) pos = -1;
+                lastk = key_at<K>(u[h], LG::S - 1);
+            }
+            // matches of the quad: the first key part with one answers
+            // (block 0 before block 1: the first of equal keys)
+            const unsigned mb = (__ballot_sync(0xffffffffu, pend[h] && pos >= 0) >> (4 * g)) & 0xFu;
+            const bool found = mb != 0;
+            const int kl = found ? __ffs(mb) - 1 : 0;
+            const int mpos = __shfl_sync(0xffffffffu, pos, 4 * g + kl);
+            // the unit's largest key (read only for units before the last,
+            // whose blocks are full): the last key of its last block
+            const int ll = 4 * g + (BPU == 2 ? 2 : 0);
+            K ulast = (K)__shfl_sync(0xffffffffu, (uint32_t)lastk, ll);
+            if constexpr (sizeof(K) == 8)
+                ulast |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)lastk >> 32), ll) << 32;
+            const bool beyond = pend[h] && !found && qq[h] > ulast && !last_unit;
+            const bool walk = beyond && un[h] + 1 <= ubq[h];
+            const bool lost = beyond && un[h] + 1 > ubq[h];
+            if (pend[h] && !walk && !lost) {
+                if (!found) {
+                    if (part == 0) out[qx[h]] = key_max<V>();
+                } else {
+                    // byte of the value within the unit: its block's value
+                    // array follows the block's key sector
+                    const int byte = (kl * 32 / LG::BS) * LG::BS + kSectorBytes + mpos * (int)sizeof(V);
+                    if (byte / 32 == part) {
+                        const int wi = (byte % 32) / 4;
+                        V val;
+                        if constexpr (sizeof(V) == 4) {
+                            val = (wi & 4) ? pick4<4>(u[h], wi & 3) : pick4<0>(u[h], wi & 3);
+                        } else {
+                            const int i = wi >> 1;
+                            val = ((uint64_t)pick4s2<1>(u[h], i) << 32) | pick4s2<0>(u[h], i);
+                        }
+                        out[qx[h]] = val;
+                    }
+                }
+                pend[h] = false;
+            } else if (walk) {
+                un[h]++;
+                if (part == 0 && it < kMaxWalk) n_extra++;
+            }
+            if (lost || (walk && it == kMaxWalk)) {
+                lost_q[h] = true;  // outside the window: answered below
+                pend[h] = false;
+            }
+            any |= pend[h];
+        }
+        if (!__any_sync(0xffffffffu, any)) break;
+    }
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        if (lost_q[h] && part == 0) {  // the tree's full descent
+            out[qx[h]] = tree_point<K, V>(t, qq[h]);
+            n_fallback++;
+        }
+    }
+}
+
+// One warp tile = 32 queries.  Phase 1 takes one lane per query (root
+// network, then the staged keys: the query's segment line); the rest runs in
+// two passes of 16 queries, a lane pair per query, each lane reading one
+// 64-byte half of the segment line and of a code line.  A query counts the
+// code line holding its predicted unit; when its window continues into the
+// neighbouring line and that line's count is needed, the query waits in its
+// warp's queue until 16 such queries make a pass of their own (so a pass
+// always counts one line per query).  Leaf units are read by lane quads.
+template <typename K, typename V, int T>
 __global__ void __launch_bounds__(T, 1)
 learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
                const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
-    using LG = LeafGeom<K, V>;
-    constexpr int KPU = unit_keys<K, V>();      // keys per unit
-    constexpr int BPU = kUnitBytes / LG::BS;    // blocks per unit (1 or 2)
+    constexpr int KPU = unit_keys<K, V>();  // keys per unit
     extern __shared__ uint4 smem_l[];
     __shared__ __align__(8) unsigned long long s_bar;
     __shared__ float4 s_mlp[mlp_units4(kMaxHidden)];
     __shared__ float s_b2;
+    __shared__ Retry s_retry[T / 32][kRetryCap];
     K *s_stage = reinterpret_cast<K *>(smem_l);
     // the staged keys: one bulk copy of the (pre-swizzled) array, completing
     // on an mbarrier; the MLP parameters meanwhile by plain loads
@@ -555,12 +737,57 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     const int lane = threadIdx.x & 31;
     const int pr = lane >> 1, hl = lane & 1, p0 = pr * 2;
     const uint64_t pol_idx = l2_evict_last(), pol_leaf = l2_evict_first();
-    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    const uint64_t leaf_bytes = t.n_sectors * (uint64_t)LG::BS;
-    const uint64_t n = t.n;
     const uint32_t U = (uint32_t)m.units;
     const uint64_t ntiles = (nq + 31) / 32;
+    Retry *rq = s_retry[threadIdx.x >> 5];
+    uint32_t qn = 0;  // entries in this warp's queue (the same in every lane)
     unsigned long long n_extra = 0, n_fallback = 0;
+
+    // Appends the queries of the pairs with `need` to the warp's queue (the
+    // line word carries the direction of the walk in its top bit).
+    auto enqueue = [&](bool need, uint64_t key, uint64_t qi, uint32_t ua, uint32_t ub,
+                       uint32_t line_dir, uint32_t skip) {
+        const unsigned qmask = __ballot_sync(0xffffffffu, hl == 0 && need);
+        if (hl == 0 && need) {
+            Retry e;
+            e.key = key;
+            e.qi = qi;
+            e.ua = ua;
+            e.ub = ub;
+            e.line = line_dir;
+            e.skip = skip;
+            rq[qn + __popc(qmask & ((1u << lane) - 1u))] = e;
+        }
+        qn += __popc(qmask);
+        __syncwarp();
+    };
+    // A pass of queued queries: pair pr takes entry first + pr (pr < cnt),
+    // the top of the queue, and counts the entry's line; a window that
+    // continues past that line as well goes back to the queue with the next
+    // line, the others are answered from the leaf.
+    auto retry_pass = [&](uint32_t first, uint32_t cnt) {
+        const bool live = (uint32_t)pr < cnt;
+        Retry e = {};
+        if (live) e = rq[first + pr];
+        __syncwarp();  // the entries are read before the queue is written again
+        qn = first;
+        const uint32_t line = e.line & 0x7FFFFFFFu;
+        const bool right = (e.line >> 31) != 0;
+        const uint32_t j0 = line * kCodesPerLine;
+        const uint32_t c = code_count(m.codes, line, live, e.key, hl, p0, pol_idx);
+        uint32_t skip = e.skip + window_part(e.ua, e.ub, j0, c);
+        const uint32_t la = e.ua / kCodesPerLine, lb = (e.ub - 1) / kCodesPerLine;
+        bool more;
+        if (right) {
+            more = live && line < lb && c >= kCodesPerLine;
+        } else {
+            more = live && line > la && c == 0;
+            if (live && line > la && c > 0) skip += j0 - e.ua;
+        }
+        enqueue(more, e.key, e.qi, e.ua, e.ub, right ? ((line + 1) | 0x80000000u) : line - 1, skip);
+        leaf_quads<K, V>(t, U, pol_leaf, live && !more, e.ua + skip, e.ub, (K)e.key, e.qi, out,
+                         n_extra, n_fallback);
+    };
 
     for (uint64_t tile = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; tile < ntiles;
          tile += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
@@ -584,38 +811,32 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             my_sl = stage_search<K>(s_stage, a, b, myq);
         }
 #pragma unroll 1
-        for (int hf = 0; hf < 2 / NQ; hf++) {
-        K qv[NQ];
-        bool live[NQ];
-        uint32_t w[NQ][16];
-#pragma unroll
-        for (int s = 0; s < NQ; s++) {
-            const int k = (hf * NQ + s) * 16 + pr;
-            qv[s] = __shfl_sync(0xffffffffu, myq, k);
-            live[s] = base + k < nq;
+        for (int hf = 0; hf < 2; hf++) {
+            const int k = hf * 16 + pr;
+            const K qv = __shfl_sync(0xffffffffu, myq, k);
+            const uint64_t qi = base + k;
+            const bool live = qi < nq;
             const uint32_t sl = __shfl_sync(0xffffffffu, my_sl, k);
-            if (live[s])
-                load_half_line(reinterpret_cast<const unsigned char *>(m.seg + sl) + hl * 64, w[s], pol_idx);
-        }
-        // ---- 2. segment -> rank window -> unit window [ua, ub]
-        // lane 0 of a pair: key[0..3] (words 0-7), r_lo[4] (8-11), cnt[4] (12-15);
-        // lane 1: slope[4] (0-3), icpt[4] (4-7), eps[4] (8-11)
-        uint32_t ua[NQ], ub[NQ];
-        int nlines[NQ];
-        int maxl = 0;
+            uint32_t w[16];
+            if (live) {
+                load_half_line(reinterpret_cast<const unsigned char *>(m.seg + sl) + hl * 64, w, pol_idx);
+            } else {
 #pragma unroll
-        for (int s = 0; s < NQ; s++) {
-            const uint64_t key = (uint64_t)qv[s];
+                for (int i = 0; i < 16; i++) w[i] = 0;
+            }
+            // ---- 2. segment -> rank window -> unit window [ua, ub]
+            // lane 0 of a pair: key[0..3] (words 0-7), r_lo[4] (8-11), cnt[4] (12-15);
+            // lane 1: slope[4] (0-3), icpt[4] (4-7), eps[4] (8-11)
+            const uint64_t key = (uint64_t)qv;
             int c = 0;
 #pragma unroll
-            for (int i = 1; i < kSegPerLine; i++)
-                c += (((uint64_t)w[s][2 * i + 1] << 32) | w[s][2 * i]) < key ? 1 : 0;
+            for (int i = 1; i < kSegPerLine; i++) c += (((uint64_t)w[2 * i + 1] << 32) | w[2 * i]) < key ? 1 : 0;
             c = __shfl_sync(0xffffffffu, c, p0);
             // this lane's fields of segment c, then the partner's
-            const uint32_t f0 = hl ? pick4<0>(w[s], c) : pick4s2<0>(w[s], c);  // slope | key lo
-            const uint32_t f1 = hl ? pick4<4>(w[s], c) : pick4s2<1>(w[s], c);  // icpt | key hi
-            const uint32_t f2 = pick4<8>(w[s], c);                             // eps | r_lo
-            const uint32_t f3 = pick4<12>(w[s], c);                            // pad | cnt
+            const uint32_t f0 = hl ? pick4<0>(w, c) : pick4s2<0>(w, c);  // slope | key lo
+            const uint32_t f1 = hl ? pick4<4>(w, c) : pick4s2<1>(w, c);  // icpt | key hi
+            const uint32_t f2 = pick4<8>(w, c);                          // eps | r_lo
+            const uint32_t f3 = pick4<12>(w, c);                         // pad | cnt
             const uint32_t g0 = __shfl_xor_sync(0xffffffffu, f0, 1);
             const uint32_t g1 = __shfl_xor_sync(0xffffffffu, f1, 1);
             const uint32_t g2 = __shfl_xor_sync(0xffffffffu, f2, 1);
@@ -629,184 +850,41 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             const uint32_t lo_r = r_lo + (uint32_t)floorf(p), hi_r = r_lo + (uint32_t)ceilf(p);
             const uint32_t ra = eps >= lo_r ? 0u : lo_r - eps - 1u;
             const uint32_t rb = hi_r + eps + 1u < hi_r ? 0xFFFFFFFFu : hi_r + eps + 1u;
-            const uint32_t a_u = min(ra / (uint32_t)KPU, U - 1);
-            const uint32_t b_u = min(rb / (uint32_t)KPU, U - 1);
-            ua[s] = a_u;
-            ub[s] = b_u < a_u ? a_u : b_u;
-            nlines[s] = (live[s] && ub[s] > ua[s])
-                            ? (int)((ub[s] - 1) / kCodesPerLine - ua[s] / kCodesPerLine) + 1
-                            : 0;
-            maxl = max(maxl, nlines[s]);
-        }
-        // ---- 3. code lines of the window: thresholds at or below the key
-        maxl = (int)__reduce_max_sync(0xffffffffu, (unsigned)maxl);
-        uint32_t skip[NQ];
-#pragma unroll
-        for (int s = 0; s < NQ; s++) skip[s] = 0;
-        for (int l = 0; l < maxl; l++) {
-            uint32_t cw[NQ][16];
-#pragma unroll
-            for (int s = 0; s < NQ; s++)
-                if (l < nlines[s])
-                    load_half_line(reinterpret_cast<const unsigned char *>(m.codes + ua[s] / kCodesPerLine + l) +
-                                       hl * 64,
-                                   cw[s], pol_idx);
-#pragma unroll
-            for (int s = 0; s < NQ; s++) {
-                const bool act = l < nlines[s];
-                const uint32_t b0 = __shfl_sync(0xffffffffu, act ? cw[s][0] : 0u, p0);
-                const uint32_t b1 = __shfl_sync(0xffffffffu, act ? cw[s][1] : 0u, p0);
-                const uint32_t shw = __shfl_sync(0xffffffffu, act ? cw[s][2] : 0u, p0);
-                const uint64_t lbase = ((uint64_t)b1 << 32) | b0;
-                const uint64_t key = (uint64_t)qv[s];
-                // A line's codes never decrease, so those at or below the
-                // key's bucket are a prefix of its 59 slots: count them two
-                // at a time (lane 0 of the pair holds slots 0-26 after the
-                // base and the shift, lane 1 slots 27-58).
-                uint32_t c = 0;
-                if (act && key >= lbase) {
-                    const uint64_t d = (key - lbase) >> (shw & 0xFFFFu);
-                    const uint32_t qd = d >= kCodeMax ? kCodeMax : (uint32_t)d;
-                    // a word holds two 15-bit codes; in (0x8000 + qd) - code
-                    // per half no borrow crosses the halves, and bit 15 of a
-                    // half is set iff code <= qd
-                    const uint32_t qq2 = (qd | (qd << 16)) | 0x80008000u;
-                    // lane 0: words 0-1 hold the base and the low half of
-                    // word 2 the shift -- made codes that never count
-                    const uint32_t w0 = hl ? cw[s][0] : 0x7FFF7FFFu;
-                    const uint32_t w1 = hl ? cw[s][1] : 0x7FFF7FFFu;
-                    const uint32_t w2x = hl ? cw[s][2] : (cw[s][2] | 0x7FFFu);
-                    c = __popc((qq2 - w0) & 0x80008000u) + __popc((qq2 - w1) & 0x80008000u) +
-                        __popc((qq2 - w2x) & 0x80008000u);
-#pragma unroll
-                    for (int w2 = 3; w2 < 16; w2++) c += __popc((qq2 - cw[s][w2]) & 0x80008000u);
-                }
-                c += __shfl_xor_sync(0xffffffffu, c, 1);
-                if (act) {
-                    // thresholds j0 .. j0 + c - 1 are at or below the key; keep
-                    // those of the window [ua, ub - 1]
-                    const uint32_t j0 = (ua[s] / kCodesPerLine + l) * kCodesPerLine;
-                    const uint32_t lo = max(ua[s], j0), hi = min(ub[s], j0 + kCodesPerLine);
-                    const uint32_t e = min(j0 + c, hi);
-                    skip[s] += e > lo ? e - lo : 0u;
-                }
-            }
-        }
-        // ---- 4. the leaf unit (walking right past a threshold bucket), read
-        // by lane quads: quad g takes the queries of pairs g and 8 + g, lane
-        // part p of the quad bytes 32 p .. 32 p + 31 of each unit, so that a
-        // unit is one request of one load instruction
-        {
-        constexpr int M = 2 * NQ;                 // queries per quad
-        const int g = lane >> 2, part = lane & 3;
-        // a key part holds the keys of block `blk` of the unit
-        const bool key_part = (part * 32) % LG::BS == 0;
-        const int blk = part * 32 / LG::BS;
-        uint32_t un[M], ubq[M];
-        K qq[M];
-        bool pend[M], lost_q[M];
-#pragma unroll
-        for (int s = 0; s < NQ; s++) {
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-                const int m2 = s * 2 + h, src = 2 * (8 * h + g);
-                un[m2] = __shfl_sync(0xffffffffu, ua[s] + skip[s], src);
-                ubq[m2] = __shfl_sync(0xffffffffu, ub[s], src);
-                pend[m2] = __shfl_sync(0xffffffffu, live[s] ? 1u : 0u, src) != 0;
-                lost_q[m2] = false;
-                if constexpr (sizeof(K) == 8)
-                    qq[m2] = ((K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)qv[s] >> 32), src) << 32) |
-                             __shfl_sync(0xffffffffu, (uint32_t)qv[s], src);
-                else
-                    qq[m2] = (K)__shfl_sync(0xffffffffu, (uint32_t)qv[s], src);
-            }
-        }
-#pragma unroll 1
-        for (int it = 0; it <= kMaxWalk; it++) {
-            uint32_t u[M][8];
-#pragma unroll
-            for (int m2 = 0; m2 < M; m2++) {
-                const uint64_t off = (uint64_t)un[m2] * kUnitBytes + part * 32;
-                if (pend[m2] && off < leaf_bytes) {
-                    load_unit32(leaves + off, u[m2], pol_leaf);
+            const uint32_t ua = min(ra / (uint32_t)KPU, U - 1);
+            const uint32_t ub = max(ua, min(rb / (uint32_t)KPU, U - 1));
+            // ---- 3. thresholds of the window at or below the key, counted on
+            // the code line of the predicted unit first
+            const bool has = live && ub > ua;
+            const uint32_t pu = min(max(lo_r / (uint32_t)KPU, ua), ub > ua ? ub - 1 : ua);
+            const uint32_t line = pu / kCodesPerLine, j0 = line * kCodesPerLine;
+            const uint32_t la = ua / kCodesPerLine, lb = has ? (ub - 1) / kCodesPerLine : la;
+            const uint32_t cl = code_count(m.codes, line, has, key, hl, p0, pol_idx);
+            uint32_t skip = window_part(ua, ub, j0, cl);
+            // The window's lines beside this one matter only where the count
+            // may continue into them: left if none of this line's thresholds
+            // is at or below the key (else every threshold left of it is),
+            // right if all of them are.
+            bool need = false, right = false;
+            if (has) {
+                if (cl == 0 && la < line) {
+                    need = true;
                 } else {
-#pragma unroll
-                    for (int k = 0; k < 8; k++) u[m2][k] = 0xFFFFFFFFu;  // padding keys
+                    if (la < line) skip += j0 - ua;
+                    if (lb > line && cl >= kCodesPerLine) need = right = true;
                 }
             }
-            bool any = false;
-#pragma unroll
-            for (int m2 = 0; m2 < M; m2++) {
-                const uint64_t r0 = (uint64_t)un[m2] * KPU + (uint64_t)blk * LG::S;
-                const bool last_unit = un[m2] + 1 >= U;
-                int pos = -1;
-                K lastk = 0;
-                if (key_part) {
-#pragma unroll
-                    for (int i = LG::S - 1; i >= 0; i--)
-                        if (key_at<K>(u[m2], i) == qq[m2]) pos = i;
-                    // the last unit's padding slots hold all-ones keys, which a
-                    // query may equal: a match there is no key
-                    if (last_unit && pos >= 0 && r0 + (uint64_t)pos >= n) pos = -1;
-                    lastk = key_at<K>(u[m2], LG::S - 1);
-                }
-                // matches of the quad: the first key part with one answers
-                // (block 0 before block 1: the first of equal keys)
-                const unsigned mb = (__ballot_sync(0xffffffffu, pend[m2] && pos >= 0) >> (4 * g)) & 0xFu;
-                const bool found = mb != 0;
-                const int kl = found ? __ffs(mb) - 1 : 0;
-                const int mpos = __shfl_sync(0xffffffffu, pos, 4 * g + kl);
-                // the unit's largest key (read only for units before the last,
-                // whose blocks are full): the last key of its last block
-                const int ll = 4 * g + (BPU == 2 ? 2 : 0);
-                K ulast = (K)__shfl_sync(0xffffffffu, (uint32_t)lastk, ll);
-                if constexpr (sizeof(K) == 8)
-                    ulast |= (K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)lastk >> 32), ll) << 32;
-                const bool beyond = pend[m2] && !found && qq[m2] > ulast && !last_unit;
-                const bool walk = beyond && un[m2] + 1 <= ubq[m2];
-                const bool lost = beyond && un[m2] + 1 > ubq[m2];
-                const uint64_t qi = base + (hf * NQ + m2 / 2) * 16 + 8 * (m2 & 1) + g;
-                if (pend[m2] && !walk && !lost) {
-                    if (!found) {
-                        if (part == 0) out[qi] = key_max<V>();
-                    } else {
-                        // byte of the value within the unit: block kl / 2 (two
-                        // blocks) or 0, after its key sector
-                        const int byte = (kl * 32 / LG::BS) * LG::BS + kSectorBytes + mpos * (int)sizeof(V);
-                        if (byte / 32 == part) {
-                            const int wi = (byte % 32) / 4;
-                            V val;
-                            if constexpr (sizeof(V) == 4) {
-                                val = (wi & 4) ? pick4<4>(u[m2], wi & 3) : pick4<0>(u[m2], wi & 3);
-                            } else {
-                                const int i = wi >> 1;
-                                val = ((uint64_t)pick4s2<1>(u[m2], i) << 32) | pick4s2<0>(u[m2], i);
-                            }
-                            out[qi] = val;
-                        }
-                    }
-                    pend[m2] = false;
-                } else if (walk) {
-                    un[m2]++;
-                    if (part == 0 && it < kMaxWalk) n_extra++;
-                }
-                if (lost || (walk && it == kMaxWalk)) {
-                    lost_q[m2] = true;  // outside the window: answered below
-                    pend[m2] = false;
-                }
-                any |= pend[m2];
-            }
-            if (!__any_sync(0xffffffffu, any)) break;
+            // queue the queries that need the next line
+            __syncwarp();
+            enqueue(need, key, qi, ua, ub, right ? ((line + 1) | 0x80000000u) : line - 1, skip);
+            // ---- 4. the leaf unit of the others
+            leaf_quads<K, V>(t, U, pol_leaf, live && !need, ua + skip, ub, qv, qi, out, n_extra,
+                             n_fallback);
+            while (qn >= 16) retry_pass(qn - 16, 16);
         }
-#pragma unroll
-        for (int m2 = 0; m2 < M; m2++) {
-            if (lost_q[m2] && part == 0) {  // the tree's full descent
-                out[base + (hf * NQ + m2 / 2) * 16 + 8 * (m2 & 1) + g] = tree_point<K, V>(t, qq[m2]);
-                n_fallback++;
-            }
-        }
-        }
-        }  // passes of the tile
+    }
+    while (qn > 0) {  // the rest of the queue
+        const uint32_t c = min(qn, 16u);
+        retry_pass(qn - c, c);
     }
     if (m.stats && (n_extra | n_fallback)) {
         atomicAdd(&m.stats[0], n_extra);
@@ -814,11 +892,11 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     }
 }
 
-template <typename K, typename V, int NQ, int T>
-bt_status learned_launch_nq(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                            cudaStream_t s) {
+template <typename K, typename V, int T>
+bt_status learned_launch_t(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
+                           cudaStream_t s) {
     const LearnedDev &m = t->learned->dev;
-    auto fn = learned_kernel<K, V, NQ, T>;
+    auto fn = learned_kernel<K, V, T>;
     const size_t smem = (size_t)m.stage_bytes;
     static int set_for[64] = {0};
     int dev = t->device;
@@ -839,10 +917,10 @@ template <typename K, typename V>
 bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
                          cudaStream_t s) {
     switch (t->learned->shape) {
-        case 1: return learned_launch_nq<K, V, 1, 1024>(t, d_q, nq, d_out, s);
-        case 3: return learned_launch_nq<K, V, 1, 640>(t, d_q, nq, d_out, s);
-        case 4: return learned_launch_nq<K, V, 2, 384>(t, d_q, nq, d_out, s);
-        default: return learned_launch_nq<K, V, 2, 512>(t, d_q, nq, d_out, s);
+        case 2: return learned_launch_t<K, V, 768>(t, d_q, nq, d_out, s);
+        case 3: return learned_launch_t<K, V, 640>(t, d_q, nq, d_out, s);
+        case 4: return learned_launch_t<K, V, 512>(t, d_q, nq, d_out, s);
+        default: return learned_launch_t<K, V, 1024>(t, d_q, nq, d_out, s);
     }
 }
 

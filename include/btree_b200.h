@@ -342,11 +342,10 @@ BT_API bt_status bt_learned_train(bt_tree *tree, const bt_learned_config *cfg, v
 BT_API bt_status bt_point_search_learned(const bt_tree *tree, const void *d_queries, uint64_t nq,
                                          void *d_out, void *stream);
 
-/* Shape of the learned search kernel (one CTA per SM): 1 = one query in
- * flight per lane pair (two lanes share a query), 1024-thread CTAs; 2 = two
- * queries, 512 threads (the default); 3 = one query, 640 threads; 4 = two
- * queries, 384 threads.  Fewer threads leave more registers to each.
- * Results do not depend on it; the autotuner picks the fastest. */
+/* Shape of the learned search kernel (one CTA per SM): 1 = 1024-thread CTAs
+ * (the default), 2 = 768, 3 = 640, 4 = 512.  Fewer threads leave more
+ * registers to each.  Results do not depend on it; the autotuner picks the
+ * fastest. */
 BT_API bt_status bt_learned_set_shape(bt_tree *tree, uint32_t shape);
 
 /* Counters of the last learned search on this tree: leaf units read beyond
