@@ -124,6 +124,7 @@ _PROTOS = {
     "bt_point_search_learned": (_I, [_P, _P, _U64, _P, _P]),
     "bt_learned_last_stats": (_I, [_P, ctypes.POINTER(_U64), ctypes.POINTER(_U64)]),
     "bt_learned_set_shape": (_I, [_P, ctypes.c_uint32]),
+    "bt_learned_last_lines": (_I, [_P, ctypes.POINTER(_U64)]),
     "bt_mlp_loss_grad": (_I, [_P, ctypes.c_uint32, _P, _P, _U64, _P, _P, _P]),
     "bt_rect_search": (_I, [_P, _P, _P, _P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64), _P]),
     "bt_rect_search_mode": (_I, [_P, _I, _P, _P, _P, _P, _U64, _P, _P, _P, _U64,
@@ -356,6 +357,12 @@ class Tree:
         _check(lib().bt_learned_last_stats(self._h, ctypes.byref(w), ctypes.byref(f)),
                "bt_learned_last_stats")
         return w.value, f.value
+
+    def learned_last_lines(self):
+        """Code lines the last learned search counted beyond each query's first."""
+        x = _U64()
+        _check(lib().bt_learned_last_lines(self._h, ctypes.byref(x)), "bt_learned_last_lines")
+        return x.value
 
     def group(self, queries, stream=None):
         """The grouping step alone: (grouped queries, caller index per slot)."""

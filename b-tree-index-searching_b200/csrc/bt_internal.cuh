@@ -71,19 +71,21 @@ constexpr int kSegPerLine = 4;      // segments per segment line
 constexpr int kCodesPerLine = 59;   // thresholds per code line
 constexpr int kUnitBytes = 128;     // a leaf unit: the 128-byte aligned piece of the leaf array
 
-// Four consecutive segments (leaf models) in one 128-byte line, fields
-// side by side: segment i covers the keys [key[i], next segment's key),
-// ranks r_lo .. r_lo + cnt - 1; rank ~ r_lo + clamp(icpt + slope * (key -
-// key[i]), 0, cnt) within eps of the truth for every key of the segment.
+// One segment (leaf model): it covers the keys [key, next segment's key),
+// ranks r_lo .. r_lo + cnt - 1; rank ~ r_lo + clamp(icpt + slope * (q -
+// key), 0, cnt) within eps of the truth for every key of the segment.
+struct SegRec {
+    uint64_t key;
+    uint32_t r_lo, cnt;
+    float slope, icpt;
+    uint32_t eps, pad;
+};
+
+// Four consecutive segments in one 128-byte line, 32 bytes each, so that
+// each lane of a pair reading a 64-byte half holds two whole segments.
 // Unused slots of the last line: key all-ones, r_lo = n, cnt = 0.
 struct SegLine {
-    uint64_t key[kSegPerLine];
-    uint32_t r_lo[kSegPerLine];
-    uint32_t cnt[kSegPerLine];
-    float slope[kSegPerLine];
-    float icpt[kSegPerLine];
-    uint32_t eps[kSegPerLine];
-    uint32_t pad[kSegPerLine];
+    SegRec s[kSegPerLine];
 };
 
 // Thresholds between consecutive leaf units, 59 per 128-byte line.

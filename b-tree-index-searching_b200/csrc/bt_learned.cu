@@ -69,6 +69,10 @@ constexpr int kMaxWalk = 8;                  // extra units read before the full
 // 1 = 1024 threads, 2 = 768, 3 = 640, 4 = 512 (fewer threads, more
 // registers per thread).
 constexpr int kLearnedShapes = 4;
+// Counters of a search (bt_learned_last_stats, bt_learned_last_lines): leaf
+// units read beyond the first, full descents, code lines counted beyond the
+// first.
+constexpr int kLearnedStats = 3;
 
 // ---------------------------------------------------------------- model ---
 
@@ -272,20 +276,20 @@ __global__ void seg_fill_kernel(const unsigned char *__restrict__ leaves, uint64
             if (g < nseg) {
                 const uint32_t a = starts[g];
                 const uint32_t b = g + 1 < nseg ? starts[g + 1] : (uint32_t)n;
-                sl.key[k] = (uint64_t)leaf_key<K, V>(leaves, a);
-                sl.r_lo[k] = a;
-                sl.cnt[k] = b - a;
-                sl.slope[k] = __double2float_rn(fmax(slopes[g], 0.0));
-                sl.icpt[k] = __double2float_rn(icpts[g]);
+                sl.s[k].key = (uint64_t)leaf_key<K, V>(leaves, a);
+                sl.s[k].r_lo = a;
+                sl.s[k].cnt = b - a;
+                sl.s[k].slope = __double2float_rn(fmax(slopes[g], 0.0));
+                sl.s[k].icpt = __double2float_rn(icpts[g]);
             } else {
-                sl.key[k] = ~0ull;
-                sl.r_lo[k] = (uint32_t)n;
-                sl.cnt[k] = 0;
-                sl.slope[k] = 0.f;
-                sl.icpt[k] = 0.f;
+                sl.s[k].key = ~0ull;
+                sl.s[k].r_lo = (uint32_t)n;
+                sl.s[k].cnt = 0;
+                sl.s[k].slope = 0.f;
+                sl.s[k].icpt = 0.f;
             }
-            sl.eps[k] = 0;
-            sl.pad[k] = 0;
+            sl.s[k].eps = 0;
+            sl.s[k].pad = 0;
         }
         seg[l] = sl;
     }
@@ -301,9 +305,9 @@ __global__ void seg_eps_kernel(const unsigned char *__restrict__ leaves, uint32_
          g += ((uint64_t)gridDim.x * blockDim.x) >> 5) {
         SegLine &sl = seg[g / kSegPerLine];
         const int k = (int)(g % kSegPerLine);
-        const uint64_t fk = sl.key[k];
-        const uint32_t a = sl.r_lo[k], cnt = sl.cnt[k];
-        const float slope = sl.slope[k], icpt = sl.icpt[k];
+        const uint64_t fk = sl.s[k].key;
+        const uint32_t a = sl.s[k].r_lo, cnt = sl.s[k].cnt;
+        const float slope = sl.s[k].slope, icpt = sl.s[k].icpt;
         float err = 0.f;
         for (uint32_t i = lane; i < cnt; i += 32) {
             const float p = seg_pred(slope, icpt, cnt, fk, (uint64_t)leaf_key<K, V>(leaves, a + i));
@@ -312,7 +316,7 @@ __global__ void seg_eps_kernel(const unsigned char *__restrict__ leaves, uint32_
         for (int o = 16; o > 0; o >>= 1) err = fmaxf(err, __shfl_xor_sync(0xffffffffu, err, o));
         if (lane == 0) {
             const float ce = ceilf(err);
-            sl.eps[k] = ce >= 4.0e9f ? 0xFFFFFFFFu : (uint32_t)ce;
+            sl.s[k].eps = ce >= 4.0e9f ? 0xFFFFFFFFu : (uint32_t)ce;
         }
     }
 }
@@ -331,7 +335,7 @@ __global__ void stage_kernel(const SegLine *__restrict__ seg, uint32_t nls, uint
             stage[swz<K>(l)] = key_max<K>();
             continue;
         }
-        const uint64_t k = seg[l].key[0];
+        const uint64_t k = seg[l].s[0].key;
         stage[swz<K>(l)] = (K)k;
         x[l] = norm_key(k, kmin, xscale);
         y[l] = (float)(((double)l + 0.5) / (double)nls);
@@ -575,7 +579,8 @@ __device__ __forceinline__ uint32_t window_part(uint32_t ua, uint32_t ub, uint32
 // in its warp's shared-memory queue until 16 of them fill a pass.
 struct Retry {
     uint64_t key;   // the query key (zero-extended)
-    uint64_t qi;    // its index in the batch
+    uint32_t qi;    // its index in the launch's batch (below 2^31)
+    uint32_t pad;
     uint32_t ua, ub;
     uint32_t line;  // the code line still to count
     uint32_t skip;  // thresholds of the window at or below the key so far
@@ -591,9 +596,9 @@ constexpr int kRetryCap = 32;  // entries per warp (at most 15 + 16 at once)
 // full descent.  Called by the whole warp.
 template <typename K, typename V>
 __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_t pol, bool live,
-                                           uint32_t unit, uint32_t ub, K key, uint64_t qi,
-                                           V *__restrict__ out, unsigned long long &n_extra,
-                                           unsigned long long &n_fallback) {
+                                           uint32_t unit, uint32_t ub, K key, uint32_t qi,
+                                           V *__restrict__ out, uint32_t &n_extra,
+                                           uint32_t &n_fallback) {
     using LG = LeafGeom<K, V>;
     constexpr int KPU = unit_keys<K, V>();
     constexpr int BPU = kUnitBytes / LG::BS;
@@ -603,9 +608,8 @@ __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_
     // a key part holds the keys of block `blk` of the unit
     const bool key_part = (part * 32) % LG::BS == 0;
     const int blk = part * 32 / LG::BS;
-    uint32_t un[2], ubq[2];
+    uint32_t un[2], ubq[2], qx[2];
     K qq[2];
-    uint64_t qx[2];
     bool pend[2], lost_q[2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
@@ -614,26 +618,26 @@ __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_
         ubq[h] = __shfl_sync(0xffffffffu, ub, src);
         pend[h] = __shfl_sync(0xffffffffu, live ? 1u : 0u, src) != 0;
         lost_q[h] = false;
-        qx[h] = ((uint64_t)__shfl_sync(0xffffffffu, (uint32_t)(qi >> 32), src) << 32) |
-                __shfl_sync(0xffffffffu, (uint32_t)qi, src);
+        qx[h] = __shfl_sync(0xffffffffu, qi, src);
         if constexpr (sizeof(K) == 8)
             qq[h] = ((K)__shfl_sync(0xffffffffu, (uint32_t)((uint64_t)key >> 32), src) << 32) |
                     __shfl_sync(0xffffffffu, (uint32_t)key, src);
         else
             qq[h] = (K)__shfl_sync(0xffffffffu, (uint32_t)key, src);
     }
+    // a sub-query that is not pending keeps the words it last read: its
+    // matches and keys are ignored below
+    uint32_t u[2][8];
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int k = 0; k < 8; k++) u[h][k] = 0xFFFFFFFFu;
 #pragma unroll 1
     for (int it = 0; it <= kMaxWalk; it++) {
-        uint32_t u[2][8];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const uint64_t off = (uint64_t)un[h] * kUnitBytes + part * 32;
-            if (pend[h] && off < leaf_bytes) {
-                load_unit32(leaves + off, u[h], pol);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 8; k++) u[h][k] = 0xFFFFFFFFu;  // padding keys
-            }
+            if (pend[h] && off < leaf_bytes) load_unit32(leaves + off, u[h], pol);
         }
         bool any = false;
 #pragma unroll
@@ -741,11 +745,11 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
     const uint64_t ntiles = (nq + 31) / 32;
     Retry *rq = s_retry[threadIdx.x >> 5];
     uint32_t qn = 0;  // entries in this warp's queue (the same in every lane)
-    unsigned long long n_extra = 0, n_fallback = 0;
+    uint32_t n_extra = 0, n_fallback = 0, n_lines = 0;
 
     // Appends the queries of the pairs with `need` to the warp's queue (the
     // line word carries the direction of the walk in its top bit).
-    auto enqueue = [&](bool need, uint64_t key, uint64_t qi, uint32_t ua, uint32_t ub,
+    auto enqueue = [&](bool need, uint64_t key, uint32_t qi, uint32_t ua, uint32_t ub,
                        uint32_t line_dir, uint32_t skip) {
         const unsigned qmask = __ballot_sync(0xffffffffu, hl == 0 && need);
         if (hl == 0 && need) {
@@ -775,6 +779,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         const bool right = (e.line >> 31) != 0;
         const uint32_t j0 = line * kCodesPerLine;
         const uint32_t c = code_count(m.codes, line, live, e.key, hl, p0, pol_idx);
+        if (live && hl == 0) n_lines++;
         uint32_t skip = e.skip + window_part(e.ua, e.ub, j0, c);
         const uint32_t la = e.ua / kCodesPerLine, lb = (e.ub - 1) / kCodesPerLine;
         bool more;
@@ -814,8 +819,8 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         for (int hf = 0; hf < 2; hf++) {
             const int k = hf * 16 + pr;
             const K qv = __shfl_sync(0xffffffffu, myq, k);
-            const uint64_t qi = base + k;
-            const bool live = qi < nq;
+            const uint32_t qi = (uint32_t)(base + k);
+            const bool live = base + k < nq;
             const uint32_t sl = __shfl_sync(0xffffffffu, my_sl, k);
             uint32_t w[16];
             if (live) {
@@ -825,37 +830,35 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
                 for (int i = 0; i < 16; i++) w[i] = 0;
             }
             // ---- 2. segment -> rank window -> unit window [ua, ub]
-            // lane 0 of a pair: key[0..3] (words 0-7), r_lo[4] (8-11), cnt[4] (12-15);
-            // lane 1: slope[4] (0-3), icpt[4] (4-7), eps[4] (8-11)
+            // lane hl of the pair holds segments 2 hl (words 0-7) and 2 hl + 1
+            // (words 8-15): key lo, key hi, r_lo, cnt, slope, icpt, eps, pad
             const uint64_t key = (uint64_t)qv;
-            int c = 0;
-#pragma unroll
-            for (int i = 1; i < kSegPerLine; i++) c += (((uint64_t)w[2 * i + 1] << 32) | w[2 * i]) < key ? 1 : 0;
-            c = __shfl_sync(0xffffffffu, c, p0);
-            // this lane's fields of segment c, then the partner's
-            const uint32_t f0 = hl ? pick4<0>(w, c) : pick4s2<0>(w, c);  // slope | key lo
-            const uint32_t f1 = hl ? pick4<4>(w, c) : pick4s2<1>(w, c);  // icpt | key hi
-            const uint32_t f2 = pick4<8>(w, c);                          // eps | r_lo
-            const uint32_t f3 = pick4<12>(w, c);                         // pad | cnt
-            const uint32_t g0 = __shfl_xor_sync(0xffffffffu, f0, 1);
-            const uint32_t g1 = __shfl_xor_sync(0xffffffffu, f1, 1);
-            const uint32_t g2 = __shfl_xor_sync(0xffffffffu, f2, 1);
-            const uint32_t g3 = __shfl_xor_sync(0xffffffffu, f3, 1);
-            const uint64_t fk = hl ? (((uint64_t)g1 << 32) | g0) : (((uint64_t)f1 << 32) | f0);
-            const uint32_t r_lo = hl ? g2 : f2, cnt = hl ? g3 : f3;
-            const float slope = __uint_as_float(hl ? f0 : g0), icpt = __uint_as_float(hl ? f1 : g1);
-            const uint32_t eps = hl ? f2 : g2;
+            const bool b_lt = (((uint64_t)w[9] << 32) | w[8]) < key;
+            const bool a_lt = (((uint64_t)w[1] << 32) | w[0]) < key;
+            // segment c = how many of the line's keys 1..3 are below the key
+            const uint32_t part = hl ? (a_lt ? 1u : 0u) + (b_lt ? 1u : 0u) : (b_lt ? 1u : 0u);
+            const uint32_t c = part + __shfl_xor_sync(0xffffffffu, part, 1);
+            // the lane holding segment c computes the window; the pair takes
+            // its result
+            const bool sb = (c & 1) != 0;
+            const uint64_t fk = sb ? (((uint64_t)w[9] << 32) | w[8]) : (((uint64_t)w[1] << 32) | w[0]);
+            const uint32_t r_lo = sb ? w[10] : w[2], cnt = sb ? w[11] : w[3];
+            const float slope = __uint_as_float(sb ? w[12] : w[4]);
+            const float icpt = __uint_as_float(sb ? w[13] : w[5]);
+            const uint32_t eps = sb ? w[14] : w[6];
             const float p = seg_pred(slope, icpt, cnt, fk, key);  // in [0, cnt]
             // ranks [r_lo + floor(p) - eps - 1, r_lo + ceil(p) + eps + 1], clamped
             const uint32_t lo_r = r_lo + (uint32_t)floorf(p), hi_r = r_lo + (uint32_t)ceilf(p);
             const uint32_t ra = eps >= lo_r ? 0u : lo_r - eps - 1u;
             const uint32_t rb = hi_r + eps + 1u < hi_r ? 0xFFFFFFFFu : hi_r + eps + 1u;
-            const uint32_t ua = min(ra / (uint32_t)KPU, U - 1);
-            const uint32_t ub = max(ua, min(rb / (uint32_t)KPU, U - 1));
+            const int owner = p0 + (int)(c >> 1);
+            const uint32_t ua = __shfl_sync(0xffffffffu, min(ra / (uint32_t)KPU, U - 1), owner);
+            const uint32_t ub = max(ua, __shfl_sync(0xffffffffu, min(rb / (uint32_t)KPU, U - 1), owner));
+            const uint32_t pu_raw = __shfl_sync(0xffffffffu, lo_r / (uint32_t)KPU, owner);
             // ---- 3. thresholds of the window at or below the key, counted on
             // the code line of the predicted unit first
             const bool has = live && ub > ua;
-            const uint32_t pu = min(max(lo_r / (uint32_t)KPU, ua), ub > ua ? ub - 1 : ua);
+            const uint32_t pu = min(max(pu_raw, ua), ub > ua ? ub - 1 : ua);
             const uint32_t line = pu / kCodesPerLine, j0 = line * kCodesPerLine;
             const uint32_t la = ua / kCodesPerLine, lb = has ? (ub - 1) / kCodesPerLine : la;
             const uint32_t cl = code_count(m.codes, line, has, key, hl, p0, pol_idx);
@@ -886,9 +889,10 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         const uint32_t c = min(qn, 16u);
         retry_pass(qn - c, c);
     }
-    if (m.stats && (n_extra | n_fallback)) {
-        atomicAdd(&m.stats[0], n_extra);
-        atomicAdd(&m.stats[1], n_fallback);
+    if (m.stats && (n_extra | n_fallback | n_lines)) {
+        atomicAdd(&m.stats[0], (unsigned long long)n_extra);
+        atomicAdd(&m.stats[1], (unsigned long long)n_fallback);
+        atomicAdd(&m.stats[2], (unsigned long long)n_lines);
     }
 }
 
@@ -904,12 +908,18 @@ bt_status learned_launch_t(const bt_tree *t, const void *d_q, uint64_t nq, void 
         BT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         set_for[dev] = (int)smem;
     }
-    const uint64_t ntiles = (nq + 31) / 32;
-    const uint64_t want = (ntiles + T / 32 - 1) / (T / 32);
-    const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, sm_count()));
-    count_launch();
-    fn<<<grid, T, smem, s>>>(t->dev, m, (const K *)d_q, nq, (V *)d_out);
-    BT_CUDA(cudaGetLastError());
+    // the kernel indexes its batch with 32-bit offsets: batches of 2^31
+    // queries and more go as several launches
+    constexpr uint64_t kChunk = 1ull << 31;
+    for (uint64_t off = 0; off < nq; off += kChunk) {
+        const uint64_t n = std::min(kChunk, nq - off);
+        const uint64_t ntiles = (n + 31) / 32;
+        const uint64_t want = (ntiles + T / 32 - 1) / (T / 32);
+        const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, sm_count()));
+        count_launch();
+        fn<<<grid, T, smem, s>>>(t->dev, m, (const K *)d_q + off, n, (V *)d_out + off);
+        BT_CUDA(cudaGetLastError());
+    }
     return BT_OK;
 }
 
@@ -1111,8 +1121,8 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     BT_CUDA(cudaMalloc(&bv.p, np * sizeof(float)));
     BT_CUDA(cudaMalloc(&berr.p, 2 * sizeof(unsigned int)));
     BT_CUDA(cudaMalloc((void **)&st->d_mlp, np * sizeof(float)));
-    BT_CUDA(cudaMalloc((void **)&st->d_stats, 2 * sizeof(unsigned long long)));
-    BT_CUDA(cudaMemsetAsync(st->d_stats, 0, 2 * sizeof(unsigned long long), s));
+    BT_CUDA(cudaMalloc((void **)&st->d_stats, kLearnedStats * sizeof(unsigned long long)));
+    BT_CUDA(cudaMemsetAsync(st->d_stats, 0, kLearnedStats * sizeof(unsigned long long), s));
     BT_CUDA(cudaMemsetAsync(berr.p, 0, 2 * sizeof(unsigned int), s));
     float *x = (float *)bx.p, *y = (float *)by.p, *grad = (float *)bg.p, *loss = grad + np;
     unsigned int *err = (unsigned int *)berr.p;
@@ -1201,11 +1211,11 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
         for (uint64_t g = 0; g < nseg; g++) {
             const SegLine &sl = segs[g / kSegPerLine];
             const int k = (int)(g % kSegPerLine);
-            esum += sl.eps[k];
-            emax = std::max<uint64_t>(emax, sl.eps[k]);
+            esum += sl.s[k].eps;
+            emax = std::max<uint64_t>(emax, sl.s[k].eps);
             // window of 2 eps + 3 ranks: units it spans, then code lines
-            const double win_units = (2.0 * sl.eps[k] + 3.0) / kpu + 1.0;
-            lsum += (double)sl.cnt[k] * (1.0 + (win_units - 1.0) / kCodesPerLine);
+            const double win_units = (2.0 * sl.s[k].eps + 3.0) / kpu + 1.0;
+            lsum += (double)sl.s[k].cnt * (1.0 + (win_units - 1.0) / kCodesPerLine);
         }
         rep->eps_mean = nseg ? esum / (double)nseg : 0;
         rep->eps_max = emax;
@@ -1233,7 +1243,7 @@ bt_status launch_learned_search(const bt_tree *t, const void *d_q, uint64_t nq, 
 }
 
 bt_status reset_learned_stats(const bt_tree *t, cudaStream_t s) {
-    BT_CUDA(cudaMemsetAsync(t->learned->d_stats, 0, 2 * sizeof(unsigned long long), s));
+    BT_CUDA(cudaMemsetAsync(t->learned->d_stats, 0, kLearnedStats * sizeof(unsigned long long), s));
     return BT_OK;
 }
 
@@ -1293,6 +1303,16 @@ bt_status bt_learned_last_stats(const bt_tree *t, uint64_t *extra, uint64_t *fal
     BT_CUDA(cudaMemcpy(h, t->learned->d_stats, sizeof(h), cudaMemcpyDeviceToHost));
     if (extra) *extra = h[0];
     if (fallback) *fallback = h[1];
+    return BT_OK;
+}
+
+bt_status bt_learned_last_lines(const bt_tree *t, uint64_t *extra_lines) {
+    using namespace bt;
+    if (!t || !t->learned) return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
+    if (!extra_lines) return fail(BT_ERR_INVALID_ARGUMENT, "extra_lines is NULL");
+    unsigned long long h[kLearnedStats] = {};
+    BT_CUDA(cudaMemcpy(h, t->learned->d_stats, sizeof(h), cudaMemcpyDeviceToHost));
+    *extra_lines = h[2];
     return BT_OK;
 }
 

@@ -834,6 +834,7 @@ def run_ours(args):
     ms = max_over_ranks(statistics.mean(step_ms), dist, device)
     value = world * nq / (ms / 1000.0)
     extra, fallback = tree.learned_last_stats()
+    extra_lines = tree.learned_last_lines()
 
     # ---- the plain tree search of the same batch ----------------------------
     for _ in range(2):
@@ -945,7 +946,8 @@ def run_ours(args):
                                                   "root_loss_initial", "root_loss_final",
                                                   "code_lines_mean", "index_bytes",
                                                   "keys_per_unit", "train_ms")},
-            "learned_stats": {"extra_unit_reads": extra, "full_descents": fallback},
+            "learned_stats": {"extra_unit_reads": extra, "full_descents": fallback,
+                              "extra_code_lines": extra_lines},
             "learned_shape": {"shape": l_shape, "autotune_ms": l_tune_ms},
             "cpu_baseline": cpu,
             "cpu_sample_matches_gpu": checked,

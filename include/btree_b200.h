@@ -354,6 +354,11 @@ BT_API bt_status bt_learned_set_shape(bt_tree *tree, uint32_t shape);
 BT_API bt_status bt_learned_last_stats(const bt_tree *tree, uint64_t *extra_unit_reads,
                                        uint64_t *fallback);
 
+/* Code lines the last learned search on this tree counted beyond each
+ * query's first (queries whose rank window continues into a neighbouring
+ * line and whose count had to go on there). */
+BT_API bt_status bt_learned_last_lines(const bt_tree *tree, uint64_t *extra_code_lines);
+
 /*
  * The root model's training kernels, exposed so their gradients can be
  * checked: for params p (3*hidden+1 floats: w1[hidden], b1[hidden],

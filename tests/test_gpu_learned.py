@@ -88,6 +88,7 @@ def test_learned_search_is_exact(bt, orc, cuda, kind, n, kt, vt, target):
             got = t.point_search_learned(dev(q, cuda)).cpu().numpy()
             assert np.array_equal(got, exp), shape
             extra, fallback = t.learned_last_stats()
+            assert 0 <= t.learned_last_lines() <= 4 * len(q)
             assert fallback == 0  # the measured bounds always hold
             assert extra <= len(q) // 20
         for bad in (0, 5):
