@@ -67,7 +67,8 @@ def parse_args(argv=None):
     p.add_argument("--no-rect", action="store_true", help="skip the rectangle-search section")
     p.add_argument("--rect-boxes-log2", type=int, default=20, help="boxes in the rectangle section")
     p.add_argument("--forest-trees", type=int, default=4096, help="trees in the forest section")
-    p.add_argument("--only", choices=["learned", "grouped", "ranges", "forest", "rect", "small"],
+    p.add_argument("--only", choices=["learned", "learned_kernel", "grouped", "ranges", "forest",
+                                      "rect", "small"],
                    help="run one extension section alone on cuda:0 and print its JSON object "
                         "(for profiling; not the bench line)")
     return p.parse_args(argv)
@@ -962,6 +963,42 @@ def run_ours(args):
     return 0
 
 
+def learned_kernel_section(args, device, bt, flush, stream):
+    """The learned search kernel alone, for profiling: build and train on the
+    learned-index workload, then `steps` learned searches (each after an L2
+    flush), timed with CUDA events and checked against the plain search."""
+    import torch
+    L = bt.lib()
+    P = ctypes.c_void_p
+    keys, vals, q = lognormal_workload(args.keys_log2, args.queries_log2, 0)
+    tree = bt.Tree.build(torch.from_numpy(keys).to(device), torch.from_numpy(vals).to(device))
+    try:
+        rep = tree.learned_train(num_segments=1 << args.segments_log2)
+        dq = torch.from_numpy(q).to(device)
+        out = torch.empty(len(q), dtype=torch.uint64, device=device)
+        ref = torch.empty_like(out)
+        sp = P(stream.cuda_stream)
+        bt._check(L.bt_point_search(tree.handle, 0, P(dq.data_ptr()), len(q), P(ref.data_ptr()), sp),
+                  "plain")
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            bt._check(L.bt_point_search(tree.handle, 2, P(dq.data_ptr()), len(q), P(out.data_ptr()),
+                                        sp), "learned")
+            e1.record(stream)
+            torch.cuda.synchronize(device)
+            ms.append(e0.elapsed_time(e1))
+        extra, fallback = tree.learned_last_stats()
+        return {"keys": len(keys), "queries": len(q), "segments": rep["num_segments"],
+                "eps_max": rep["eps_max"], "ms": ms, "equals_plain": bool(torch.equal(out, ref)),
+                "extra_unit_reads": extra, "full_descents": fallback,
+                "extra_code_lines": tree.learned_last_lines()}
+    finally:
+        tree.close()
+
+
 def run_only(args):
     import torch
     bt = importlib.import_module(PKG)
@@ -973,7 +1010,9 @@ def run_only(args):
         return run_ours(argparse.Namespace(**{**vars(args), "no_serving": True, "no_grouped": True,
                                               "no_forest": True, "no_rect": True,
                                               "no_reference_gpu": True, "no_cpu_baseline": True}))
-    if args.only in ("grouped", "ranges"):
+    if args.only == "learned_kernel":
+        sec = learned_kernel_section(args, device, bt, flush, stream)
+    elif args.only in ("grouped", "ranges"):
         sec, gtree, gkeys = grouped_section(args, device, bt, flush, stream)
         if args.only == "ranges":
             sec = range_section(args, device, bt, flush, gtree, gkeys)
