@@ -675,7 +675,8 @@ def grouped_section(args, device, bt, flush, stream, rank=0):
                      "achieved": alg / (search_ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": alg / (search_ms / 1e3) / 1e9 / peak,
                      "traffic": None if tq is None else tq * nq,
-                     "traffic_source": "ncu dram bytes per query of the grouped search kernel "
+                     "traffic_source": "not measured in this run: ncu DRAM bytes per query of "
+                                       "the grouped search kernel from a 2^22-query capture "
                                        "(profiles/search_kernels_zipf_k26_q22.md) x queries",
                      "random_gather_ceiling": {"reads_per_s": gather_rps, "block_bytes": 64,
                                                "frac": nq / (search_ms / 1e3) / gather_rps}},
@@ -931,8 +932,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": None if tq is None else tq * nq,
-                         "traffic_source": "ncu dram bytes per query of learned_kernel "
-                                           "(profiles/learned_kernel_lognormal_2e28.md) x queries",
+                         "traffic_source": "not measured in this run: ncu DRAM bytes per query "
+                                           "of learned_kernel from a 2^24-key capture "
+                                           "(profiles/traffic.json, command there) x queries",
                          "kernel": "learned_kernel",
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "kernel_ms": statistics.mean(step_ms),
