@@ -104,6 +104,7 @@ _PROTOS = {
     "bt_get_info": (_I, [_P, ctypes.POINTER(bt_info)]),
     "bt_point_search": (_I, [_P, _I, _P, _U64, _P, _P]),
     "bt_point_search_host": (_I, [_P, _I, _P, _U64, _P, _P]),
+    "bt_point_search_found": (_I, [_P, _I, _P, _U64, _P, _P, _P]),
     "bt_group_queries": (_I, [_P, _P, _U64, _P, _P, _P]),
     "bt_range_count": (_I, [_P, _I, _P, _P, _U64, _P, _P]),
     "bt_range_search": (_I, [_P, _I, _P, _P, _U64, _P, _P, _P, _U64, ctypes.POINTER(_U64), _P]),
@@ -297,6 +298,25 @@ class Tree:
     SEARCH_CONFIGS = ((8, 1), (8, 2), (4, 1), (4, 2), (2, 1))
 
     # -- point search ---------------------------------------------------
+    def point_search_found(self, queries, mode="basic", stream=None):
+        """(values, found): the values of the queried keys (all-ones on a
+        miss) and a uint8 flag per query, 1 when the key is in the tree
+        (bt_point_search_found).  CUDA tensors in and out, asynchronous on
+        `stream`."""
+        import torch
+        if not _is_cuda(queries):
+            raise ValueError("point_search_found takes a CUDA tensor")
+        if queries.element_size() != self.key_bytes:
+            raise ValueError("query width differs from the tree's key width")
+        queries = queries.contiguous()
+        n = len(queries)
+        out = torch.empty(n, dtype=_torch_dtype(self.value_bytes), device=queries.device)
+        found = torch.empty(n, dtype=torch.uint8, device=queries.device)
+        _check(lib().bt_point_search_found(self._h, POINT_MODES[mode], _P(queries.data_ptr()), n,
+                                           _P(out.data_ptr()), _P(found.data_ptr()),
+                                           _stream_ptr(stream)), "bt_point_search_found")
+        return out, found
+
     def point_search(self, queries, mode="basic", out=None, stream=None):
         """Values of the queried keys (all-ones on a miss), in query order.
         CUDA tensor in -> CUDA tensor out (asynchronous on `stream`);

@@ -54,15 +54,16 @@ bt_status pipe_streams(int dev, cudaStream_t (&out)[kPipeSlots]) {
 }
 
 bt_status point_device(const bt_tree *t, int mode, const void *d_q, uint64_t nq, void *d_out,
-                       cudaStream_t s) {
-    if (mode == BT_POINT_BASIC || t->n == 0) return launch_point_search(t, d_q, nullptr, nq, d_out, s);
-    if (mode == BT_POINT_LEARNED) return launch_learned_search(t, d_q, nq, d_out, s);
+                       cudaStream_t s, uint8_t *d_found = nullptr) {
+    if (mode == BT_POINT_BASIC || t->n == 0)
+        return launch_point_search(t, d_q, nullptr, nq, d_out, s, d_found);
+    if (mode == BT_POINT_LEARNED) return launch_learned_search(t, d_q, nq, d_out, d_found, s);
     void *gq = nullptr;
     uint32_t *perm = nullptr;
     bt_status st = ws_alloc(&gq, nq * t->key_bytes, s);
     if (st == BT_OK) st = ws_alloc((void **)&perm, nq * sizeof(uint32_t), s);
     if (st == BT_OK) st = launch_partition(t, kPartPoint, d_q, nullptr, nq, gq, nullptr, perm, s);
-    if (st == BT_OK) st = launch_point_search(t, gq, perm, nq, d_out, s);
+    if (st == BT_OK) st = launch_point_search(t, gq, perm, nq, d_out, s, d_found);
     ws_free(gq, s);
     ws_free(perm, s);
     return st;
@@ -175,6 +176,26 @@ bt_status bt_point_search(const bt_tree *t, int mode, const void *d_queries, uin
         if (st != BT_OK) return st;
     }
     return point_device(t, mode, d_queries, nq, d_out, (cudaStream_t)stream);
+}
+
+bt_status bt_point_search_found(const bt_tree *t, int mode, const void *d_queries, uint64_t nq,
+                                void *d_out, uint8_t *d_found, void *stream) {
+    using namespace bt;
+    bt_status st = check_tree(t);
+    if (st != BT_OK) return st;
+    if (!valid_point_mode(mode)) return fail(BT_ERR_INVALID_ARGUMENT, "unknown point mode");
+    if (mode == BT_POINT_LEARNED && !t->learned)
+        return fail(BT_ERR_INVALID_ARGUMENT, "the tree has no trained learned index");
+    if (nq == 0) return BT_OK;
+    if (!d_queries || !d_out || !d_found)
+        return fail(BT_ERR_INVALID_ARGUMENT, "queries, out or found is NULL");
+    if (nq >= (1ull << 32)) return fail(BT_ERR_INVALID_ARGUMENT, "nq must be below 2^32");
+    DeviceGuard g(t->device);
+    if (mode == BT_POINT_LEARNED) {
+        st = reset_learned_stats(t, (cudaStream_t)stream);
+        if (st != BT_OK) return st;
+    }
+    return point_device(t, mode, d_queries, nq, d_out, (cudaStream_t)stream, d_found);
 }
 
 bt_status bt_point_search_host(const bt_tree *t, int mode, const void *h_queries, uint64_t nq,

@@ -202,7 +202,8 @@ inline int bitlen64(uint64_t v) {
 
 // Host launchers implemented in the .cu files.
 bt_status launch_point_search(const bt_tree *t, const void *d_q, const uint32_t *d_perm,
-                              uint64_t nq, void *d_out, cudaStream_t s);
+                              uint64_t nq, void *d_out, cudaStream_t s,
+                              uint8_t *d_found = nullptr);
 bt_status launch_bounds(const bt_tree *t, const void *d_lo, const void *d_hi,
                         const uint32_t *d_perm, uint64_t nq, uint64_t *d_counts,
                         uint64_t *d_lb, cudaStream_t s);
@@ -244,7 +245,7 @@ void free_learned(bt::LearnedState *s);
 // Learned point search of d_q into d_out on s (the tree has a learned index;
 // the counters of bt_learned_last_stats accumulate).
 bt_status launch_learned_search(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                                cudaStream_t s);
+                                uint8_t *d_found, cudaStream_t s);
 // Zeroes those counters (stream-ordered).
 bt_status reset_learned_stats(const bt_tree *t, cudaStream_t s);
 

@@ -437,19 +437,27 @@ __device__ __forceinline__ uint32_t stage_search(const K *__restrict__ s, uint32
     return base;
 }
 
-// Scalar full descent of the tree for one query (the fallback).
+// Scalar full descent of the tree for one query (the fallback): writes its
+// value, or all-ones on a miss, to *dst and, when hit is not null, 1 or 0 to
+// *hit.
 template <typename K, typename V>
-__device__ __noinline__ V tree_point(const DevTree &t, K q) {
+__device__ __noinline__ void tree_point(const DevTree &t, K q, V *dst, uint8_t *hit) {
     using LG = LeafGeom<K, V>;
     const K tmax = (K)t.max_key;
-    if (q > tmax) return key_max<V>();
-    const uint32_t blk = block_lower_bound<K>(t, q);
-    const unsigned char *b = static_cast<const unsigned char *>(t.leaves) + (size_t)blk * LG::BS;
-    const K *kb = reinterpret_cast<const K *>(b);
-    for (int i = 0; i < LG::S; i++)
-        if (kb[i] == q && (uint64_t)blk * LG::S + i < t.n)
-            return reinterpret_cast<const V *>(b + kSectorBytes)[i];
-    return key_max<V>();
+    V v = key_max<V>();
+    bool f = false;
+    if (q <= tmax) {
+        const uint32_t blk = block_lower_bound<K>(t, q);
+        const unsigned char *b = static_cast<const unsigned char *>(t.leaves) + (size_t)blk * LG::BS;
+        const K *kb = reinterpret_cast<const K *>(b);
+        for (int i = 0; i < LG::S && !f; i++)
+            if (kb[i] == q && (uint64_t)blk * LG::S + i < t.n) {
+                v = reinterpret_cast<const V *>(b + kSectorBytes)[i];
+                f = true;
+            }
+    }
+    *dst = v;
+    if (hit) *hit = f ? 1 : 0;
 }
 
 // 64-byte half of an index line: two 32-byte loads, evict-last in L2.
@@ -597,8 +605,8 @@ constexpr int kRetryCap = 32;  // entries per warp (at most 15 + 16 at once)
 template <typename K, typename V>
 __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_t pol, bool live,
                                            uint32_t unit, uint32_t ub, K key, uint32_t qi,
-                                           V *__restrict__ out, uint32_t &n_extra,
-                                           uint32_t &n_fallback) {
+                                           V *__restrict__ out, uint8_t *__restrict__ fnd,
+                                           uint32_t &n_extra, uint32_t &n_fallback) {
     using LG = LeafGeom<K, V>;
     constexpr int KPU = unit_keys<K, V>();
     constexpr int BPU = kUnitBytes / LG::BS;
@@ -671,6 +679,7 @@ __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_
             const bool walk = beyond && un[h] + 1 <= ubq[h];
             const bool lost = beyond && un[h] + 1 > ubq[h];
             if (pend[h] && !walk && !lost) {
+                if (part == 0 && fnd) fnd[qx[h]] = found ? 1 : 0;
                 if (!found) {
                     if (part == 0) out[qx[h]] = key_max<V>();
                 } else {
@@ -705,7 +714,7 @@ __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_
 #pragma unroll
     for (int h = 0; h < 2; h++) {
         if (lost_q[h] && part == 0) {  // the tree's full descent
-            out[qx[h]] = tree_point<K, V>(t, qq[h]);
+            tree_point<K, V>(t, qq[h], out + qx[h], fnd ? fnd + qx[h] : nullptr);
             n_fallback++;
         }
     }
@@ -722,7 +731,8 @@ __device__ __forceinline__ void leaf_quads(const DevTree &t, uint32_t U, uint64_
 template <typename K, typename V, int T>
 __global__ void __launch_bounds__(T, 1)
 learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ LearnedDev m,
-               const K *__restrict__ q, uint64_t nq, V *__restrict__ out) {
+               const K *__restrict__ q, uint64_t nq, V *__restrict__ out,
+               uint8_t *__restrict__ found) {
     constexpr int KPU = unit_keys<K, V>();  // keys per unit
     extern __shared__ uint4 smem_l[];
     __shared__ __align__(8) unsigned long long s_bar;
@@ -791,7 +801,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         }
         enqueue(more, e.key, e.qi, e.ua, e.ub, right ? ((line + 1) | 0x80000000u) : line - 1, skip);
         leaf_quads<K, V>(t, U, pol_leaf, live && !more, e.ua + skip, e.ub, (K)e.key, e.qi, out,
-                         n_extra, n_fallback);
+                         found, n_extra, n_fallback);
     };
 
     for (uint64_t tile = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; tile < ntiles;
@@ -802,7 +812,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
         const K myq = my < nq ? q[my] : (K)0;
         if (!staged) {  // the staged keys never arrived: the tree's full descent
             if (my < nq) {
-                out[my] = tree_point<K, V>(t, myq);
+                tree_point<K, V>(t, myq, out + my, found ? found + my : nullptr);
                 n_fallback++;
             }
             continue;
@@ -880,8 +890,8 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
             __syncwarp();
             enqueue(need, key, qi, ua, ub, right ? ((line + 1) | 0x80000000u) : line - 1, skip);
             // ---- 4. the leaf unit of the others
-            leaf_quads<K, V>(t, U, pol_leaf, live && !need, ua + skip, ub, qv, qi, out, n_extra,
-                             n_fallback);
+            leaf_quads<K, V>(t, U, pol_leaf, live && !need, ua + skip, ub, qv, qi, out, found,
+                             n_extra, n_fallback);
             while (qn >= 16) retry_pass(qn - 16, 16);
         }
     }
@@ -898,7 +908,7 @@ learned_kernel(const __grid_constant__ DevTree t, const __grid_constant__ Learne
 
 template <typename K, typename V, int T>
 bt_status learned_launch_t(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                           cudaStream_t s) {
+                           uint8_t *d_found, cudaStream_t s) {
     const LearnedDev &m = t->learned->dev;
     auto fn = learned_kernel<K, V, T>;
     const size_t smem = (size_t)m.stage_bytes;
@@ -917,7 +927,8 @@ bt_status learned_launch_t(const bt_tree *t, const void *d_q, uint64_t nq, void 
         const uint64_t want = (ntiles + T / 32 - 1) / (T / 32);
         const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(want, sm_count()));
         count_launch();
-        fn<<<grid, T, smem, s>>>(t->dev, m, (const K *)d_q + off, n, (V *)d_out + off);
+        fn<<<grid, T, smem, s>>>(t->dev, m, (const K *)d_q + off, n, (V *)d_out + off,
+                                 d_found ? d_found + off : nullptr);
         BT_CUDA(cudaGetLastError());
     }
     return BT_OK;
@@ -925,12 +936,12 @@ bt_status learned_launch_t(const bt_tree *t, const void *d_q, uint64_t nq, void 
 
 template <typename K, typename V>
 bt_status learned_launch(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                         cudaStream_t s) {
+                         uint8_t *d_found, cudaStream_t s) {
     switch (t->learned->shape) {
-        case 2: return learned_launch_t<K, V, 768>(t, d_q, nq, d_out, s);
-        case 3: return learned_launch_t<K, V, 640>(t, d_q, nq, d_out, s);
-        case 4: return learned_launch_t<K, V, 512>(t, d_q, nq, d_out, s);
-        default: return learned_launch_t<K, V, 1024>(t, d_q, nq, d_out, s);
+        case 2: return learned_launch_t<K, V, 768>(t, d_q, nq, d_out, d_found, s);
+        case 3: return learned_launch_t<K, V, 640>(t, d_q, nq, d_out, d_found, s);
+        case 4: return learned_launch_t<K, V, 512>(t, d_q, nq, d_out, d_found, s);
+        default: return learned_launch_t<K, V, 1024>(t, d_q, nq, d_out, d_found, s);
     }
 }
 
@@ -1233,13 +1244,13 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
 }  // namespace
 
 bt_status launch_learned_search(const bt_tree *t, const void *d_q, uint64_t nq, void *d_out,
-                                cudaStream_t s) {
+                                uint8_t *d_found, cudaStream_t s) {
     if (nq == 0) return BT_OK;
     if (t->key_bytes == 4)
-        return t->val_bytes == 4 ? learned_launch<uint32_t, uint32_t>(t, d_q, nq, d_out, s)
-                                 : learned_launch<uint32_t, uint64_t>(t, d_q, nq, d_out, s);
-    return t->val_bytes == 4 ? learned_launch<uint64_t, uint32_t>(t, d_q, nq, d_out, s)
-                             : learned_launch<uint64_t, uint64_t>(t, d_q, nq, d_out, s);
+        return t->val_bytes == 4 ? learned_launch<uint32_t, uint32_t>(t, d_q, nq, d_out, d_found, s)
+                                 : learned_launch<uint32_t, uint64_t>(t, d_q, nq, d_out, d_found, s);
+    return t->val_bytes == 4 ? learned_launch<uint64_t, uint32_t>(t, d_q, nq, d_out, d_found, s)
+                             : learned_launch<uint64_t, uint64_t>(t, d_q, nq, d_out, d_found, s);
 }
 
 bt_status reset_learned_stats(const bt_tree *t, cudaStream_t s) {

@@ -58,7 +58,8 @@ __host__ __device__ inline size_t scratch_offset(const DevTree &t) { return ((si
 template <typename K, typename V, int G, int R, bool PERM>
 __global__ void __launch_bounds__(kThreads)
 point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
-             const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out) {
+             const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out,
+             uint8_t *__restrict__ found) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *s_lvl = reinterpret_cast<K *>(smem_raw);
     stage_level<K>(s_lvl, t);
@@ -105,11 +106,17 @@ point_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
                 up[s] = false;
             }
             walk_global<K, G, I>(t, qe, up, node, grp, gl);
-            leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
-                const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                if (qi >= nq) return nullptr;
-                return out + (PERM ? (uint64_t)pv[s] : qi);
-            });
+            leaf_point<K, V, G, I>(
+                leaves, node, qv, qe, tmax, grp, gl,
+                [&](int s) -> V * {
+                    const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
+                    if (qi >= nq) return nullptr;
+                    return out + (PERM ? (uint64_t)pv[s] : qi);
+                },
+                [&](int s) -> uint8_t * {
+                    const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
+                    return found ? found + (PERM ? (uint64_t)pv[s] : qi) : nullptr;
+                });
         }
     }
 }
@@ -146,7 +153,8 @@ constexpr uint64_t kWinMinQueries = 1ull << 21;
 template <typename K, typename V, int G, int R>
 __global__ void __launch_bounds__(kWinThreads, 1)
 point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
-                    const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out, int shift) {
+                    const uint32_t *__restrict__ perm, uint64_t nq, V *__restrict__ out,
+                    uint8_t *__restrict__ found, int shift) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     K *s_win = reinterpret_cast<K *>(smem_raw);
     __shared__ uint32_t s_blk[2];
@@ -229,11 +237,14 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
                 up[s] = false;
             }
             walk_from<K, G, I>(t, from, qe, up, node, grp, gl);
-            leaf_point<K, V, G, I>(leaves, node, qv, qe, tmax, grp, gl, [&](int s) -> V * {
-                const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
-                if (qi >= nq) return nullptr;
-                return out + pv[s];
-            });
+            leaf_point<K, V, G, I>(
+                leaves, node, qv, qe, tmax, grp, gl,
+                [&](int s) -> V * {
+                    const uint64_t qi = base + (uint64_t)(r * (NG * I) + s * NG + grp);
+                    if (qi >= nq) return nullptr;
+                    return out + pv[s];
+                },
+                [&](int s) -> uint8_t * { return found ? found + pv[s] : nullptr; });
         }
     }
 }
@@ -526,21 +537,21 @@ bt_status set_smem(Fn fn, size_t smem) {
 
 template <typename K, typename V, int G, int R, bool PERM>
 bt_status point_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
-                       void *d_out, cudaStream_t s) {
+                       void *d_out, uint8_t *d_found, cudaStream_t s) {
     auto fn = point_kernel<K, V, G, R, PERM>;
     const size_t smem = scratch_offset(t->dev);
     bt_status st = set_smem(fn, smem);
     if (st != BT_OK) return st;
     const unsigned grid = persistent_grid((const void *)fn, smem, nq, kThreads);
     count_launch();
-    fn<<<grid, kThreads, smem, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out);
+    fn<<<grid, kThreads, smem, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out, d_found);
     BT_CUDA(cudaGetLastError());
     return BT_OK;
 }
 
 template <typename K, typename V, int G, int R>
 bt_status window_launch(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
-                        void *d_out, cudaStream_t s) {
+                        void *d_out, uint8_t *d_found, cudaStream_t s) {
     auto fn = point_window_kernel<K, V, G, R>;
     bt_status st = set_smem(fn, kWinBytes);
     if (st != BT_OK) return st;
@@ -548,29 +559,30 @@ bt_status window_launch(const bt_tree *t, const void *d_q, const uint32_t *d_per
     const unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ntiles, sm_count()));
     const int shift = std::max(0, bitlen64(t->max_key) - kPointGroupBits);  // as the grouping pass
     count_launch();
-    fn<<<grid, kWinThreads, kWinBytes, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out, shift);
+    fn<<<grid, kWinThreads, kWinBytes, s>>>(t->dev, (const K *)d_q, d_perm, nq, (V *)d_out, d_found,
+                                            shift);
     BT_CUDA(cudaGetLastError());
     return BT_OK;
 }
 
 template <typename K, typename V, bool PERM>
 bt_status point_cfg(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
-                    void *d_out, cudaStream_t s) {
+                    void *d_out, uint8_t *d_found, cudaStream_t s) {
     if (PERM && nq >= kWinMinQueries) {
         switch (t->search_cfg) {
-            case 0: return window_launch<K, V, 8, 1>(t, d_q, d_perm, nq, d_out, s);
-            case 1: return window_launch<K, V, 8, 2>(t, d_q, d_perm, nq, d_out, s);
-            case 2: return window_launch<K, V, 4, 1>(t, d_q, d_perm, nq, d_out, s);
-            case 3: return window_launch<K, V, 4, 2>(t, d_q, d_perm, nq, d_out, s);
-            default: return window_launch<K, V, 2, 1>(t, d_q, d_perm, nq, d_out, s);
+            case 0: return window_launch<K, V, 8, 1>(t, d_q, d_perm, nq, d_out, d_found, s);
+            case 1: return window_launch<K, V, 8, 2>(t, d_q, d_perm, nq, d_out, d_found, s);
+            case 2: return window_launch<K, V, 4, 1>(t, d_q, d_perm, nq, d_out, d_found, s);
+            case 3: return window_launch<K, V, 4, 2>(t, d_q, d_perm, nq, d_out, d_found, s);
+            default: return window_launch<K, V, 2, 1>(t, d_q, d_perm, nq, d_out, d_found, s);
         }
     }
     switch (t->search_cfg) {
-        case 0: return point_launch<K, V, 8, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 1: return point_launch<K, V, 8, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 2: return point_launch<K, V, 4, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
-        case 3: return point_launch<K, V, 4, 2, PERM>(t, d_q, d_perm, nq, d_out, s);
-        default: return point_launch<K, V, 2, 1, PERM>(t, d_q, d_perm, nq, d_out, s);
+        case 0: return point_launch<K, V, 8, 1, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
+        case 1: return point_launch<K, V, 8, 2, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
+        case 2: return point_launch<K, V, 4, 1, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
+        case 3: return point_launch<K, V, 4, 2, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
+        default: return point_launch<K, V, 2, 1, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
     }
 }
 
@@ -604,12 +616,12 @@ bt_status bounds_cfg(const bt_tree *t, const void *d_lo, const void *d_hi, const
 
 template <bool PERM>
 bt_status point_types(const bt_tree *t, const void *d_q, const uint32_t *d_perm, uint64_t nq,
-                      void *d_out, cudaStream_t s) {
+                      void *d_out, uint8_t *d_found, cudaStream_t s) {
     if (t->key_bytes == 4)
-        return t->val_bytes == 4 ? point_cfg<uint32_t, uint32_t, PERM>(t, d_q, d_perm, nq, d_out, s)
-                                 : point_cfg<uint32_t, uint64_t, PERM>(t, d_q, d_perm, nq, d_out, s);
-    return t->val_bytes == 4 ? point_cfg<uint64_t, uint32_t, PERM>(t, d_q, d_perm, nq, d_out, s)
-                             : point_cfg<uint64_t, uint64_t, PERM>(t, d_q, d_perm, nq, d_out, s);
+        return t->val_bytes == 4 ? point_cfg<uint32_t, uint32_t, PERM>(t, d_q, d_perm, nq, d_out, d_found, s)
+                                 : point_cfg<uint32_t, uint64_t, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
+    return t->val_bytes == 4 ? point_cfg<uint64_t, uint32_t, PERM>(t, d_q, d_perm, nq, d_out, d_found, s)
+                             : point_cfg<uint64_t, uint64_t, PERM>(t, d_q, d_perm, nq, d_out, d_found, s);
 }
 
 template <bool PERM>
@@ -627,7 +639,7 @@ bt_status bounds_types(const bt_tree *t, const void *d_lo, const void *d_hi, con
 }  // namespace
 
 bt_status launch_point_search(const bt_tree *t, const void *d_q, const uint32_t *d_perm,
-                              uint64_t nq, void *d_out, cudaStream_t s) {
+                              uint64_t nq, void *d_out, cudaStream_t s, uint8_t *d_found) {
     if (nq == 0) return BT_OK;
     if (t->n == 0) {
         unsigned g = (unsigned)std::min<uint64_t>((nq + 255) / 256, 4096);
@@ -637,10 +649,11 @@ bt_status launch_point_search(const bt_tree *t, const void *d_q, const uint32_t 
         else
             fill_kernel<uint64_t><<<g, 256, 0, s>>>((uint64_t *)d_out, nq, ~0ull);
         BT_CUDA(cudaGetLastError());
+        if (d_found) BT_CUDA(cudaMemsetAsync(d_found, 0, nq, s));
         return BT_OK;
     }
-    return d_perm ? point_types<true>(t, d_q, d_perm, nq, d_out, s)
-                  : point_types<false>(t, d_q, d_perm, nq, d_out, s);
+    return d_perm ? point_types<true>(t, d_q, d_perm, nq, d_out, d_found, s)
+                  : point_types<false>(t, d_q, d_perm, nq, d_out, d_found, s);
 }
 
 bt_status launch_bounds(const bt_tree *t, const void *d_lo, const void *d_hi,

@@ -215,15 +215,22 @@ struct LeafStage {
     static constexpr int KCPL = (NKC + G - 1) / G;       // key chunks per lane
 };
 
+// No found flags (leaf_point's default).
+struct NoFound {
+    __device__ uint8_t *operator()(int) const { return nullptr; }
+};
+
 // Leaf stage of I point queries.  Each query's leaf block (key chunks, then
 // value chunks) is loaded by its lane group with 16-byte streaming loads, the
 // lower-bound slot and the match are found, and the lane holding the value
-// writes it -- or all-ones on a miss -- to dst(s); dst returns null to skip
-// a slot.  leaves points at leaf block 0 of the tree; node[s] is the block.
-template <typename K, typename V, int G, int I, typename Dst>
+// writes it -- or all-ones on a miss -- to dst(s), and 1 or 0 to fdst(s)
+// when that is not null; dst returns null to skip a slot.  leaves points at
+// leaf block 0 of the tree; node[s] is the block.
+template <typename K, typename V, int G, int I, typename Dst, typename FDst = NoFound>
 __device__ __forceinline__ void leaf_point(const unsigned char *__restrict__ leaves,
                                            const uint32_t (&node)[I], const K (&qv)[I],
-                                           const K (&qe)[I], K tmax, int grp, int gl, Dst dst) {
+                                           const K (&qe)[I], K tmax, int grp, int gl, Dst dst,
+                                           FDst fdst = FDst()) {
     using LG = LeafGeom<K, V>;
     using LS = LeafStage<K, V, G>;
     const unsigned gmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (grp * G);
@@ -287,6 +294,7 @@ __device__ __forceinline__ void leaf_point(const unsigned char *__restrict__ lea
                     }
                 }
                 *d = found ? val : key_max<V>();
+                if (uint8_t *f = fdst(s)) *f = found ? 1 : 0;
             }
         }
     }

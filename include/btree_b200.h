@@ -170,6 +170,16 @@ BT_API bt_status bt_set_search_config(bt_tree *tree, int lanes_per_query, int ro
 BT_API bt_status bt_point_search(const bt_tree *tree, int mode, const void *d_queries, uint64_t nq,
                           void *d_out, void *stream);
 
+/*
+ * Point search with a found flag per query: as bt_point_search, and
+ * d_found[i] = 1 when key d_queries[i] is in the tree, else 0 (one byte per
+ * query).  The flag tells a stored value of all-ones from a miss, which the
+ * value alone cannot (the reference returns INVALID_DATA, BPTree.h:12, for
+ * both).  Same modes and limits as bt_point_search.
+ */
+BT_API bt_status bt_point_search_found(const bt_tree *tree, int mode, const void *d_queries,
+                                       uint64_t nq, void *d_out, uint8_t *d_found, void *stream);
+
 /* Same with host buffers; copies are pipelined with the search in chunks.
  * Returns when h_out is filled. */
 BT_API bt_status bt_point_search_host(const bt_tree *tree, int mode, const void *h_queries,
