@@ -142,6 +142,7 @@ _PROTOS = {
     "bt_server_get_stats": (_I, [_P, ctypes.POINTER(bt_server_stats)]),
     "bt_server_destroy": (_I, [_P]),
     "bt_server_replay": (_I, [_P, _U64, _P, _P, _P, _P, _P, ctypes.POINTER(ctypes.c_double)]),
+    "bt_forest_set_stage_fanout": (_I, [_P, ctypes.c_uint32]),
 }
 
 
@@ -472,6 +473,12 @@ class Forest:
                                      self.value_bytes, _stream_ptr(stream), ctypes.byref(h)),
                "bt_forest_build")
         self._h = h
+
+    def set_stage_fanout(self, entries_per_descent):
+        """Fanout of the shared-memory root for plans made afterwards
+        (bt_forest_set_stage_fanout; default 16)."""
+        _check(lib().bt_forest_set_stage_fanout(self._h, entries_per_descent),
+               "bt_forest_set_stage_fanout")
 
     def plan(self, queries, q_offsets, out, lo=None, hi=None, r_offsets=None, counts=None,
              lanes_per_query=4, rounds=1, tile=1024):

@@ -101,6 +101,9 @@ def tune(tree, queries, mode="basic", hi=None, repeats=5, cache_path=None, confi
 
 FOREST_SHAPES = ((4, 1), (8, 1), (8, 2))
 FOREST_TILES = (512, 2048, 8192)
+# staged-root fanouts (bt_forest_set_stage_fanout), tried at the best shape
+# and tile found with the default 16
+FOREST_FANOUTS = (4, 16, 64)
 
 
 def _forest_key(forest, nq, nr):
@@ -109,51 +112,67 @@ def _forest_key(forest, nq, nr):
 
 
 def tune_forest(forest, queries, q_offsets, out, lo=None, hi=None, r_offsets=None, counts=None,
-                shapes=FOREST_SHAPES, tiles=FOREST_TILES, repeats=3, flush=None,
-                cache_path=None):
-    """Pick the forest search plan's (lanes per query, rounds, tile) for this
-    batch: every candidate is planned (one captured CUDA-graph launch) and
-    timed with CUDA events (an L2 flush before each timed launch when
-    `flush`, a CUDA tensor, is given).  Returns (lanes, rounds, tile, {name:
-    ms}); with cache_path the decision is stored and reused per forest and
-    batch shape."""
+                shapes=FOREST_SHAPES, tiles=FOREST_TILES, fanouts=FOREST_FANOUTS, repeats=3,
+                flush=None, cache_path=None):
+    """Pick the forest search plan's (lanes per query, rounds, tile) and the
+    staged-root fanout for this batch: every (shape, tile) candidate is
+    planned at fanout 16 (one captured CUDA-graph launch) and timed with CUDA
+    events (an L2 flush before each timed launch when `flush`, a CUDA tensor,
+    is given), then the fanouts are tried at the best of them.  Sets the
+    chosen fanout on `forest` and returns (lanes, rounds, tile, fanout,
+    {name: ms}); with cache_path the decision is stored and reused per forest
+    and batch shape."""
     import torch
     key = _forest_key(forest, len(queries), 0 if lo is None else len(lo))
     if cache_path and os.path.exists(cache_path):
         with open(cache_path) as f:
             cached = json.load(f).get(key)
         if cached:
-            lanes, rounds, tile = cached["best"]
-            return lanes, rounds, tile, cached["ms"]
+            lanes, rounds, tile, fanout = cached["best"]
+            forest.set_stage_fanout(fanout)
+            return lanes, rounds, tile, fanout, cached["ms"]
     stream = torch.cuda.current_stream(queries.device)
     ms = {}
+
+    def time_plan(lanes, rounds, tile):
+        with forest.plan(queries, q_offsets, out, lo, hi, r_offsets, counts, lanes, rounds,
+                         tile=tile) as p:
+            p.run(stream)
+            ts = []
+            for _ in range(repeats):
+                if flush is not None:
+                    flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                p.run(stream)
+                b.record(stream)
+                b.synchronize()
+                ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    forest.set_stage_fanout(16)
     for lanes, rounds in shapes:
         for tile in tiles:
-            with forest.plan(queries, q_offsets, out, lo, hi, r_offsets, counts, lanes, rounds,
-                             tile=tile) as p:
-                p.run(stream)
-                ts = []
-                for _ in range(repeats):
-                    if flush is not None:
-                        flush.zero_()
-                    a = torch.cuda.Event(enable_timing=True)
-                    b = torch.cuda.Event(enable_timing=True)
-                    a.record(stream)
-                    p.run(stream)
-                    b.record(stream)
-                    b.synchronize()
-                    ts.append(a.elapsed_time(b))
-                ms[f"{lanes}x{rounds}/t{tile}"] = statistics.median(ts)
+            ms[f"{lanes}x{rounds}/t{tile}/f16"] = time_plan(lanes, rounds, tile)
     best = min(ms, key=ms.get)
     lanes, rounds = (int(x) for x in best.split("/")[0].split("x"))
-    tile = int(best.split("/t")[1])
+    tile = int(best.split("/t")[1].split("/")[0])
+    for fo in fanouts:
+        name = f"{lanes}x{rounds}/t{tile}/f{fo}"
+        if name not in ms:
+            forest.set_stage_fanout(fo)
+            ms[name] = time_plan(lanes, rounds, tile)
+    best = min(ms, key=ms.get)
+    fanout = int(best.split("/f")[1])
+    forest.set_stage_fanout(fanout)
     if cache_path:
         data = {}
         if os.path.exists(cache_path):
             with open(cache_path) as f:
                 data = json.load(f)
-        data[key] = {"best": [lanes, rounds, tile], "ms": ms}
+        data[key] = {"best": [lanes, rounds, tile, fanout], "ms": ms}
         os.makedirs(os.path.dirname(os.path.abspath(cache_path)), exist_ok=True)
         with open(cache_path, "w") as f:
             json.dump(data, f, indent=1, sort_keys=True)
-    return lanes, rounds, tile, ms
+    return lanes, rounds, tile, fanout, ms

@@ -133,6 +133,9 @@ struct bt_forest {
     void *d_seps = nullptr;
     bt::FTree *d_desc = nullptr;
     std::vector<bt::FTree> h_desc;
+    // staged-root fanout: separator entries a work item may stage in shared
+    // memory per descent it makes (bt_forest_set_stage_fanout)
+    uint32_t stage_fanout = 16;
 };
 
 struct bt_forest_plan {
@@ -533,7 +536,9 @@ bt_status bt_forest_plan_create(const bt_forest *f, const void *d_q, const uint6
             return fail(BT_ERR_INVALID_ARGUMENT, "lo, hi or counts is NULL");
     }
     // The level each item stages: the deepest one that fits kFStageBytes and
-    // is not much larger than the descents it saves (16 entries per descent).
+    // is not much larger than the descents it saves (stage_fanout entries
+    // per descent: the fanout of the shared-memory root the item's queries
+    // search first).
     {
         const int kb = f->key_bytes;
         const uint64_t S = kSectorBytes / kb, F = kLineBytes / kb;
@@ -545,7 +550,7 @@ bt_status bt_forest_plan_create(const bt_forest *f, const void *d_q, const uint6
                 const uint64_t nb = (d.n + S - 1) / S;
                 const uint64_t ent = l + 1 < d.nlevels ? d.lvl_off[l + 1] - d.lvl_off[l]
                                                        : (nb + F - 1) / F * F;
-                if (ent * kb <= kFStageBytes && ent <= 16 * descents) {
+                if (ent * kb <= kFStageBytes && ent <= (uint64_t)f->stage_fanout * descents) {
                     it.slvl = l;
                     it.sm = (uint32_t)ent;
                     break;
@@ -584,6 +589,15 @@ bt_status bt_forest_plan_create(const bt_forest *f, const void *d_q, const uint6
         return st;
     }
     *out = p;
+    return BT_OK;
+}
+
+bt_status bt_forest_set_stage_fanout(bt_forest *f, uint32_t entries_per_descent) {
+    using namespace bt;
+    if (!f) return fail(BT_ERR_INVALID_ARGUMENT, "forest is NULL");
+    if (entries_per_descent < 1 || entries_per_descent > 4096)
+        return fail(BT_ERR_INVALID_ARGUMENT, "entries_per_descent must be 1..4096");
+    f->stage_fanout = entries_per_descent;
     return BT_OK;
 }
 

@@ -364,8 +364,8 @@ def forest_section(args, device, bt, flush):
     out = torch.empty(len(q), dtype=torch.uint32, device=device)
     counts = torch.empty(len(lo), dtype=torch.uint64, device=device)
     at = importlib.import_module(PKG + ".autotune")
-    lanes, rounds, tile, tried = at.tune_forest(f, dq, qoff, out, dlo, dhi, roff, counts,
-                                                flush=flush)
+    lanes, rounds, tile, fanout, tried = at.tune_forest(f, dq, qoff, out, dlo, dhi, roff, counts,
+                                                        flush=flush)
     with f.plan(dq, qoff, out, dlo, dhi, roff, counts, lanes, rounds, tile=tile) as p:
         l0 = bt.kernel_launches()
         ms = _timed_ms(lambda: p.run(stream), stream, flush, args.steps)
@@ -401,7 +401,7 @@ def forest_section(args, device, bt, flush):
                      f"U~[10,20]); {len(q)} point queries (80% hits) + {len(lo)} range queries"),
         "value": total / (ms / 1e3), "unit": "queries/s", "ms_per_batch": ms,
         "graph_launches_per_batch": launches, "lanes_per_query": lanes, "rounds": rounds,
-        "tile": tile, "autotune_ms": tried, "answers_consistent": ok,
+        "tile": tile, "stage_fanout": fanout, "autotune_ms": tried, "answers_consistent": ok,
         "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": alg / (ms / 1e3) / 1e9 / peak},
     }

@@ -413,6 +413,18 @@ BT_API bt_status bt_forest_plan_create(const bt_forest *forest, const void *d_qu
                                        const void *d_hi, const uint64_t *h_r_offsets,
                                        uint64_t *d_counts, int lanes_per_query, int rounds,
                                        uint32_t tile, bt_forest_plan **out);
+/*
+ * Fanout of the shared-memory root of the forest search, used by the plans
+ * made after the call: each work item stages in shared memory the deepest
+ * separator level of its tree that fits 16 KB and has at most
+ * entries_per_descent entries per descent the item makes (default 16), and
+ * one binary search there replaces every level above it.  A larger value
+ * stages deeper levels for fewer queries.  Node lines themselves stay 128
+ * bytes (16 u64 or 32 u32 separators); the reference's fixed fanout is
+ * PAGESIZE = 5000 (BPTree.h:8).  The autotuner (autotune.tune_forest) picks
+ * it with the tile and lanes per query.  Results do not depend on it.
+ */
+BT_API bt_status bt_forest_set_stage_fanout(bt_forest *forest, uint32_t entries_per_descent);
 /* Launch the plan's graph on `stream` (asynchronous). */
 BT_API bt_status bt_forest_plan_run(bt_forest_plan *plan, void *stream);
 BT_API bt_status bt_forest_plan_destroy(bt_forest_plan *plan);

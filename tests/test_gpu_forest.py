@@ -19,12 +19,10 @@ def make_forest(g, sizes, kt):
     return keys, np.array(off, dtype=np.uint64)
 
 
-@pytest.mark.parametrize("kt,vt", [(np.uint32, np.uint32), (np.uint64, np.uint64),
-                                   (np.uint32, np.uint64)])
-@pytest.mark.parametrize("cfg,tile", [((4, 1), 1024), ((8, 2), 256), ((2, 1), 32), ((8, 1), 4096)])
-def test_forest_matches_oracle(bt, orc, cuda, kt, vt, cfg, tile):
+def forest_case(kt, vt, cuda, seed=7):
+    """Uneven trees (some empty) with point queries (80% hits) and ranges."""
     import torch
-    g = np.random.default_rng(7)
+    g = np.random.default_rng(seed)
     sizes = [0, 1, 7, 8, 9, 100, 1000, 5000, 0, 33333, 2, 70001, 1 << 16, 3]
     keys, off = make_forest(g, sizes, kt)
     vals = [np.arange(len(k), dtype=vt) * 3 + 1 for k in keys]
@@ -48,27 +46,82 @@ def test_forest_matches_oracle(bt, orc, cuda, kt, vt, cfg, tile):
         his.append(hi.astype(kt))
         roff.append(roff[-1] + r)
     cat = lambda xs, t: np.concatenate(xs).astype(t) if len(xs) else np.zeros(0, t)  # noqa: E731
-    dq = dev(cat(qs, kt), cuda)
-    dlo, dhi = dev(cat(los, kt), cuda), dev(cat(his, kt), cuda)
-    out = torch.empty(len(dq), dtype={4: torch.uint32, 8: torch.uint64}[np.dtype(vt).itemsize],
-                      device=cuda)
-    counts = torch.empty(len(dlo), dtype=torch.uint64, device=cuda)
-    with bt.Forest(dev(cat(keys, kt), cuda), dev(cat(vals, vt), cuda), off) as f:
-        with f.plan(dq, qoff, out, dlo, dhi, roff, counts, *cfg, tile=tile) as p:
+    c = dict(keys=keys, vals=vals, off=off, qs=qs, qoff=qoff, los=los, his=his, roff=roff)
+    c["dkeys"], c["dvals"] = dev(cat(keys, kt), cuda), dev(cat(vals, vt), cuda)
+    c["dq"] = dev(cat(qs, kt), cuda)
+    c["dlo"], c["dhi"] = dev(cat(los, kt), cuda), dev(cat(his, kt), cuda)
+    c["out"] = torch.empty(len(c["dq"]), dtype={4: torch.uint32, 8: torch.uint64}[np.dtype(vt).itemsize],
+                           device=cuda)
+    c["counts"] = torch.empty(len(c["dlo"]), dtype=torch.uint64, device=cuda)
+    return c
+
+
+def check_forest(orc, c, vt):
+    got, gotc = c["out"].cpu().numpy(), c["counts"].cpu().numpy()
+    for t, k in enumerate(c["keys"]):
+        sl = slice(int(c["qoff"][t]), int(c["qoff"][t + 1]))
+        exp = orc.point_search(k, c["vals"][t], c["qs"][t]) if len(k) else \
+            np.full(len(c["qs"][t]), np.iinfo(vt).max, dtype=vt)
+        assert np.array_equal(got[sl], exp), t
+        rs = slice(int(c["roff"][t]), int(c["roff"][t + 1]))
+        expc = orc.range_count(k, c["los"][t], c["his"][t]) if len(k) else np.zeros(len(c["los"][t]))
+        assert np.array_equal(gotc[rs], expc), t
+
+
+def run_plan(f, c, cfg, tile):
+    import torch
+    with f.plan(c["dq"], c["qoff"], c["out"], c["dlo"], c["dhi"], c["roff"], c["counts"], *cfg,
+                tile=tile) as p:
+        c["out"].fill_(0)
+        c["counts"].fill_(7)
+        p.run()
+        torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("kt,vt", [(np.uint32, np.uint32), (np.uint64, np.uint64),
+                                   (np.uint32, np.uint64)])
+@pytest.mark.parametrize("cfg,tile", [((4, 1), 1024), ((8, 2), 256), ((2, 1), 32), ((8, 1), 4096)])
+def test_forest_matches_oracle(bt, orc, cuda, kt, vt, cfg, tile):
+    import torch
+    c = forest_case(kt, vt, cuda)
+    with bt.Forest(c["dkeys"], c["dvals"], c["off"]) as f:
+        with f.plan(c["dq"], c["qoff"], c["out"], c["dlo"], c["dhi"], c["roff"], c["counts"], *cfg,
+                    tile=tile) as p:
             for _ in range(2):  # the graph replays
-                out.fill_(0)
-                counts.fill_(7)
+                c["out"].fill_(0)
+                c["counts"].fill_(7)
                 p.run()
                 torch.cuda.synchronize()
-                got, gotc = out.cpu().numpy(), counts.cpu().numpy()
-                for t, k in enumerate(keys):
-                    sl = slice(int(qoff[t]), int(qoff[t + 1]))
-                    exp = orc.point_search(k, vals[t], qs[t]) if len(k) else \
-                        np.full(len(qs[t]), np.iinfo(vt).max, dtype=vt)
-                    assert np.array_equal(got[sl], exp), t
-                    rs = slice(int(roff[t]), int(roff[t + 1]))
-                    expc = orc.range_count(k, los[t], his[t]) if len(k) else np.zeros(len(los[t]))
-                    assert np.array_equal(gotc[rs], expc), t
+                check_forest(orc, c, vt)
+
+
+@pytest.mark.parametrize("fanout", [1, 4, 64, 4096])
+def test_forest_stage_fanout(bt, orc, cuda, fanout):
+    """The staged-root fanout changes which level a work item stages, never
+    the answers."""
+    c = forest_case(np.uint64, np.uint32, cuda, seed=11)
+    with bt.Forest(c["dkeys"], c["dvals"], c["off"]) as f:
+        f.set_stage_fanout(fanout)
+        run_plan(f, c, (4, 1), 512)
+        check_forest(orc, c, np.uint32)
+
+
+def test_forest_tuner_picks_fanout_and_caches(bt, orc, cuda, tmp_path):
+    import importlib
+    at = importlib.import_module("b-tree-index-searching_b200.autotune")
+    c = forest_case(np.uint32, np.uint32, cuda, seed=3)
+    cache = str(tmp_path / "forest.json")
+    with bt.Forest(c["dkeys"], c["dvals"], c["off"]) as f:
+        args = (f, c["dq"], c["qoff"], c["out"], c["dlo"], c["dhi"], c["roff"], c["counts"])
+        lanes, rounds, tile, fanout, ms = at.tune_forest(*args, repeats=1, cache_path=cache)
+        assert fanout in at.FOREST_FANOUTS and (lanes, rounds) in at.FOREST_SHAPES
+        assert len(ms) == len(at.FOREST_SHAPES) * len(at.FOREST_TILES) + len(at.FOREST_FANOUTS) - 1
+        assert at.tune_forest(*args, repeats=1, cache_path=cache)[:4] == (lanes, rounds, tile, fanout)
+        run_plan(f, c, (lanes, rounds), tile)
+        check_forest(orc, c, np.uint32)
+    with bt.Forest(c["dkeys"], c["dvals"], c["off"]) as f:
+        with pytest.raises(bt.BTreeError):
+            f.set_stage_fanout(0)
 
 
 def test_forest_rejects_unsorted_tree(bt, cuda):
