@@ -128,56 +128,6 @@ __device__ __forceinline__ int box_runs(uint32_t x0, uint32_t y0, uint32_t x1, u
     return nruns;
 }
 
-// Bounds of up to NR runs (NR = 8 or 16), 2 NR descents in one round with
-// 4 lanes per descent: descent d < NR is the lower bound of run d's first
-// code, d >= NR the upper bound of run d - NR's last code.  Lane r < 16
-// receives the first key position of run r, lane 16 + r the position after
-// its last key (as cell_bounds does for cells).
-template <typename V, int NR>
-__device__ __forceinline__ uint32_t run_bounds(const DevTree &t, const uint32_t *s_lvl,
-                                               uint32_t *res, const Cell &run, int lane) {
-    using LG = LeafGeom<uint32_t, V>;
-    constexpr int G = 4, NG = 32 / G, I = 2 * NR / NG;
-    const int grp = lane / G, gl = lane % G;
-    const uint32_t tmax = (uint32_t)t.max_key;
-    // the query of descent d = lane (lanes >= 2 NR idle in the search)
-    const int d = lane;
-    const int ri = d % NR;
-    const bool upper = d >= NR;
-    const uint32_t zs = __shfl_sync(0xffffffffu, run.zs, ri);
-    const uint32_t ze = __shfl_sync(0xffffffffu, run.ze, ri);
-    const uint32_t a = upper ? ze : zs;
-    const bool up = upper && a < tmax;
-    const uint32_t qa = a < tmax ? a : tmax;
-    const uint32_t nd = d < 2 * NR ? smem_bound<uint32_t>(s_lvl, t.smem_entries, qa, up) : 0u;
-    uint32_t qe[I], node[I];
-    bool ups[I];
-#pragma unroll
-    for (int s = 0; s < I; s++) {
-        const int k = s * NG + grp;
-        qe[s] = __shfl_sync(0xffffffffu, qa, k);
-        node[s] = __shfl_sync(0xffffffffu, nd, k);
-        ups[s] = __shfl_sync(0xffffffffu, (int)up, k) != 0;
-    }
-    walk_global<uint32_t, G, I>(t, qe, ups, node, grp, gl);
-    int pos[I];
-    leaf_bound<uint32_t, V, G, I>(static_cast<const unsigned char *>(t.leaves), node, qe, ups, grp,
-                                  gl, pos);
-#pragma unroll
-    for (int s = 0; s < I; s++)
-        if (gl == 0) res[s * NG + grp] = node[s] * (uint32_t)LG::S + (uint32_t)pos[s];
-    __syncwarp();
-    const int r = lane % kMaxCells;
-    const bool want_upper = lane >= kMaxCells;
-    // beyond the keys: a lower bound of a code above the largest key, or an
-    // upper bound of one at or above it, is n
-    const uint32_t mine = want_upper ? run.ze : run.zs;
-    const bool beyond = want_upper ? mine >= tmax : mine > tmax;
-    const uint32_t v = r < NR ? res[(want_upper ? NR : 0) + r] : 0u;
-    __syncwarp();
-    return beyond ? (uint32_t)t.n : v;
-}
-
 // Exclusive prefix sum over the warp.
 __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, int lane, uint32_t &total) {
     uint32_t x = v;
@@ -188,6 +138,75 @@ __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, int lane, uint32_
     }
     total = __shfl_sync(0xffffffffu, x, 31);
     return x - v;
+}
+
+// Lower bounds of the codes held by lanes c < nc (lane c receives the first
+// key position at or above its code; n when the code is above every key):
+// 4 lanes per descent, I descents in flight per lane group, so up to 8 I
+// codes in one round.  res is 32 words of per-warp scratch.
+template <typename V, int I>
+__device__ __forceinline__ uint32_t code_lower_bounds(const DevTree &t, const uint32_t *s_lvl,
+                                                      uint32_t *res, uint32_t code, bool have,
+                                                      int lane) {
+    using LG = LeafGeom<uint32_t, V>;
+    constexpr int G = 4, NG = 32 / G;
+    const int grp = lane / G, gl = lane % G;
+    const uint32_t tmax = (uint32_t)t.max_key;
+    const uint32_t qa = code < tmax ? code : tmax;
+    const uint32_t nd = have ? smem_bound<uint32_t>(s_lvl, t.smem_entries, qa, false) : 0u;
+    uint32_t qe[I], node[I];
+    bool ups[I];
+#pragma unroll
+    for (int s = 0; s < I; s++) {
+        const int k = s * NG + grp;
+        qe[s] = __shfl_sync(0xffffffffu, qa, k);
+        node[s] = __shfl_sync(0xffffffffu, nd, k);
+        ups[s] = false;
+    }
+    walk_global<uint32_t, G, I>(t, qe, ups, node, grp, gl);
+    int pos[I];
+    leaf_bound<uint32_t, V, G, I>(static_cast<const unsigned char *>(t.leaves), node, qe, ups, grp,
+                                  gl, pos);
+#pragma unroll
+    for (int s = 0; s < I; s++)
+        if (gl == 0) res[s * NG + grp] = node[s] * (uint32_t)LG::S + (uint32_t)pos[s];
+    __syncwarp();
+    const uint32_t v = res[lane];
+    __syncwarp();
+    return code > tmax ? (uint32_t)t.n : v;
+}
+
+// Key positions of the box's runs: run r (lane r < nruns) holds the keys
+// [lower(zs_r), lower(ze_r + 1)).  When run r + 1 starts at ze_r + 1 the two
+// bounds are one descent, so the distinct boundary codes (at most 2 nruns,
+// in Z order) are gathered first and each is descended once.  Lane r < 16
+// receives lo = the first key position of run r and hi = the position after
+// its last key.
+template <typename V>
+__device__ __forceinline__ void run_bounds(const DevTree &t, const uint32_t *s_lvl, uint32_t *res,
+                                           const Cell &run, int nruns, int lane, uint32_t &lo,
+                                           uint32_t &hi) {
+    const bool rv = lane < nruns;
+    const uint32_t nzs = __shfl_sync(0xffffffffu, run.zs, (lane + 1) & 31);
+    const bool top = run.ze == 0xFFFFFFFFu;  // no code above: the run ends with the keys
+    const bool own_end = rv && !top && !(lane + 1 < nruns && nzs == run.ze + 1u);
+    uint32_t nc;
+    const uint32_t at = warp_excl_scan(rv ? 1u + (own_end ? 1u : 0u) : 0u, lane, nc);
+    if (rv) {
+        res[at] = run.zs;
+        if (own_end) res[at + 1] = run.ze + 1u;
+    }
+    __syncwarp();
+    const bool have = (uint32_t)lane < nc;
+    const uint32_t code = have ? res[lane] : 0u;
+    __syncwarp();
+    const uint32_t lb = nc <= 8    ? code_lower_bounds<V, 1>(t, s_lvl, res, code, have, lane)
+                        : nc <= 16 ? code_lower_bounds<V, 2>(t, s_lvl, res, code, have, lane)
+                                   : code_lower_bounds<V, 4>(t, s_lvl, res, code, have, lane);
+    lo = __shfl_sync(0xffffffffu, lb, at & 31);
+    // the code after run r's: its own end, or the next run's start
+    const uint32_t nx = __shfl_sync(0xffffffffu, lb, (at + 1) & 31);
+    hi = top ? (uint32_t)t.n : nx;
 }
 
 // Cell (0..15) whose run holds item k of the concatenated runs, given each
@@ -238,9 +257,8 @@ rect_count_kernel(const __grid_constant__ DevTree t, const uint16_t *__restrict_
         const ZBox box(x0, y0, x1, y1);
         Cell cell;
         const int nruns = box_runs(x0, y0, x1, y1, lane, res, cell);
-        const uint32_t b = nruns <= 8 ? run_bounds<V, 8>(t, s_lvl, res, cell, lane)
-                                      : run_bounds<V, 16>(t, s_lvl, res, cell, lane);
-        const uint32_t ub = __shfl_sync(0xffffffffu, b, (lane + kMaxCells) & 31);
+        uint32_t b, ub;
+        run_bounds<V>(t, s_lvl, res, cell, nruns, lane, b, ub);
         const uint32_t len = (lane < kMaxCells && cell.valid && ub > b) ? ub - b : 0u;
         uint32_t total;
         // whole runs of the cells inside the box; edge cells are scanned
