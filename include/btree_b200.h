@@ -303,12 +303,14 @@ BT_API bt_status bt_range_count_host(const bt_tree *tree, int mode, const void *
  *    GPU by full-batch Adam with this library's own forward/backward kernels;
  *    its worst error over the lines' first keys bounds a shared-memory search
  *    over those keys;
- *  - unit thresholds: one 16-bit code per leaf-unit boundary (59 per
+ *  - unit thresholds: one 15-bit code per leaf-unit boundary (59 per
  *    128-byte line with a 64-bit base and a shift), an exact separator
  *    between the units' key ranges.
  * A query: the root and a short shared-memory search give the segment line
- * (one L2 read), the segment's line and eps a window of ranks, the window's
- * codes (one or two L2 lines) the leaf unit, which is the only DRAM read.
+ * (one L2 read), the segment's line and eps a window of ranks, the code line
+ * of the predicted unit (one L2 read; the neighbouring line too for the
+ * queries whose count continues there) the leaf unit, which is the only
+ * DRAM read.
  * A query whose key lies past the unit's last key reads the next unit; one
  * that leaves the window takes the tree's full descent: results are always
  * the plain search's.
