@@ -182,20 +182,18 @@ __device__ __forceinline__ double pla_line_at0(const PlaPt &a, const PlaPt &b, d
 // lines of largest (M = Ma-Mb) and smallest (N = Na-Nb) slope; a point is
 // feasible iff its lower point is not above M and its upper point not below
 // N.  A segment also closes when a hull would exceed kHullCap points.
-// COUNT: counts[y * nchunks + c] = segments of chunk c at the bound
-// eps_list[y] (y = blockIdx.y: several bounds in one launch).  Otherwise
-// writes segment k of chunk c (bound eps) at offsets[c] + k: first rank and
-// the mean of M and N as rank - first = icpt + slope * (key - first key).
+// COUNT: counts[c] = segments of chunk c.  Otherwise writes segment k of
+// chunk c at offsets[c] + k: first rank and the mean of M and N as
+// rank - first = icpt + slope * (key - first key).
 template <typename K, typename V, bool COUNT>
 __global__ void pla_kernel(const unsigned char *__restrict__ leaves, uint64_t n, uint32_t eps,
-                           const uint32_t *__restrict__ eps_list, uint64_t nchunks,
-                           uint64_t *__restrict__ counts, const uint64_t *__restrict__ offsets,
-                           uint32_t *__restrict__ starts, double *__restrict__ slopes,
-                           double *__restrict__ icpts) {
+                           uint64_t nchunks, uint64_t *__restrict__ counts,
+                           const uint64_t *__restrict__ offsets, uint32_t *__restrict__ starts,
+                           double *__restrict__ slopes, double *__restrict__ icpts) {
     const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (c >= nchunks) return;
     PlaPt lh[kHullCap], uh[kHullCap];
-    const int64_t e = (int64_t)(COUNT ? eps_list[blockIdx.y] : eps);
+    const int64_t e = (int64_t)eps;
     const uint64_t end = min(n, (c + 1) * kPlaChunk);
     uint64_t nseg = 0, out = COUNT ? 0 : offsets[c];
     uint64_t i = c * kPlaChunk;
@@ -260,23 +258,7 @@ __global__ void pla_kernel(const unsigned char *__restrict__ leaves, uint64_t n,
         nseg++;
         i = j;
     }
-    if (COUNT) counts[(uint64_t)blockIdx.y * nchunks + c] = nseg;
-}
-
-// totals[y] = sum of counts[y * n .. y * n + n - 1] (one block per row).
-__global__ void row_sums_kernel(const uint64_t *__restrict__ counts, uint64_t n,
-                                uint64_t *__restrict__ totals) {
-    __shared__ unsigned long long part[32];
-    unsigned long long v = 0;
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) v += counts[(uint64_t)blockIdx.y * n + i];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        v = threadIdx.x < blockDim.x / 32 ? part[threadIdx.x] : 0ull;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (threadIdx.x == 0) totals[blockIdx.y] = v;
-    }
+    if (COUNT) counts[c] = nseg;
 }
 
 // Segment lines from the segmentation (one thread per line): first keys,
@@ -1076,36 +1058,10 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     BT_CUDA(cudaMalloc(&btot.p, sizeof(uint64_t)));
     uint64_t *cnt = (uint64_t *)bcnt.p, *off = (uint64_t *)boff.p, *tot = (uint64_t *)btot.p;
     const unsigned pg = (unsigned)((nchunks + 63) / 64);
-    // segment totals of up to kEpsBatch bounds per launch (one grid row per
-    // bound): the search for the least bound meeting the target takes a few
-    // launches instead of one per bisection step
-    constexpr int kEpsBatch = 15;
-    DevBuf bcm, bel, btm;
-    BT_CUDA(cudaMalloc(&bcm.p, (size_t)kEpsBatch * nchunks * sizeof(uint64_t)));
-    BT_CUDA(cudaMalloc(&bel.p, kEpsBatch * sizeof(uint32_t)));
-    BT_CUDA(cudaMalloc(&btm.p, kEpsBatch * sizeof(uint64_t)));
-    auto count_many = [&](const std::vector<uint32_t> &cands, std::vector<uint64_t> &totals) -> bt_status {
-        const int m = (int)cands.size();
-        BT_CUDA(cudaMemcpyAsync(bel.p, cands.data(), m * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-        count_launch();
-        pla_kernel<K, V, true><<<dim3(pg, m), 64, 0, s>>>(leaves, n, 0, (const uint32_t *)bel.p, nchunks,
-                                                         (uint64_t *)bcm.p, nullptr, nullptr, nullptr,
-                                                         nullptr);
-        BT_CUDA(cudaGetLastError());
-        count_launch();
-        row_sums_kernel<<<dim3(1, m), 256, 0, s>>>((const uint64_t *)bcm.p, nchunks, (uint64_t *)btm.p);
-        BT_CUDA(cudaGetLastError());
-        totals.assign(m, 0);
-        BT_CUDA(cudaMemcpyAsync(totals.data(), btm.p, m * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
-        BT_CUDA(cudaStreamSynchronize(s));
-        return BT_OK;
-    };
     auto count_at = [&](uint32_t eps, uint64_t *total) -> bt_status {
-        const uint32_t one = eps;
-        BT_CUDA(cudaMemcpyAsync(bel.p, &one, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
         count_launch();
-        pla_kernel<K, V, true><<<pg, 64, 0, s>>>(leaves, n, 0, (const uint32_t *)bel.p, nchunks, cnt,
-                                                 nullptr, nullptr, nullptr, nullptr);
+        pla_kernel<K, V, true><<<pg, 64, 0, s>>>(leaves, n, eps, nchunks, cnt, nullptr, nullptr,
+                                                 nullptr, nullptr);
         BT_CUDA(cudaGetLastError());
         bt_status r = launch_scan_u64(cnt, off, nchunks, tot, s);
         if (r != BT_OK) return r;
@@ -1117,42 +1073,20 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     uint64_t nseg = 0;
     bt_status r;
     if (eps == 0) {
-        // The least bound whose segmentation has at most num_segments
-        // segments (the count does not grow with the bound): first the
-        // bounds 8, 16, .., 8 * 2^14 in one launch, then the bracket
-        // (lo, hi] cut into kEpsBatch + 1 parts per launch.
-        uint32_t lo = 0, hi = 0;
-        std::vector<uint32_t> cands;
-        std::vector<uint64_t> tots;
-        for (uint32_t start = 8; hi == 0;) {
-            cands.clear();
-            for (int k = 0; k < kEpsBatch && start <= (1u << 30); k++, start *= 2) cands.push_back(start);
-            if ((r = count_many(cands, tots)) != BT_OK) return r;
-            for (size_t k = 0; k < cands.size() && hi == 0; k++) {
-                if (tots[k] <= cfg.num_segments) hi = cands[k];
-                else lo = cands[k];
-            }
-            if (hi == 0 && start > (1u << 30)) hi = cands.back();  // the loosest bound tried
+        // the least bound whose segmentation has at most num_segments segments
+        uint32_t lo = 0, hi = 8;
+        for (;;) {
+            if ((r = count_at(hi, &nseg)) != BT_OK) return r;
+            if (nseg <= cfg.num_segments || hi >= (1u << 30)) break;
+            lo = hi;
+            hi *= 2;
         }
         while (hi - lo > 1) {
-            cands.clear();
-            const uint64_t w = hi - lo;
-            for (int k = 1; k <= kEpsBatch; k++) {
-                const uint32_t c = lo + (uint32_t)((w * (uint64_t)k) / (kEpsBatch + 1));
-                if (c > lo && c < hi && (cands.empty() || c > cands.back())) cands.push_back(c);
-            }
-            if (cands.empty()) break;
-            if ((r = count_many(cands, tots)) != BT_OK) return r;
-            uint32_t nlo = lo, nhi = hi;
-            for (size_t k = 0; k < cands.size(); k++) {
-                if (tots[k] <= cfg.num_segments) {
-                    nhi = cands[k];
-                    break;
-                }
-                nlo = cands[k];
-            }
-            lo = nlo;
-            hi = nhi;
+            const uint32_t mid = lo + (hi - lo) / 2;
+            uint64_t c = 0;
+            if ((r = count_at(mid, &c)) != BT_OK) return r;
+            if (c <= cfg.num_segments) hi = mid;
+            else lo = mid;
         }
         eps = hi;
     }
@@ -1170,7 +1104,7 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     BT_CUDA(cudaMalloc(&bsl.p, nseg * sizeof(double)));
     BT_CUDA(cudaMalloc(&bic.p, nseg * sizeof(double)));
     count_launch();
-    pla_kernel<K, V, false><<<pg, 64, 0, s>>>(leaves, n, eps, nullptr, nchunks, nullptr, off,
+    pla_kernel<K, V, false><<<pg, 64, 0, s>>>(leaves, n, eps, nchunks, nullptr, off,
                                               (uint32_t *)bst.p, (double *)bsl.p, (double *)bic.p);
     BT_CUDA(cudaGetLastError());
 
