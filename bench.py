@@ -12,7 +12,9 @@ uniformly over the ranks, 10% uniform in [min, max].
 Prints ONE JSON line on rank 0.  `value` is whole-job queries/s of the learned
 search with the queries resident in HBM (device-timed with CUDA events, max
 over ranks); `plain` is the same batch through the plain tree search, and
-`learned_over_plain` their ratio; `e2e` is the learned search through the
+`learned_over_plain` their ratio; `plain_grouped` the reference's batched
+path (radix grouping + grouped search, the grouping timed) on the same batch
+and `learned_over_plain_grouped` that ratio; `e2e` is the learned search through the
 host-buffer C-ABI call bt_point_search_host(BT_POINT_LEARNED) (H2D of the
 queries and D2H of the results inside the timed region).  The path shards as
 independent replicas (every rank holds the tree and answers its own batch, no
@@ -851,6 +853,24 @@ def run_ours(args):
     plain_ms = max_over_ranks(statistics.mean(e[0].elapsed_time(e[1]) for e in pev), dist, device)
     plain_res = out.cpu().numpy()
 
+    # ---- the reference's batched path on the same batch: radix grouping then
+    # the grouped search (BT_POINT_GROUPED, the grouping inside the timing) ---
+    def search_grouped():
+        bt._check(L.bt_point_search(tree.handle, 1, P(dq.data_ptr()), nq, P(out.data_ptr()), sp),
+                  "grouped")
+
+    for _ in range(2):
+        search_grouped()
+    gev = [[torch.cuda.Event(enable_timing=True) for _ in range(2)] for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        gev[i][0].record(stream)
+        search_grouped()
+        gev[i][1].record(stream)
+    torch.cuda.synchronize(device)
+    grouped_ms = max_over_ranks(statistics.mean(e[0].elapsed_time(e[1]) for e in gev), dist, device)
+    grouped_same = bool(np.array_equal(out.cpu().numpy(), plain_res))
+
     # ---- end to end through the host-buffer C-ABI call ----------------------
     hq = torch.from_numpy(q).pin_memory()
     hout = torch.empty(nq, dtype=torch.uint64).pin_memory()
@@ -927,7 +947,12 @@ def run_ours(args):
             "plain": {"value": world * nq / (plain_ms / 1e3), "unit": "queries/s",
                       "ms_per_step": plain_ms, "lanes_per_query": p_lanes, "rounds": p_rounds,
                       "api": "bt_point_search(BT_POINT_BASIC)"},
+            "plain_grouped": {"value": world * nq / (grouped_ms / 1e3), "unit": "queries/s",
+                              "ms_per_step": grouped_ms, "equals_plain": grouped_same,
+                              "api": "bt_point_search(BT_POINT_GROUPED): radix grouping + grouped "
+                                     "search, the grouping timed"},
             "learned_over_plain": plain_ms / ms,
+            "learned_over_plain_grouped": grouped_ms / ms,
             "learned_equals_plain": bool(np.array_equal(learned_res, plain_res)),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
