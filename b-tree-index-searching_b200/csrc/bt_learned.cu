@@ -63,6 +63,8 @@ namespace {
 
 constexpr uint64_t kPlaChunk = 1ull << 14;  // keys per segmentation thread
 constexpr int kHullCap = 32;                 // points per convex hull
+constexpr int kPlaThreads = 64;              // segmentation threads per CTA
+constexpr int kPlaHullStride = 2 * kHullCap + 1;  // hull points per thread in shared memory
 constexpr size_t kStageBudget = 160 * 1024;  // shared memory for the staged keys
 constexpr int kMaxWalk = 8;                  // extra units read before the full descent
 // Search CTA shapes (one CTA per SM: the staged keys), bt_learned_set_shape:
@@ -192,7 +194,11 @@ __global__ void pla_kernel(const unsigned char *__restrict__ leaves, uint64_t n,
                            double *__restrict__ slopes, double *__restrict__ icpts) {
     const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (c >= nchunks) return;
-    PlaPt lh[kHullCap], uh[kHullCap];
+    // the two hulls of this thread in shared memory (kPlaHullStride points
+    // apart per thread: the padding spreads the threads over the banks)
+    extern __shared__ PlaPt pla_sh[];
+    PlaPt *lh = pla_sh + (size_t)threadIdx.x * kPlaHullStride;
+    PlaPt *uh = lh + kHullCap;
     const int64_t e = (int64_t)eps;
     const uint64_t end = min(n, (c + 1) * kPlaChunk);
     uint64_t nseg = 0, out = COUNT ? 0 : offsets[c];
@@ -1057,10 +1063,15 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     BT_CUDA(cudaMalloc(&boff.p, nchunks * sizeof(uint64_t)));
     BT_CUDA(cudaMalloc(&btot.p, sizeof(uint64_t)));
     uint64_t *cnt = (uint64_t *)bcnt.p, *off = (uint64_t *)boff.p, *tot = (uint64_t *)btot.p;
-    const unsigned pg = (unsigned)((nchunks + 63) / 64);
+    const unsigned pg = (unsigned)((nchunks + kPlaThreads - 1) / kPlaThreads);
+    const size_t pla_smem = (size_t)kPlaThreads * kPlaHullStride * sizeof(PlaPt);
+    BT_CUDA(cudaFuncSetAttribute(pla_kernel<K, V, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pla_smem));
+    BT_CUDA(cudaFuncSetAttribute(pla_kernel<K, V, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pla_smem));
     auto count_at = [&](uint32_t eps, uint64_t *total) -> bt_status {
         count_launch();
-        pla_kernel<K, V, true><<<pg, 64, 0, s>>>(leaves, n, eps, nchunks, cnt, nullptr, nullptr,
+        pla_kernel<K, V, true><<<pg, kPlaThreads, pla_smem, s>>>(leaves, n, eps, nchunks, cnt, nullptr, nullptr,
                                                  nullptr, nullptr);
         BT_CUDA(cudaGetLastError());
         bt_status r = launch_scan_u64(cnt, off, nchunks, tot, s);
@@ -1104,7 +1115,7 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     BT_CUDA(cudaMalloc(&bsl.p, nseg * sizeof(double)));
     BT_CUDA(cudaMalloc(&bic.p, nseg * sizeof(double)));
     count_launch();
-    pla_kernel<K, V, false><<<pg, 64, 0, s>>>(leaves, n, eps, nchunks, nullptr, off,
+    pla_kernel<K, V, false><<<pg, kPlaThreads, pla_smem, s>>>(leaves, n, eps, nchunks, nullptr, off,
                                               (uint32_t *)bst.p, (double *)bsl.p, (double *)bic.p);
     BT_CUDA(cudaGetLastError());
 
