@@ -30,6 +30,7 @@
 // with correct bounds) takes the tree's full descent.  Results therefore
 // always equal the plain search.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -918,11 +919,20 @@ bt_status learned_launch_t(const bt_tree *t, const void *d_q, uint64_t nq, void 
     const LearnedDev &m = t->learned->dev;
     auto fn = learned_kernel<K, V, T>;
     const size_t smem = (size_t)m.stage_bytes;
-    static int set_for[64] = {0};
-    int dev = t->device;
-    if (dev >= 0 && dev < 64 && set_for[dev] < (int)smem) {
+    // the largest dynamic shared-memory size this kernel was opened for, per
+    // device (host threads may launch concurrently: atomic, and setting the
+    // attribute twice is harmless)
+    static std::atomic<int> set_for[64];
+    const int dev = t->device;
+    const bool cached = dev >= 0 && dev < 64;
+    if (!cached || set_for[dev].load(std::memory_order_acquire) < (int)smem) {
         BT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        set_for[dev] = (int)smem;
+        if (cached) {
+            int prev = set_for[dev].load(std::memory_order_relaxed);
+            while (prev < (int)smem &&
+                   !set_for[dev].compare_exchange_weak(prev, (int)smem, std::memory_order_release))
+                ;
+        }
     }
     // the kernel indexes its batch with 32-bit offsets: batches of 2^31
     // queries and more go as several launches
