@@ -1093,25 +1093,52 @@ bt_status train_impl(bt_tree *t, const bt_learned_config &cfg, cudaStream_t s,
     uint32_t eps = cfg.max_error;
     uint64_t nseg = 0;
     bt_status r;
+    uint32_t counted = 0;  // the bound of the last count (its per-chunk offsets are in off)
     if (eps == 0) {
-        // the least bound whose segmentation has at most num_segments segments
+        // The least bound whose segmentation has at most num_segments
+        // segments (the count does not grow with the bound).  The bracket
+        // (lo, hi] -- count(lo) above the target, count(hi) at or below --
+        // grows by 4x from 8, then narrows by interpolating log(count)
+        // against log(bound), with a bisection step whenever an
+        // interpolated step fails to halve it.
+        const double tgt = (double)cfg.num_segments;
         uint32_t lo = 0, hi = 8;
+        uint64_t c_lo = 0, c_hi = 0;
         for (;;) {
-            if ((r = count_at(hi, &nseg)) != BT_OK) return r;
-            if (nseg <= cfg.num_segments || hi >= (1u << 30)) break;
+            if ((r = count_at(hi, &c_hi)) != BT_OK) return r;
+            counted = hi;
+            if (c_hi <= cfg.num_segments || hi >= (1u << 30)) break;
             lo = hi;
-            hi *= 2;
+            c_lo = c_hi;
+            hi = std::min<uint32_t>(hi * 4, 1u << 30);
         }
+        bool bisect = false;
         while (hi - lo > 1) {
-            const uint32_t mid = lo + (hi - lo) / 2;
+            uint32_t m = lo + (hi - lo) / 2;
+            if (!bisect && lo > 0 && c_hi > 0 && c_lo > c_hi) {
+                const double f = (std::log((double)c_lo) - std::log(tgt)) /
+                                 (std::log((double)c_lo) - std::log((double)c_hi));
+                const double lm = std::log((double)lo) + f * (std::log((double)hi) - std::log((double)lo));
+                const double g = std::ceil(std::exp(lm));
+                m = g <= (double)lo ? lo + 1 : g >= (double)hi ? hi - 1 : (uint32_t)g;
+            }
             uint64_t c = 0;
-            if ((r = count_at(mid, &c)) != BT_OK) return r;
-            if (c <= cfg.num_segments) hi = mid;
-            else lo = mid;
+            if ((r = count_at(m, &c)) != BT_OK) return r;
+            counted = m;
+            const uint32_t w = hi - lo;
+            if (c <= cfg.num_segments) {
+                hi = m;
+                c_hi = c;
+            } else {
+                lo = m;
+                c_lo = c;
+            }
+            bisect = !bisect && (hi - lo) * 2 > w;
         }
         eps = hi;
     }
-    if ((r = count_at(eps, &nseg)) != BT_OK) return r;
+    if (counted != eps && (r = count_at(eps, &nseg)) != BT_OK) return r;
+    if (counted == eps) BT_CUDA(cudaMemcpy(&nseg, tot, sizeof(uint64_t), cudaMemcpyDeviceToHost));
     const uint32_t nls = (uint32_t)((nseg + kSegPerLine - 1) / kSegPerLine);
     const uint32_t row = 128;  // stage in whole bank rows (the swizzle permutes within rows)
     const uint64_t stage_bytes = ((uint64_t)nls * sizeof(K) + row - 1) / row * row;
