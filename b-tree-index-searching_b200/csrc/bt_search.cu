@@ -6,7 +6,7 @@
 // match, all-ones otherwise), but the grouped variant compares keys, not
 // data[] (:269-276), and writes results back in the caller's order.
 //
-// bounds_kernel replaces the range endpoint + count kernels
+// bounds_line_kernel replaces the range endpoint + count kernels
 // (BtreeRangeSearch.cu:215-374 and :33-211).  With implicit leaf positions
 // the count is upper_bound(hi) - lower_bound(lo); no leaf-chain walk.
 //
@@ -249,85 +249,6 @@ point_window_kernel(const __grid_constant__ DevTree t, const K *__restrict__ q,
     }
 }
 
-// Lower bound of lo and upper bound of hi per query: 64 descents per warp
-// tile of 32 queries (d < 32: lower bound of query d, else upper bound of
-// query d - 32), passed in 2R rounds.  counts[i] = ub - lb (0 if lo > hi);
-// lb_out[i] = lb.
-template <typename K, typename V, int G, int R, bool PERM>
-__global__ void __launch_bounds__(kThreads, 2)
-bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
-              const K *__restrict__ hi, const uint32_t *__restrict__ perm, uint64_t nq,
-              uint64_t *__restrict__ counts, uint64_t *__restrict__ lb_out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    K *s_lvl = reinterpret_cast<K *>(smem_raw);
-    stage_level<K>(s_lvl, t);
-    __syncthreads();
-
-    using LG = LeafGeom<K, V>;
-    constexpr int NG = 32 / G;
-    constexpr int I = G / R;
-    const int lane = threadIdx.x & 31;
-    const int grp = lane / G;
-    const int gl = lane % G;
-    uint64_t *res = reinterpret_cast<uint64_t *>(smem_raw + scratch_offset(t)) + (threadIdx.x >> 5) * 64;
-    const K tmax = (K)t.max_key;
-    const unsigned char *leaves = static_cast<const unsigned char *>(t.leaves);
-    // tile assignment as in point_kernel (CTA-blocked for grouped input)
-    const uint64_t ntiles = (nq + 31) / 32;
-    const uint64_t per_cta = PERM ? (ntiles + gridDim.x - 1) / gridDim.x : 0;
-    const uint64_t t_begin = PERM ? blockIdx.x * per_cta + (threadIdx.x >> 5)
-                                  : (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t t_end = PERM ? min(ntiles, (blockIdx.x + 1) * per_cta) : ntiles;
-    const uint64_t t_step = PERM ? (blockDim.x >> 5) : ((uint64_t)gridDim.x * blockDim.x) >> 5;
-
-    for (uint64_t tile = t_begin; tile < t_end; tile += t_step) {
-        const uint64_t base = tile * 32;
-        const uint64_t my = base + lane;
-        const bool v = my < nq;
-        const K a = v ? lo[my] : (K)0;
-        const K b = v ? hi[my] : (K)0;
-        // lower bound of a: a > max gives n (walk on max instead)
-        const K qa = a <= tmax ? a : tmax;
-        // upper bound of b: b >= max gives n (walk a lower bound of max instead)
-        const K qb = b < tmax ? b : tmax;
-        const bool ub_upper = b < tmax;
-        const uint32_t na = smem_bound<K>(s_lvl, t.smem_entries, qa, false);
-        const uint32_t nb = smem_bound<K>(s_lvl, t.smem_entries, qb, ub_upper);
-
-#pragma unroll
-        for (int r = 0; r < 2 * R; r++) {
-            const bool which = r >= R;  // uniform per round: lower bounds first
-            K qe[I];
-            bool up[I];
-            uint32_t node[I];
-#pragma unroll
-            for (int s = 0; s < I; s++) {
-                const int k = (r % R) * (NG * I) + s * NG + grp;
-                qe[s] = __shfl_sync(0xffffffffu, which ? qb : qa, k);
-                node[s] = __shfl_sync(0xffffffffu, which ? nb : na, k);
-                up[s] = which ? __shfl_sync(0xffffffffu, ub_upper, k) : false;
-            }
-            walk_global<K, G, I>(t, qe, up, node, grp, gl);
-            int pos[I];
-            leaf_bound<K, V, G, I>(leaves, node, qe, up, grp, gl, pos);
-#pragma unroll
-            for (int s = 0; s < I; s++)
-                if (gl == 0)
-                    res[(which ? 32 : 0) + (r % R) * (NG * I) + s * NG + grp] =
-                        (uint64_t)node[s] * LG::S + pos[s];
-        }
-        __syncwarp();
-        if (v) {
-            const uint64_t lb = a <= tmax ? res[lane] : t.n;
-            const uint64_t ub = b < tmax ? res[32 + lane] : t.n;
-            const uint64_t dst = PERM ? (uint64_t)perm[my] : my;
-            counts[dst] = (a <= b && ub > lb) ? ub - lb : 0;
-            if (lb_out) lb_out[dst] = lb;
-        }
-        __syncwarp();
-    }
-}
-
 // Range bounds with the upper bound taken from the lower bound's path.
 // A narrow range usually ends in the same bottom separator line as it
 // starts: while the group walks lo down, it counts that line's separators
@@ -335,7 +256,7 @@ bounds_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
 // leaf block whenever the line's last separator is above hi; both leaf
 // blocks are then read together.  Only the queries whose range leaves that
 // line take a second descent, compacted per warp into as few rounds as they
-// need.  Same results as bounds_kernel.
+// need.  counts[i] = ub - lb (0 if lo > hi); lb_out[i] = lb.
 template <typename K, typename V, int G, int R, bool PERM>
 __global__ void __launch_bounds__(kThreads, 2)
 bounds_line_kernel(const __grid_constant__ DevTree t, const K *__restrict__ lo,
