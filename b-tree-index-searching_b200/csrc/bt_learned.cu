@@ -16,14 +16,16 @@
 //   2. segment line (one L2 read): four leaf models; the key's segment gives
 //      a predicted rank p and its bound eps, so the key's rank lies in
 //      [p - eps - 1, p + eps + 1].
-//   3. code lines (one or two L2 reads): the thresholds between the leaf
-//      units of that window; the thresholds at or below the key count the
-//      units to skip.
-//   4. leaf unit (the DRAM read): the key's block(s) and values.
+//   3. code line (one L2 read; two for the queries whose count continues
+//      into the neighbouring line, which wait in a per-warp queue for a
+//      pass of their own): the thresholds between the leaf units of that
+//      window; the thresholds at or below the key count the units to skip.
+//   4. leaf unit (the DRAM read, by a lane quad: one request per unit): the
+//      key's block(s) and values.
 //
 // Exactness.  Every bound used above is measured on the device with the
-// search's own FP32 operations (explicit round-to-nearest intrinsics, no
-// contraction), and every function of the key involved is monotone, so a
+// search's own FP32 operations (explicit round-to-nearest intrinsics and
+// fused multiply-adds, no implicit contraction), and every function of the key involved is monotone, so a
 // bound measured at the keys holds for every query between them.  A query
 // whose key lies just above a unit's threshold bucket lands one unit early
 // and reads the next one; a query that would leave its window (impossible
